@@ -1,0 +1,297 @@
+"""gv_b200 — B200-native GraphVine dynamic-graph store and analytics.
+
+Python mirror of the reference's host API (class GraphVine in
+include/dynamicStructure/graphvine.cuh:29-58 and the algorithm entry points
+static_pagerank / dynamic_pagerank / static_tc / dynamic_tc / bc), calling
+libgv.so through its C ABI.  Arrays are numpy (host memory) or torch CUDA
+tensors (device memory); vertex ids are 0-based uint32.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+
+from . import _lib
+from ._lib import GV_MEM_DEVICE, GV_MEM_HOST, GV_OK, STATUS_NAMES, gv_config
+
+__all__ = ["GraphVine", "GvError", "gen_rmat", "gen_uniform", "kernel_launches", "version"]
+
+
+class GvError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        self.status = status
+        msg = _lib.lib().gv_last_error_string().decode(errors="replace")
+        super().__init__(f"{where}: {STATUS_NAMES.get(status, status)}: {msg}")
+
+
+def _check(st: int, where: str) -> None:
+    if st != GV_OK:
+        raise GvError(st, where)
+
+
+def _is_torch_cuda(a) -> bool:
+    return hasattr(a, "is_cuda") and a.is_cuda
+
+
+def _ptr(a, dtype) -> tuple[int, int, object]:
+    """(pointer, mem flag, keep-alive) for a numpy array or a torch CUDA tensor."""
+    if a is None:
+        return 0, GV_MEM_HOST, None
+    if _is_torch_cuda(a):
+        import torch
+        want = {np.uint32: (torch.int32, torch.uint32), np.float32: (torch.float32,),
+                np.uint64: (torch.int64, torch.uint64), np.int32: (torch.int32,), np.uint8: (torch.uint8,)}[dtype]
+        if a.dtype not in want:
+            raise TypeError(f"device tensor must have dtype {want[0]}, got {a.dtype}")
+        if not a.is_contiguous():
+            raise ValueError("device tensor must be contiguous")
+        return a.data_ptr(), GV_MEM_DEVICE, a
+    arr = np.ascontiguousarray(a, dtype=dtype)
+    return arr.ctypes.data, GV_MEM_HOST, arr
+
+
+def _stream(stream) -> int:
+    if stream is None:
+        return 0
+    if isinstance(stream, int):
+        return stream
+    return int(stream.cuda_stream)
+
+
+def kernel_launches() -> int:
+    return int(_lib.lib().gv_kernel_launches())
+
+
+def version() -> str:
+    return _lib.lib().gv_version().decode()
+
+
+def gen_rmat(scale: int, num_pairs: int, seed: int, first: int = 0, device=None, stream=None):
+    """R-MAT pairs (src, dst) as numpy arrays, or torch CUDA tensors if device is given."""
+    L = _lib.lib()
+    if device is not None:
+        import torch
+        src = torch.empty(num_pairs, dtype=torch.int32, device=device)
+        dst = torch.empty(num_pairs, dtype=torch.int32, device=device)
+        _check(L.gv_gen_rmat(scale, first, num_pairs, seed, src.data_ptr(), dst.data_ptr(), GV_MEM_DEVICE,
+                             _stream(stream)), "gv_gen_rmat")
+        return src, dst
+    src = np.empty(num_pairs, np.uint32)
+    dst = np.empty(num_pairs, np.uint32)
+    _check(L.gv_gen_rmat(scale, first, num_pairs, seed, src.ctypes.data, dst.ctypes.data, GV_MEM_HOST, 0), "gv_gen_rmat")
+    return src, dst
+
+
+def gen_uniform(n: int, count: int, seed: int, device=None, stream=None):
+    L = _lib.lib()
+    if device is not None:
+        import torch
+        src = torch.empty(count, dtype=torch.int32, device=device)
+        dst = torch.empty(count, dtype=torch.int32, device=device)
+        _check(L.gv_gen_uniform(n, count, seed, src.data_ptr(), dst.data_ptr(), GV_MEM_DEVICE, _stream(stream)),
+               "gv_gen_uniform")
+        return src, dst
+    src = np.empty(count, np.uint32)
+    dst = np.empty(count, np.uint32)
+    _check(L.gv_gen_uniform(n, count, seed, src.ctypes.data, dst.ctypes.data, GV_MEM_HOST, 0), "gv_gen_uniform")
+    return src, dst
+
+
+class GraphVine:
+    """A dynamic graph resident on one GPU (edge-block CBT store)."""
+
+    def __init__(self, num_vertices: int, *, block_size: int = 128, threads_per_vertex: int = 8,
+                 directed: bool = False, weighted: bool = False, device: int = 0, pool_blocks: int = 0,
+                 hbm_budget_bytes: int = 0, max_batch_pairs: int = 1 << 20):
+        L = _lib.lib()
+        cfg = gv_config()
+        _check(L.gv_config_init(C.byref(cfg), num_vertices), "gv_config_init")
+        cfg.block_size = block_size
+        cfg.threads_per_vertex = threads_per_vertex
+        cfg.directed = int(directed)
+        cfg.weighted = int(weighted)
+        cfg.device = device
+        cfg.pool_blocks = pool_blocks
+        cfg.hbm_budget_bytes = hbm_budget_bytes
+        cfg.max_batch_pairs = max_batch_pairs
+        h = C.c_void_p()
+        _check(L.gv_create(C.byref(cfg), C.byref(h)), "gv_create")
+        self._h = h
+        self.n = num_vertices
+        self.weighted = weighted
+        self.directed = directed
+        self.device = device
+
+    # -- lifecycle ---------------------------------------------------------
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            _lib.lib().gv_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self) -> int:
+        return self._h.value
+
+    # -- updates (GraphVine::bulkBuild / batchInsert / batchDelete / compaction)
+    def bulk_build(self, offsets, dst, weights=None, stream=None) -> None:
+        po, mem, k1 = _ptr(offsets, np.uint64)
+        pd, _, k2 = _ptr(dst, np.uint32)
+        pw, _, k3 = _ptr(weights, np.float32)
+        _check(_lib.lib().gv_bulk_build_csr(self._h, po, pd, pw or None, mem, _stream(stream)), "gv_bulk_build_csr")
+
+    def batch_insert(self, src, dst, weights=None, stream=None) -> None:
+        ps, mem, k1 = _ptr(src, np.uint32)
+        pd, _, k2 = _ptr(dst, np.uint32)
+        pw, _, k3 = _ptr(weights, np.float32)
+        k = len(src)
+        _check(_lib.lib().gv_insert_edges(self._h, ps, pd, pw or None, k, mem, _stream(stream)), "gv_insert_edges")
+        if mem == GV_MEM_HOST:
+            self._keep = (k1, k2, k3)
+
+    def batch_delete(self, src, dst, stream=None) -> None:
+        ps, mem, k1 = _ptr(src, np.uint32)
+        pd, _, k2 = _ptr(dst, np.uint32)
+        _check(_lib.lib().gv_delete_edges(self._h, ps, pd, len(src), mem, _stream(stream)), "gv_delete_edges")
+        if mem == GV_MEM_HOST:
+            self._keep = (k1, k2)
+
+    def compaction(self, stream=None) -> None:
+        _check(_lib.lib().gv_compact(self._h, _stream(stream)), "gv_compact")
+
+    def synchronize(self, stream=None) -> None:
+        _check(_lib.lib().gv_synchronize(self._h, _stream(stream)), "gv_synchronize")
+
+    # -- facts -------------------------------------------------------------
+    def num_edges(self) -> int:
+        m = C.c_uint64()
+        _check(_lib.lib().gv_num_edges(self._h, C.byref(m)), "gv_num_edges")
+        return m.value
+
+    def pool_stats(self) -> tuple[int, int]:
+        cap, free = C.c_uint64(), C.c_uint64()
+        _check(_lib.lib().gv_pool_stats(self._h, C.byref(cap), C.byref(free)), "gv_pool_stats")
+        return cap.value, free.value
+
+    def degrees(self) -> np.ndarray:
+        out = np.empty(self.n, np.uint32)
+        _check(_lib.lib().gv_degrees(self._h, out.ctypes.data, GV_MEM_HOST, 0), "gv_degrees")
+        return out
+
+    def export_csr(self, with_weights: bool = False):
+        """(offsets[n+1] uint64, dst[m] uint32, weights[m] float32 or None), storage order."""
+        m = self.num_edges()
+        off = np.empty(self.n + 1, np.uint64)
+        dst = np.empty(max(m, 1), np.uint32)
+        w = np.empty(max(m, 1), np.float32) if with_weights else None
+        _check(_lib.lib().gv_export_csr(self._h, off.ctypes.data, dst.ctypes.data,
+                                        w.ctypes.data if w is not None else None, m, GV_MEM_HOST, 0), "gv_export_csr")
+        return off, dst[:m], (w[:m] if w is not None else None)
+
+    def affected(self) -> np.ndarray:
+        out = np.empty(self.n, np.uint8)
+        _check(_lib.lib().gv_affected(self._h, out.ctypes.data, GV_MEM_HOST, 0), "gv_affected")
+        return out
+
+    def clear_affected(self, stream=None) -> None:
+        _check(_lib.lib().gv_clear_affected(self._h, _stream(stream)), "gv_clear_affected")
+
+    def check(self) -> tuple[int, int, int]:
+        v, code, vert = C.c_uint64(), C.c_uint32(), C.c_uint32()
+        _check(_lib.lib().gv_check(self._h, C.byref(v), C.byref(code), C.byref(vert)), "gv_check")
+        return v.value, code.value, vert.value
+
+    # -- analytics (static_pagerank / dynamic_pagerank / static_tc / bc) ------
+    def static_pagerank(self, alpha: float = 0.85, epsilon: float = 1e-6, max_iter: int = 100, out=None, stream=None):
+        x = np.empty(self.n, np.float32) if out is None else out
+        px, mem, _ = _ptr(x, np.float32)
+        sw = C.c_int32()
+        _check(_lib.lib().gv_pagerank(self._h, alpha, epsilon, max_iter, px, C.byref(sw), mem, _stream(stream)),
+               "gv_pagerank")
+        return x, sw.value
+
+    def dynamic_pagerank(self, x, alpha: float = 0.85, epsilon: float = 1e-6, max_iter: int = 100, stream=None):
+        """Warm start from x (updated in place for device tensors; returns the result)."""
+        if _is_torch_cuda(x):
+            px, mem, _ = _ptr(x, np.float32)
+            xr = x
+        else:
+            xr = np.array(x, dtype=np.float32, copy=True)
+            px, mem = xr.ctypes.data, GV_MEM_HOST
+        sw = C.c_int32()
+        _check(_lib.lib().gv_pagerank_dynamic(self._h, alpha, epsilon, max_iter, px, C.byref(sw), mem,
+                                              _stream(stream)), "gv_pagerank_dynamic")
+        return xr, sw.value
+
+    def ppr(self, source: int, alpha: float = 0.85, epsilon: float = 1e-6, max_iter: int = 100, stream=None):
+        x = np.empty(self.n, np.float32)
+        sw = C.c_int32()
+        _check(_lib.lib().gv_ppr(self._h, source, alpha, epsilon, max_iter, x.ctypes.data, C.byref(sw),
+                                 GV_MEM_HOST, _stream(stream)), "gv_ppr")
+        return x, sw.value
+
+    def static_tc(self, per_vertex: bool = True, stream=None):
+        pv = np.empty(self.n, np.uint64) if per_vertex else None
+        tot = C.c_uint64()
+        _check(_lib.lib().gv_tc(self._h, pv.ctypes.data if pv is not None else None, C.byref(tot), GV_MEM_HOST,
+                                _stream(stream)), "gv_tc")
+        return pv, tot.value
+
+    def tc_subset(self, subset, stream=None) -> np.ndarray:
+        s = np.ascontiguousarray(subset, dtype=np.uint32)
+        out = np.empty(len(s), np.uint64)
+        _check(_lib.lib().gv_tc_subset(self._h, s.ctypes.data, len(s), out.ctypes.data, GV_MEM_HOST,
+                                       _stream(stream)), "gv_tc_subset")
+        return out
+
+    def bc(self, sources=None, stream=None) -> np.ndarray:
+        out = np.empty(self.n, np.float32)
+        if sources is None:
+            ps, ns = None, 0
+        else:
+            s = np.ascontiguousarray(sources, dtype=np.uint32)
+            ps, ns = s.ctypes.data, len(s)
+        _check(_lib.lib().gv_bc(self._h, ps, ns, out.ctypes.data, GV_MEM_HOST, _stream(stream)), "gv_bc")
+        return out
+
+    def bfs_sigma(self, source: int, stream=None):
+        dist = np.empty(self.n, np.int32)
+        sigma = np.empty(self.n, np.uint64)
+        _check(_lib.lib().gv_bfs_sigma(self._h, source, dist.ctypes.data, sigma.ctypes.data, GV_MEM_HOST,
+                                       _stream(stream)), "gv_bfs_sigma")
+        return dist, sigma
+
+    # -- differentiation ---------------------------------------------------
+    def wpr_forward(self, alpha: float = 0.85, tol: float = 1e-7, max_iter: int = 200, stream=None):
+        x = np.empty(self.n, np.float32)
+        sw = C.c_int32()
+        _check(_lib.lib().gv_wpr_forward(self._h, alpha, tol, max_iter, x.ctypes.data, C.byref(sw), GV_MEM_HOST,
+                                         _stream(stream)), "gv_wpr_forward")
+        return x, sw.value
+
+    def wpr_backward(self, x, c, alpha: float = 0.85, tol: float = 1e-7, max_iter: int = 200, mode: int = 0,
+                     stream=None):
+        """(grad per entry in export order, lambda, sweeps)."""
+        m = self.num_edges()
+        xa = np.ascontiguousarray(x, dtype=np.float32)
+        ca = np.ascontiguousarray(c, dtype=np.float32)
+        grad = np.empty(max(m, 1), np.float32)
+        lam = np.empty(self.n, np.float32)
+        sw = C.c_int32()
+        _check(_lib.lib().gv_wpr_backward(self._h, alpha, tol, max_iter, xa.ctypes.data, ca.ctypes.data, mode,
+                                          grad.ctypes.data, m, lam.ctypes.data, C.byref(sw), GV_MEM_HOST,
+                                          _stream(stream)), "gv_wpr_backward")
+        return grad[:m], lam, sw.value

@@ -1,0 +1,1254 @@
+// Analytics that traverse the edge-block CBT store directly: PageRank,
+// personalised PageRank, exact triangle counting, betweenness centrality and
+// weighted PageRank with its adjoint.
+//
+// Reference kernels replaced:
+//   PageRank   src/algorithm/pagerank/pr_kernel.cu:3-103, pagerank.cu:3-132
+//              (push + float atomics + host reduce per sweep) -> pull over
+//              the symmetric store, deterministic, residual reduced on the
+//              device, no host round trip per sweep;
+//   TC         src/algorithm/tc/tc_kernel.cu:3-147 (triple linear scans,
+//              float counts) -> degree-oriented sorted snapshot + merge-path
+//              intersection, uint64 counts;
+//   BC         src/algorithm/bc/bc_kernel.cu:3-119, bc.cu:3-88 (one source
+//              per host loop, int sigma, unordered dependency pass) ->
+//              batched multi-source level-synchronous BFS with uint64 sigma
+//              and a level-ordered fp64 dependency sweep.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+#include "store.cuh"
+#include "group.cuh"
+#include "prims.cuh"
+#include "launch.hpp"
+
+namespace gv {
+namespace {
+
+constexpr int AN_THREADS = 256;
+constexpr int BIG_TAB_A = 1024;
+
+// ----------------------------------------------------------- pull sweeps
+// out[v] = base(v) + alpha * scale(v) * sum_{u in N(v)} w(v,u) * gather[u]
+struct PullArgs {
+    const float *gather;
+    float alpha;
+    float base_all;       // added to every vertex
+    uint32_t base_src;    // vertex that also gets base_src_val (GV_NIL: none)
+    float base_src_val;
+    const float *cvec;    // per-vertex additive term (nullable)
+    const float *rscale;  // per-vertex multiplier of the sum (nullable)
+    const float *xold;    // previous iterate (residual)
+    float *xnew;
+    float *contrib;       // xnew / deg (nullable)
+    double *partial;      // one slot per CTA (+ heavy kernel slots)
+    const int *state;     // [0] done flag
+};
+
+__device__ __forceinline__ float pull_finish(const PullArgs &a, uint32_t v, float sum, uint32_t deg,
+                                             double &res) {
+    float base = a.base_all + (v == a.base_src ? a.base_src_val : 0.f);
+    if (a.cvec) base += a.cvec[v];
+    const float sc = a.rscale ? a.rscale[v] : 1.f;
+    const float xv = base + a.alpha * (sc * sum);
+    a.xnew[v] = xv;
+    if (a.contrib) a.contrib[v] = deg ? xv / (float)deg : 0.f;
+    res += (double)fabsf(xv - a.xold[v]);
+    return xv;
+}
+
+template <int TPV, bool W>
+__global__ void __launch_bounds__(AN_THREADS) k_pull(DevGraph g, PullArgs a) {
+    __shared__ double red[AN_THREADS / 32];
+    if (a.state[0]) return;
+    constexpr int GPC = AN_THREADS / TPV;
+    __shared__ uint32_t tabs[GPC][BIG_BLOCKS];
+    Group<TPV> G;
+    uint32_t *tab = tabs[threadIdx.x / TPV];
+    const uint32_t ngroups = gridDim.x * GPC;
+    double res = 0.0;
+    for (uint32_t v = blockIdx.x * GPC + threadIdx.x / TPV; v < g.n; v += ngroups) {
+        const uint4 rec = g.vtx[v];
+        const uint32_t fill = rec.y, nb = blocks_for(fill, g.logB);
+        if (nb > BIG_BLOCKS) continue;  // k_pull_heavy
+        float sum = 0.f;
+        if (nb == 1) {
+            const size_t base = (size_t)rec.x << g.logB;
+            for (uint32_t e = G.gl * 4; e < fill; e += TPV * 4) {
+                const uint4 q = *reinterpret_cast<const uint4 *>(g.pool + base + e);
+                float4 wq = make_float4(1.f, 1.f, 1.f, 1.f);
+                if (W) wq = *reinterpret_cast<const float4 *>(g.wpool + base + e);
+                const uint32_t ev[4] = {q.x, q.y, q.z, q.w};
+                const float wv[4] = {wq.x, wq.y, wq.z, wq.w};
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    if (e + j < fill && ev[j] != GV_TOMB) sum += W ? wv[j] * __ldg(a.gather + ev[j]) : __ldg(a.gather + ev[j]);
+            }
+        } else if (nb > 1) {
+            fill_block_table(g, rec.x, 0, nb, tab, G.gl, TPV);
+            G.sync();
+            const uint32_t nq = (fill + 3) >> 2;
+            for (uint32_t qi = G.gl; qi < nq; qi += TPV) {
+                const uint32_t e = qi << 2;
+                const size_t at = ((size_t)tab[e >> g.logB] << g.logB) + (e & (g.B - 1));
+                const uint4 q = *reinterpret_cast<const uint4 *>(g.pool + at);
+                float4 wq = make_float4(1.f, 1.f, 1.f, 1.f);
+                if (W) wq = *reinterpret_cast<const float4 *>(g.wpool + at);
+                const uint32_t ev[4] = {q.x, q.y, q.z, q.w};
+                const float wv[4] = {wq.x, wq.y, wq.z, wq.w};
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    if (e + j < fill && ev[j] != GV_TOMB) sum += W ? wv[j] * __ldg(a.gather + ev[j]) : __ldg(a.gather + ev[j]);
+            }
+            G.sync();
+        }
+        sum = G.sum(sum);
+        if (G.gl == 0) pull_finish(a, v, sum, rec.z, res);
+    }
+    res = warp_sum(res);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = res;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int i = 0; i < AN_THREADS / 32; ++i) t += red[i];
+        a.partial[blockIdx.x] = t;
+    }
+}
+
+template <bool W>
+__global__ void __launch_bounds__(BIG_THREADS) k_pull_heavy(DevGraph g, PullArgs a, const uint32_t *__restrict__ heavy,
+                                                            uint32_t nheavy, uint32_t part_base) {
+    __shared__ uint32_t tab[BIG_TAB_A];
+    __shared__ float wred[BIG_THREADS / 32];
+    if (a.state[0]) return;
+    double res = 0.0;
+    for (uint32_t hi = blockIdx.x; hi < nheavy; hi += gridDim.x) {
+        const uint32_t v = heavy[hi];
+        const uint4 rec = g.vtx[v];
+        const uint32_t fill = rec.y, nb = blocks_for(fill, g.logB);
+        float sum = 0.f;
+        for (uint32_t k0 = 0; k0 < nb; k0 += BIG_TAB_A) {
+            const uint32_t kc = min((uint32_t)BIG_TAB_A, nb - k0);
+            fill_block_table(g, rec.x, k0, kc, tab, threadIdx.x, BIG_THREADS);
+            __syncthreads();
+            const uint32_t e0 = k0 << g.logB, e1 = min(fill, (k0 + kc) << g.logB);
+            const uint32_t nq = (e1 - e0 + 3) >> 2;
+            for (uint32_t qi = threadIdx.x; qi < nq; qi += BIG_THREADS) {
+                const uint32_t e = e0 + (qi << 2);
+                const size_t at = ((size_t)tab[(e >> g.logB) - k0] << g.logB) + (e & (g.B - 1));
+                const uint4 q = *reinterpret_cast<const uint4 *>(g.pool + at);
+                float4 wq = make_float4(1.f, 1.f, 1.f, 1.f);
+                if (W) wq = *reinterpret_cast<const float4 *>(g.wpool + at);
+                const uint32_t ev[4] = {q.x, q.y, q.z, q.w};
+                const float wv[4] = {wq.x, wq.y, wq.z, wq.w};
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    if (e + j < fill && ev[j] != GV_TOMB) sum += W ? wv[j] * __ldg(a.gather + ev[j]) : __ldg(a.gather + ev[j]);
+            }
+            __syncthreads();
+        }
+        sum = warp_sum(sum);
+        if ((threadIdx.x & 31) == 0) wred[threadIdx.x >> 5] = sum;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            float t = 0.f;
+            for (int i = 0; i < BIG_THREADS / 32; ++i) t += wred[i];
+            pull_finish(a, v, t, rec.z, res);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) a.partial[part_base + blockIdx.x] = res;
+}
+
+// Sums the per-CTA residuals in a fixed order; latches convergence.
+__global__ void k_iter_done(const double *__restrict__ partial, uint32_t nparts, float eps, int *state,
+                            double *last_res) {
+    __shared__ double red[32];
+    if (state[0]) return;
+    double t = 0.0;
+    for (uint32_t i = threadIdx.x; i < nparts; i += blockDim.x) t += partial[i];
+    t = warp_sum(t);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = t;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int i = 0; i < (int)(blockDim.x / 32); ++i) s += red[i];
+        *last_res = s;
+        state[1] += 1;
+        if (s < (double)eps) state[0] = 1;
+    }
+}
+
+__global__ void k_heavy_list(DevGraph g, uint32_t *list, unsigned long long *cnt) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < g.n; v += gridDim.x * blockDim.x) {
+        const uint32_t nb = blocks_for(g.vtx[v].y, g.logB);
+        if (nb > BIG_BLOCKS) list[atomicAdd(cnt, 1ull)] = v;
+    }
+}
+
+__global__ void k_fill_f32(float *x, uint32_t n, float val, uint32_t one_at, float one_val) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+        x[v] = (v == one_at) ? one_val : val;
+}
+
+// contrib[u] = x[u] * scale(u), scale = 1/deg (PageRank) or 1/s_u (weighted)
+__global__ void k_contrib(DevGraph g, const float *__restrict__ x, const float *__restrict__ rscale,
+                          float *__restrict__ contrib) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < g.n; v += gridDim.x * blockDim.x) {
+        if (rscale) contrib[v] = x[v] * rscale[v];
+        else {
+            const uint32_t d = g.vtx[v].z;
+            contrib[v] = d ? x[v] / (float)d : 0.f;
+        }
+    }
+}
+
+// ------------------------------------------------------------ PR driver
+struct IterBufs {
+    float *x0, *x1, *c0, *c1;
+    double *partial;
+    int *state;  // [0] done, [1] sweeps
+    double *res;
+    uint32_t *heavy;
+    unsigned long long *nheavy;
+};
+
+size_t iter_bytes(uint32_t n, uint32_t parts) {
+    return (size_t)n * 4 * 4 + (size_t)parts * 8 + 64 + (size_t)n * 4 + 64;
+}
+
+IterBufs carve_iter(void *base, uint32_t n, uint32_t parts) {
+    char *p = static_cast<char *>(base);
+    IterBufs b;
+    b.x0 = (float *)p; p += (size_t)n * 4;
+    b.x1 = (float *)p; p += (size_t)n * 4;
+    b.c0 = (float *)p; p += (size_t)n * 4;
+    b.c1 = (float *)p; p += (size_t)n * 4;
+    b.partial = (double *)p; p += (size_t)parts * 8;
+    b.state = (int *)p; p += 16;
+    b.res = (double *)p; p += 16;
+    b.nheavy = (unsigned long long *)p; p += 32;
+    b.heavy = (uint32_t *)p;
+    return b;
+}
+
+constexpr unsigned PULL_GRID = 148 * 8;
+constexpr unsigned HEAVY_GRID = 148;
+
+// Runs pull sweeps until convergence or max_iter.  Result in *result (one of
+// x0/x1).  `weighted_rscale` non-null selects the weighted gather (adjoint).
+gv_status run_sweeps(gv_graph *g, cudaStream_t s, IterBufs &b, PullArgs proto, bool weighted,
+                     const float *weighted_rscale, float eps, int max_iter, bool contrib_pr,
+                     int *sweeps_out, float **result) {
+    DevGraph d = g->d;
+    cudaMemsetAsync(b.nheavy, 0, 8, s);
+    GV_LAUNCH(k_heavy_list, grid_for(d.n, 256), 256, 0, s, d, b.heavy, b.nheavy);
+    unsigned long long nheavy = 0;
+    cudaMemcpyAsync(&nheavy, b.nheavy, 8, cudaMemcpyDeviceToHost, s);
+    cudaMemsetAsync(b.state, 0, 16, s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_status(e, "sweeps");
+    const uint32_t nparts = PULL_GRID + HEAVY_GRID;
+    cudaMemsetAsync(b.partial, 0, (size_t)nparts * 8, s);
+    int h_state[2] = {0, 0};
+    float *xa = b.x0, *xb = b.x1, *ca = b.c0, *cb = b.c1;
+    int launched = 0;
+    while (launched < max_iter) {
+        const int chunk = std::min(8, max_iter - launched);
+        for (int i = 0; i < chunk; ++i) {
+            PullArgs a = proto;
+            a.gather = contrib_pr ? ca : (weighted ? xa : ca);
+            a.xold = xa;
+            a.xnew = xb;
+            a.contrib = contrib_pr ? cb : nullptr;
+            a.partial = b.partial;
+            a.state = b.state;
+            if (!contrib_pr && !weighted) a.gather = ca;
+            dispatch_tpv(g->cfg.threads_per_vertex, [&](auto t) {
+                constexpr int T = decltype(t)::value;
+                if (weighted) GV_LAUNCH((k_pull<T, true>), PULL_GRID, AN_THREADS, 0, s, d, a);
+                else GV_LAUNCH((k_pull<T, false>), PULL_GRID, AN_THREADS, 0, s, d, a);
+            });
+            if (nheavy) {
+                if (weighted) GV_LAUNCH(k_pull_heavy<true>, HEAVY_GRID, BIG_THREADS, 0, s, d, a, b.heavy, (uint32_t)nheavy, PULL_GRID);
+                else GV_LAUNCH(k_pull_heavy<false>, HEAVY_GRID, BIG_THREADS, 0, s, d, a, b.heavy, (uint32_t)nheavy, PULL_GRID);
+            }
+            GV_LAUNCH(k_iter_done, 1, 256, 0, s, b.partial, nparts, eps, b.state, b.res);
+            std::swap(xa, xb);
+            std::swap(ca, cb);
+        }
+        launched += chunk;
+        e = cudaMemcpyAsync(h_state, b.state, 8, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return cuda_status(e, "sweeps");
+        if (h_state[0]) break;
+    }
+    (void)weighted_rscale;
+    *sweeps_out = h_state[1];
+    // sweep i (1-based) wrote x1 when i is odd
+    *result = (h_state[1] & 1) ? b.x1 : b.x0;
+    return GV_OK;
+}
+
+gv_status copy_out_f32(const float *src, float *dst, uint32_t n, int mem, cudaStream_t s) {
+    cudaError_t e = cudaMemcpyAsync(dst, src, (size_t)n * 4,
+                                    mem == GV_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    return cuda_status(e, "copy out");
+}
+
+gv_status pagerank_impl(gv_graph *g, float alpha, float eps, int max_iter, const float *x_init, int init_mem,
+                        uint32_t source, float *x_out, int32_t *sweeps, int mem, cudaStream_t s) {
+    const uint32_t n = g->d.n;
+    if (g->cfg.directed) { set_error("PageRank pull needs an undirected (symmetric) store"); return GV_ERR_STATE; }
+    const uint32_t parts = PULL_GRID + HEAVY_GRID;
+    void *buf = analytics_scratch(g, iter_bytes(n, parts));
+    if (!buf) return GV_ERR_NOMEM;
+    IterBufs b = carve_iter(buf, n, parts);
+    DevGraph d = g->d;
+    if (x_init) {
+        cudaError_t e = cudaMemcpyAsync(b.x0, x_init, (size_t)n * 4,
+                                        init_mem == GV_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess) return cuda_status(e, "pagerank init");
+    } else if (source == GV_NIL) {
+        GV_LAUNCH(k_fill_f32, grid_for(n, 256), 256, 0, s, b.x0, n, 1.0f / (float)n, GV_NIL, 0.f);
+    } else {
+        GV_LAUNCH(k_fill_f32, grid_for(n, 256), 256, 0, s, b.x0, n, 0.f, source, 1.f);
+    }
+    GV_LAUNCH(k_contrib, grid_for(n, 256), 256, 0, s, d, (const float *)b.x0, (const float *)nullptr, b.c0);
+    PullArgs a{};
+    a.alpha = alpha;
+    if (source == GV_NIL) {
+        a.base_all = (1.0f - alpha) / (float)n;
+        a.base_src = GV_NIL;
+    } else {
+        a.base_all = 0.f;
+        a.base_src = source;
+        a.base_src_val = 1.0f - alpha;
+    }
+    int sw = 0;
+    float *res = nullptr;
+    gv_status st = run_sweeps(g, s, b, a, false, nullptr, eps, max_iter, true, &sw, &res);
+    if (st != GV_OK) return st;
+    if (sweeps) *sweeps = sw;
+    return copy_out_f32(res, x_out, n, mem, s);
+}
+
+// ------------------------------------------------------------------- TC
+// Orientation: u -> v iff (deg u, u) < (deg v, v).  Max out-degree <= sqrt(2m).
+__device__ __forceinline__ bool rank_less(uint32_t du, uint32_t u, uint32_t dv, uint32_t v) {
+    return du < dv || (du == dv && u < v);
+}
+
+template <int TPV>
+__global__ void __launch_bounds__(AN_THREADS) k_tc_outdeg(DevGraph g, uint32_t *__restrict__ dplus) {
+    constexpr int GPC = AN_THREADS / TPV;
+    __shared__ uint32_t tabs[GPC][BIG_BLOCKS];
+    Group<TPV> G;
+    uint32_t *tab = tabs[threadIdx.x / TPV];
+    const uint32_t ngroups = gridDim.x * GPC;
+    for (uint32_t u = blockIdx.x * GPC + threadIdx.x / TPV; u < g.n; u += ngroups) {
+        const uint4 rec = g.vtx[u];
+        const uint32_t fill = rec.y, nb = blocks_for(fill, g.logB), du = rec.z;
+        uint32_t c = 0;
+        for (uint32_t k0 = 0; k0 < nb; k0 += BIG_BLOCKS) {
+            const uint32_t kc = min((uint32_t)BIG_BLOCKS, nb - k0);
+            fill_block_table(g, rec.x, k0, kc, tab, G.gl, TPV);
+            G.sync();
+            const uint32_t e0 = k0 << g.logB, e1 = min(fill, (k0 + kc) << g.logB);
+            for (uint32_t e = e0 + G.gl; e < e1; e += TPV) {
+                const uint32_t v = g.pool[((size_t)tab[(e >> g.logB) - k0] << g.logB) + (e & (g.B - 1))];
+                if (v != GV_TOMB && rank_less(du, u, g.vtx[v].z, v)) ++c;
+            }
+            G.sync();
+        }
+        c = G.sum(c);
+        if (G.gl == 0) dplus[u] = c;
+    }
+}
+
+template <int TPV>
+__global__ void __launch_bounds__(AN_THREADS) k_tc_write(DevGraph g, const unsigned long long *__restrict__ off,
+                                                         uint32_t *__restrict__ snap, uint32_t *__restrict__ mid_list,
+                                                         uint32_t *__restrict__ big_list, unsigned long long *cnts) {
+    constexpr int GPC = AN_THREADS / TPV;
+    __shared__ uint32_t tabs[GPC][BIG_BLOCKS];
+    Group<TPV> G;
+    uint32_t *tab = tabs[threadIdx.x / TPV];
+    const uint32_t ngroups = gridDim.x * GPC;
+    for (uint32_t u = blockIdx.x * GPC + threadIdx.x / TPV; u < g.n; u += ngroups) {
+        const uint4 rec = g.vtx[u];
+        const uint32_t fill = rec.y, nb = blocks_for(fill, g.logB), du = rec.z;
+        unsigned long long w = off[u];
+        const unsigned long long wend = off[u + 1];
+        const uint32_t len = (uint32_t)(wend - w);
+        for (uint32_t k0 = 0; k0 < nb; k0 += BIG_BLOCKS) {
+            const uint32_t kc = min((uint32_t)BIG_BLOCKS, nb - k0);
+            fill_block_table(g, rec.x, k0, kc, tab, G.gl, TPV);
+            G.sync();
+            const uint32_t e0 = k0 << g.logB, e1 = min(fill, (k0 + kc) << g.logB);
+            for (uint32_t c0 = e0; c0 < e1; c0 += TPV) {
+                const uint32_t e = c0 + G.gl;
+                uint32_t v = GV_TOMB;
+                if (e < e1) v = g.pool[((size_t)tab[(e >> g.logB) - k0] << g.logB) + (e & (g.B - 1))];
+                const uint32_t keep = (v != GV_TOMB && rank_less(du, u, g.vtx[v].z, v)) ? 1u : 0u;
+                uint32_t tot;
+                const uint32_t pre = G.excl_scan(keep, tot);
+                if (keep && w + pre < wend) snap[w + pre] = v;
+                w += tot;
+            }
+            G.sync();
+        }
+        if (G.gl == 0 && len > 16) {
+            if (len <= 1024) mid_list[atomicAdd(&cnts[0], 1ull)] = u;
+            else big_list[atomicAdd(&cnts[1], 1ull)] = u;
+        }
+        if (len > 1 && len <= 16) {
+            // tiny lists: one lane sorts (insertion sort)
+            if (G.gl == 0) {
+                uint32_t *a = snap + off[u];
+                for (uint32_t i = 1; i < len; ++i) {
+                    const uint32_t x = a[i];
+                    uint32_t j = i;
+                    while (j > 0 && a[j - 1] > x) { a[j] = a[j - 1]; --j; }
+                    a[j] = x;
+                }
+            }
+        }
+        G.sync();
+    }
+}
+
+// Bitonic sort of a[0, len) using smem buffer s of size P (power of two >= len).
+__device__ void smem_bitonic(uint32_t *a, uint32_t len, uint32_t *s, uint32_t P, uint32_t t, uint32_t nt,
+                             bool warp_only) {
+    for (uint32_t i = t; i < P; i += nt) s[i] = i < len ? a[i] : 0xFFFFFFFFu;
+    if (warp_only) __syncwarp(); else __syncthreads();
+    for (uint32_t k = 2; k <= P; k <<= 1) {
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            for (uint32_t i = t; i < P; i += nt) {
+                const uint32_t ixj = i ^ j;
+                if (ixj > i) {
+                    const bool up = (i & k) == 0;
+                    const uint32_t x = s[i], y = s[ixj];
+                    if ((x > y) == up) { s[i] = y; s[ixj] = x; }
+                }
+            }
+            if (warp_only) __syncwarp(); else __syncthreads();
+        }
+    }
+    for (uint32_t i = t; i < len; i += nt) a[i] = s[i];
+    if (warp_only) __syncwarp(); else __syncthreads();
+}
+
+__global__ void __launch_bounds__(AN_THREADS) k_tc_sort_mid(const unsigned long long *__restrict__ off,
+                                                            uint32_t *__restrict__ snap,
+                                                            const uint32_t *__restrict__ list,
+                                                            const unsigned long long *cnt) {
+    __shared__ uint32_t buf[AN_THREADS / 32][1024];
+    const uint32_t nl = (uint32_t)cnt[0];
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t nw = gridDim.x * (AN_THREADS / 32);
+    for (uint32_t i = blockIdx.x * (AN_THREADS / 32) + warp; i < nl; i += nw) {
+        const uint32_t u = list[i];
+        const uint32_t len = (uint32_t)(off[u + 1] - off[u]);
+        uint32_t P = 32;
+        while (P < len) P <<= 1;
+        smem_bitonic(snap + off[u], len, buf[warp], P, lane, 32, true);
+    }
+}
+
+__global__ void __launch_bounds__(1024) k_tc_sort_big(const unsigned long long *__restrict__ off,
+                                                      uint32_t *__restrict__ snap, const uint32_t *__restrict__ list,
+                                                      const unsigned long long *cnt, uint32_t cap) {
+    extern __shared__ uint32_t sbuf[];
+    const uint32_t nl = (uint32_t)cnt[1];
+    for (uint32_t i = blockIdx.x; i < nl; i += gridDim.x) {
+        const uint32_t u = list[i];
+        const uint32_t len = (uint32_t)(off[u + 1] - off[u]);
+        uint32_t P = 1024;
+        while (P < len) P <<= 1;
+        if (P > cap) continue;  // cannot happen: cap is sized from the longest list
+        smem_bitonic(snap + off[u], len, sbuf, P, threadIdx.x, blockDim.x, false);
+    }
+}
+
+// Co-rank on diagonal d of merging A (ties first) and B.
+__device__ __forceinline__ uint32_t corank(const uint32_t *A, uint32_t la, const uint32_t *B, uint32_t lb, uint32_t d) {
+    uint32_t lo = d > lb ? d - lb : 0, hi = d < la ? d : la;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (A[mid] <= B[d - mid - 1]) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+// Group per oriented edge (u -> v): merge-path intersection of N+(u), N+(v).
+// INCIDENT: credit all three vertices; else credit the smallest id (the
+// reference's owner, tc_kernel.cu:25-30).
+template <int TPV, bool INCIDENT>
+__global__ void __launch_bounds__(AN_THREADS) k_tc_count(const unsigned long long *__restrict__ off,
+                                                         const uint32_t *__restrict__ snap,
+                                                         const uint32_t *__restrict__ esrc, uint64_t m_plus,
+                                                         unsigned long long *__restrict__ tcount) {
+    constexpr int GPC = AN_THREADS / TPV;
+    Group<TPV> G;
+    const uint64_t ngroups = (uint64_t)gridDim.x * GPC;
+    for (uint64_t ei = (uint64_t)blockIdx.x * GPC + threadIdx.x / TPV; ei < m_plus; ei += ngroups) {
+        const uint32_t u = esrc[ei], v = snap[ei];
+        const uint32_t *A = snap + off[u];
+        const uint32_t la = (uint32_t)(off[u + 1] - off[u]);
+        const uint32_t *Bv = snap + off[v];
+        const uint32_t lb = (uint32_t)(off[v + 1] - off[v]);
+        const uint32_t tot = la + lb;
+        const uint32_t per = (tot + TPV - 1) / TPV;
+        const uint32_t d0 = min(tot, G.gl * per), d1 = min(tot, d0 + per);
+        uint32_t i = corank(A, la, Bv, lb, d0), j = d0 - i;
+        uint32_t cu = 0, cv = 0;
+        const uint32_t uv_min = min(u, v);
+        for (uint32_t d = d0; d < d1; ++d) {
+            if (i < la && (j >= lb || A[i] <= Bv[j])) {
+                const uint32_t w = A[i];
+                if (j < lb && Bv[j] == w) {
+                    if (INCIDENT) {
+                        ++cu; ++cv;
+                        atomicAdd(&tcount[w], 1ull);
+                    } else if (w < uv_min) {
+                        atomicAdd(&tcount[w], 1ull);
+                    } else if (u < v) {
+                        ++cu;
+                    } else {
+                        ++cv;
+                    }
+                }
+                ++i;
+            } else {
+                ++j;
+            }
+        }
+        cu = G.sum(cu);
+        cv = G.sum(cv);
+        if (G.gl == 0) {
+            if (cu) atomicAdd(&tcount[u], (unsigned long long)cu);
+            if (cv) atomicAdd(&tcount[v], (unsigned long long)cv);
+        }
+    }
+}
+
+__global__ void k_tc_esrc(const unsigned long long *__restrict__ off, uint32_t n, uint32_t *__restrict__ esrc) {
+    for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x)
+        for (unsigned long long i = off[u]; i < off[u + 1]; ++i) esrc[i] = u;
+}
+
+__global__ void k_sum_u64(const unsigned long long *__restrict__ x, uint32_t n, unsigned long long *out) {
+    unsigned long long t = 0;
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) t += x[v];
+    t = warp_sum(t);
+    if ((threadIdx.x & 31) == 0 && t) atomicAdd(out, t);
+}
+
+__global__ void k_gather_u64(const unsigned long long *__restrict__ x, const uint32_t *__restrict__ idx, uint64_t k,
+                             unsigned long long *__restrict__ out) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < k; i += (uint64_t)gridDim.x * blockDim.x)
+        out[i] = x[idx[i]];
+}
+
+struct TcBufs {
+    uint32_t *dplus;
+    unsigned long long *off;
+    uint32_t *snap, *esrc, *mid, *big;
+    unsigned long long *cnts;
+    unsigned long long *tcount;
+};
+
+// Builds the oriented sorted snapshot and counts.  tcount[n] receives the
+// per-vertex counts (owner or incident).  Returns m_plus via *mplus.
+gv_status tc_run(gv_graph *g, cudaStream_t s, bool incident, unsigned long long **tcount_out) {
+    if (g->cfg.directed) { set_error("triangle counting needs an undirected store"); return GV_ERR_STATE; }
+    DevGraph d = g->d;
+    const uint32_t n = d.n;
+    // Phase 1: oriented out-degrees and offsets, then size the snapshot exactly.
+    const size_t head = ((size_t)n + 1) * 8 + (size_t)n * 8 + 64 + (size_t)n * 4 * 3;
+    void *buf = analytics_scratch(g, head + 256);
+    if (!buf) return GV_ERR_NOMEM;
+    TcBufs b;
+    auto carve = [&](void *base, uint64_t mp) {
+        char *p = (char *)base;
+        b.off = (unsigned long long *)p; p += ((size_t)n + 1) * 8;
+        b.tcount = (unsigned long long *)p; p += (size_t)n * 8;
+        b.cnts = (unsigned long long *)p; p += 64;
+        b.dplus = (uint32_t *)p; p += (size_t)n * 4;
+        b.mid = (uint32_t *)p; p += (size_t)n * 4;
+        b.big = (uint32_t *)p; p += (size_t)n * 4;
+        b.snap = (uint32_t *)p; p += mp * 4;
+        b.esrc = (uint32_t *)p;
+    };
+    carve(buf, 0);
+    const uint32_t tpv = g->cfg.threads_per_vertex;
+    dispatch_tpv(tpv, [&](auto t) {
+        constexpr int T = decltype(t)::value;
+        GV_LAUNCH((k_tc_outdeg<T>), grid_for(n, AN_THREADS / T), AN_THREADS, 0, s, d, b.dplus);
+    });
+    scan_exclusive_u32_to_u64(b.dplus, b.off, n, b.off + n, g->bs.scan_tmp, s);
+    unsigned long long mplus = 0;
+    {
+        cudaError_t e = cudaMemcpyAsync(&mplus, b.off + n, 8, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return cuda_status(e, "tc");
+    }
+    if (g->an_bytes < head + 2 * (mplus + 1) * 4 + 256) {
+        // grow the scratch and keep the offsets computed so far
+        std::vector<unsigned long long> hoff((size_t)n + 1);
+        cudaMemcpy(hoff.data(), b.off, hoff.size() * 8, cudaMemcpyDeviceToHost);
+        buf = analytics_scratch(g, head + 2 * (mplus + 1) * 4 + 256);
+        if (!buf) return GV_ERR_NOMEM;
+        carve(buf, mplus + 1);
+        cudaMemcpyAsync(b.off, hoff.data(), hoff.size() * 8, cudaMemcpyHostToDevice, s);
+    } else {
+        carve(buf, mplus + 1);
+    }
+    cudaMemsetAsync(b.cnts, 0, 64, s);
+    cudaMemsetAsync(b.tcount, 0, (size_t)n * 8, s);
+    dispatch_tpv(tpv, [&](auto t) {
+        constexpr int T = decltype(t)::value;
+        GV_LAUNCH((k_tc_write<T>), grid_for(n, AN_THREADS / T), AN_THREADS, 0, s, d, (const unsigned long long *)b.off,
+                  b.snap, b.mid, b.big, b.cnts);
+    });
+    GV_LAUNCH(k_tc_sort_mid, 148 * 4, AN_THREADS, 0, s, (const unsigned long long *)b.off, b.snap,
+              (const uint32_t *)b.mid, (const unsigned long long *)b.cnts);
+    // longest list bounds the CTA sort's shared memory
+    unsigned long long h[2] = {0, 0};
+    cudaMemcpyAsync(h, b.cnts, 16, cudaMemcpyDeviceToHost, s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_status(e, "tc");
+    if (h[1]) {
+        std::vector<uint32_t> bl(h[1]);
+        std::vector<unsigned long long> hoff(n + 1);
+        cudaMemcpy(hoff.data(), b.off, ((size_t)n + 1) * 8, cudaMemcpyDeviceToHost);
+        cudaMemcpy(bl.data(), b.big, h[1] * 4, cudaMemcpyDeviceToHost);
+        uint64_t mx = 0;
+        for (uint32_t u : bl) mx = std::max<uint64_t>(mx, hoff[u + 1] - hoff[u]);
+        uint32_t P = 1024;
+        while (P < mx) P <<= 1;
+        const size_t smem = (size_t)P * 4;
+        if (smem > 227 * 1024) { set_error("oriented out-degree exceeds the shared-memory sort"); return GV_ERR_UNSUPPORTED; }
+        cudaFuncSetAttribute(k_tc_sort_big, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        GV_LAUNCH(k_tc_sort_big, 148, 1024, smem, s, (const unsigned long long *)b.off, b.snap,
+                  (const uint32_t *)b.big, (const unsigned long long *)b.cnts, P);
+    }
+    GV_LAUNCH(k_tc_esrc, grid_for(n, 256), 256, 0, s, (const unsigned long long *)b.off, n, b.esrc);
+    const unsigned cgrid = grid_for(mplus, AN_THREADS / 8, 148 * 16);
+    if (incident) GV_LAUNCH((k_tc_count<8, true>), cgrid, AN_THREADS, 0, s, (const unsigned long long *)b.off, b.snap, b.esrc, mplus, b.tcount);
+    else GV_LAUNCH((k_tc_count<8, false>), cgrid, AN_THREADS, 0, s, (const unsigned long long *)b.off, b.snap, b.esrc, mplus, b.tcount);
+    *tcount_out = b.tcount;
+    return cuda_status(cudaGetLastError(), "tc launch");
+}
+
+// ------------------------------------------------------------------- BC
+// Batched multi-source BFS: source slot b of the batch owns rows b*n.. of
+// dist/sigma/delta and a BFS order queue; all slots advance one level per
+// launch (grid.y = slot).
+struct BcBufs {
+    int32_t *dist;
+    unsigned long long *sigma;
+    double *delta;
+    uint32_t *queue;              // BFS order per slot (levels contiguous)
+    unsigned long long *lstart;   // [slot][MAXL+1] level boundaries
+    unsigned long long *qtail;    // per slot
+    int *active;                  // any slot still expanding
+    double *bc;                   // fp64 accumulator (n)
+};
+
+constexpr int BC_MAXL = 4096;
+
+template <int TPV>
+__global__ void __launch_bounds__(AN_THREADS) k_bfs_level(DevGraph g, BcBufs b, uint32_t level) {
+    constexpr int GPC = AN_THREADS / TPV;
+    __shared__ uint32_t tabs[GPC][BIG_BLOCKS];
+    const uint32_t slot = blockIdx.y, n = g.n;
+    const unsigned long long *ls = b.lstart + (size_t)slot * (BC_MAXL + 1);
+    const unsigned long long f0 = ls[level], f1 = ls[level + 1];
+    if (f0 >= f1) return;
+    int32_t *dist = b.dist + (size_t)slot * n;
+    unsigned long long *sigma = b.sigma + (size_t)slot * n;
+    uint32_t *queue = b.queue + (size_t)slot * n;
+    Group<TPV> G;
+    uint32_t *tab = tabs[threadIdx.x / TPV];
+    const int32_t nl = (int32_t)level + 1;
+    const unsigned long long ngroups = (unsigned long long)gridDim.x * GPC;
+    for (unsigned long long fi = f0 + (unsigned long long)blockIdx.x * GPC + threadIdx.x / TPV; fi < f1; fi += ngroups) {
+        const uint32_t v = queue[fi];
+        const unsigned long long sv = sigma[v];
+        const uint4 rec = g.vtx[v];
+        const uint32_t fill = rec.y, nb = blocks_for(fill, g.logB);
+        for (uint32_t k0 = 0; k0 < nb; k0 += BIG_BLOCKS) {
+            const uint32_t kc = min((uint32_t)BIG_BLOCKS, nb - k0);
+            fill_block_table(g, rec.x, k0, kc, tab, G.gl, TPV);
+            G.sync();
+            const uint32_t e0 = k0 << g.logB, e1 = min(fill, (k0 + kc) << g.logB);
+            for (uint32_t e = e0 + G.gl; e < e1; e += TPV) {
+                const uint32_t w = g.pool[((size_t)tab[(e >> g.logB) - k0] << g.logB) + (e & (g.B - 1))];
+                if (w == GV_TOMB) continue;
+                int32_t dw = dist[w];
+                if (dw < 0) {
+                    dw = atomicCAS(&dist[w], -1, nl);
+                    if (dw < 0) {
+                        dw = nl;
+                        const unsigned long long p = atomicAdd(&b.qtail[slot], 1ull);
+                        queue[p] = w;
+                    }
+                }
+                if (dw == nl) atomicAdd(&sigma[w], sv);
+            }
+            G.sync();
+        }
+    }
+}
+
+// Closes a level for every slot: records where the next level ends.
+__global__ void k_bfs_close(BcBufs b, uint32_t nslots, uint32_t level) {
+    const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= nslots) return;
+    unsigned long long *ls = b.lstart + (size_t)slot * (BC_MAXL + 1);
+    const unsigned long long t = b.qtail[slot];
+    ls[level + 2] = t;
+    if (t > ls[level + 1]) atomicOr(b.active, 1);
+}
+
+__global__ void k_bfs_init(BcBufs b, uint32_t n, const uint32_t *__restrict__ sources, uint32_t nslots) {
+    const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= nslots) return;
+    const uint32_t s = sources[slot];
+    b.dist[(size_t)slot * n + s] = 0;
+    b.sigma[(size_t)slot * n + s] = 1ull;
+    b.queue[(size_t)slot * n] = s;
+    b.qtail[slot] = 1;
+    unsigned long long *ls = b.lstart + (size_t)slot * (BC_MAXL + 1);
+    ls[0] = 0;
+    ls[1] = 1;
+}
+
+template <int TPV>
+__global__ void __launch_bounds__(AN_THREADS) k_bc_dep(DevGraph g, BcBufs b, uint32_t level) {
+    constexpr int GPC = AN_THREADS / TPV;
+    __shared__ uint32_t tabs[GPC][BIG_BLOCKS];
+    const uint32_t slot = blockIdx.y, n = g.n;
+    const unsigned long long *ls = b.lstart + (size_t)slot * (BC_MAXL + 1);
+    const unsigned long long f0 = ls[level], f1 = ls[level + 1];
+    if (f0 >= f1) return;
+    const int32_t *dist = b.dist + (size_t)slot * n;
+    const unsigned long long *sigma = b.sigma + (size_t)slot * n;
+    double *delta = b.delta + (size_t)slot * n;
+    const uint32_t *queue = b.queue + (size_t)slot * n;
+    Group<TPV> G;
+    uint32_t *tab = tabs[threadIdx.x / TPV];
+    const int32_t nl = (int32_t)level + 1;
+    const unsigned long long ngroups = (unsigned long long)gridDim.x * GPC;
+    for (unsigned long long fi = f0 + (unsigned long long)blockIdx.x * GPC + threadIdx.x / TPV; fi < f1; fi += ngroups) {
+        const uint32_t v = queue[fi];
+        const double sv = (double)sigma[v];
+        const uint4 rec = g.vtx[v];
+        const uint32_t fill = rec.y, nb = blocks_for(fill, g.logB);
+        double acc = 0.0;
+        for (uint32_t k0 = 0; k0 < nb; k0 += BIG_BLOCKS) {
+            const uint32_t kc = min((uint32_t)BIG_BLOCKS, nb - k0);
+            fill_block_table(g, rec.x, k0, kc, tab, G.gl, TPV);
+            G.sync();
+            const uint32_t e0 = k0 << g.logB, e1 = min(fill, (k0 + kc) << g.logB);
+            for (uint32_t e = e0 + G.gl; e < e1; e += TPV) {
+                const uint32_t w = g.pool[((size_t)tab[(e >> g.logB) - k0] << g.logB) + (e & (g.B - 1))];
+                if (w == GV_TOMB) continue;
+                if (dist[w] == nl) acc += (sv / (double)sigma[w]) * (1.0 + delta[w]);
+            }
+            G.sync();
+        }
+        acc = G.sum(acc);
+        if (G.gl == 0) delta[v] = acc;
+    }
+}
+
+// bc[v] += sum over slots of delta (fixed slot order), skipping each slot's source.
+__global__ void k_bc_reduce(BcBufs b, uint32_t n, uint32_t nslots, const uint32_t *__restrict__ sources) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        double t = 0.0;
+        for (uint32_t s = 0; s < nslots; ++s)
+            if (sources[s] != v && b.dist[(size_t)s * n + v] > 0) t += b.delta[(size_t)s * n + v];
+        b.bc[v] += t;
+    }
+}
+
+__global__ void k_f64_to_f32(const double *__restrict__ x, float *__restrict__ y, uint32_t n) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) y[v] = (float)x[v];
+}
+
+// Runs forward BFS for a batch of sources; returns the deepest level count.
+gv_status bfs_batch(gv_graph *g, cudaStream_t s, BcBufs &b, const uint32_t *dsrc, uint32_t nslots, uint32_t *depth_out,
+                    int *h_active) {
+    DevGraph d = g->d;
+    const uint32_t n = d.n;
+    cudaMemsetAsync(b.dist, 0xFF, (size_t)nslots * n * 4, s);
+    cudaMemsetAsync(b.sigma, 0, (size_t)nslots * n * 8, s);
+    GV_LAUNCH(k_bfs_init, (nslots + 63) / 64, 64, 0, s, b, n, dsrc, nslots);
+    uint32_t level = 0;
+    const unsigned gx = grid_for((uint64_t)n, AN_THREADS, 148 * 8 / std::max(1u, nslots) + 1);
+    while (true) {
+        const int chunk = 4;
+        cudaMemsetAsync(b.active, 0, 4, s);
+        for (int i = 0; i < chunk; ++i) {
+            if (level + 2 > BC_MAXL) { set_error("BFS deeper than the level table"); return GV_ERR_UNSUPPORTED; }
+            dispatch_tpv(g->cfg.threads_per_vertex, [&](auto t) {
+                constexpr int T = decltype(t)::value;
+                GV_LAUNCH((k_bfs_level<T>), dim3(gx, nslots), AN_THREADS, 0, s, d, b, level);
+            });
+            GV_LAUNCH(k_bfs_close, (nslots + 63) / 64, 64, 0, s, b, nslots, level);
+            ++level;
+        }
+        cudaError_t e = cudaMemcpyAsync(h_active, b.active, 4, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return cuda_status(e, "bfs");
+        if (!*h_active) break;
+    }
+    *depth_out = level;
+    return GV_OK;
+}
+
+gv_status bc_impl(gv_graph *g, const uint32_t *sources, uint64_t ns, float *bc_out, int mem, cudaStream_t s) {
+    DevGraph d = g->d;
+    const uint32_t n = d.n;
+    std::vector<uint32_t> src_all;
+    const uint32_t *hs = sources;
+    if (!sources || ns == 0) {
+        src_all.resize(n);
+        for (uint32_t i = 0; i < n; ++i) src_all[i] = i;
+        hs = src_all.data();
+        ns = n;
+    } else if (mem == GV_MEM_DEVICE) {
+        src_all.resize(ns);
+        cudaMemcpy(src_all.data(), sources, ns * 4, cudaMemcpyDeviceToHost);
+        hs = src_all.data();
+    }
+    for (uint64_t i = 0; i < ns; ++i)
+        if (hs[i] >= n) { set_error("BC source out of range"); return GV_ERR_INVALID; }
+    // slots per batch: bounded by memory (~24 B per vertex per slot)
+    uint64_t slots = 64;
+    const uint64_t per_slot = (uint64_t)n * (4 + 8 + 8 + 4) + (BC_MAXL + 1) * 8 + 16;
+    size_t fr = 0, tot = 0;
+    cudaMemGetInfo(&fr, &tot);
+    while (slots > 1 && slots * per_slot > fr / 4) slots >>= 1;
+    if (slots > ns) slots = ns;
+    const size_t bytes = slots * per_slot + (size_t)n * 8 + slots * 4 + 256;
+    void *buf = analytics_scratch(g, bytes);
+    if (!buf) return GV_ERR_NOMEM;
+    char *p = (char *)buf;
+    BcBufs b;
+    b.bc = (double *)p; p += (size_t)n * 8;
+    b.delta = (double *)p; p += slots * n * 8;
+    b.sigma = (unsigned long long *)p; p += slots * n * 8;
+    b.lstart = (unsigned long long *)p; p += slots * (BC_MAXL + 1) * 8;
+    b.qtail = (unsigned long long *)p; p += slots * 8;
+    b.dist = (int32_t *)p; p += slots * n * 4;
+    b.queue = (uint32_t *)p; p += slots * n * 4;
+    b.active = (int *)p; p += 16;
+    uint32_t *dsrc = (uint32_t *)p;
+    cudaMemsetAsync(b.bc, 0, (size_t)n * 8, s);
+    std::vector<unsigned long long> hls;
+    int *h_active = nullptr;
+    cudaMallocHost(&h_active, 16);
+    gv_status st = GV_OK;
+    for (uint64_t s0 = 0; s0 < ns; s0 += slots) {
+        const uint32_t nsl = (uint32_t)std::min<uint64_t>(slots, ns - s0);
+        cudaMemcpyAsync(dsrc, hs + s0, nsl * 4, cudaMemcpyHostToDevice, s);
+        uint32_t depth = 0;
+        st = bfs_batch(g, s, b, dsrc, nsl, &depth, h_active);
+        if (st != GV_OK) break;
+        cudaMemsetAsync(b.delta, 0, (size_t)nsl * n * 8, s);
+        const unsigned gx = grid_for((uint64_t)n, AN_THREADS, 148 * 8 / std::max(1u, nsl) + 1);
+        for (int32_t lv = (int32_t)depth; lv >= 0; --lv) {
+            dispatch_tpv(g->cfg.threads_per_vertex, [&](auto t) {
+                constexpr int T = decltype(t)::value;
+                GV_LAUNCH((k_bc_dep<T>), dim3(gx, nsl), AN_THREADS, 0, s, d, b, (uint32_t)lv);
+            });
+        }
+        GV_LAUNCH(k_bc_reduce, grid_for(n, 256), 256, 0, s, b, n, nsl, (const uint32_t *)dsrc);
+    }
+    cudaFreeHost(h_active);
+    if (st != GV_OK) return st;
+    float *tmp = (float *)b.dist;  // reuse: n floats fit in the dist rows
+    GV_LAUNCH(k_f64_to_f32, grid_for(n, 256), 256, 0, s, (const double *)b.bc, tmp, n);
+    return copy_out_f32(tmp, bc_out, n, mem, s);
+}
+
+// ------------------------------------------------------- weighted PageRank
+__global__ void k_row_sums(DevGraph g, float *__restrict__ rinv) {
+    for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < g.n; u += gridDim.x * blockDim.x) {
+        const uint4 rec = g.vtx[u];
+        const uint32_t fill = rec.y, nb = blocks_for(fill, g.logB);
+        double sacc = 0.0;
+        for (uint32_t k = 0; k < nb; ++k) {
+            const uint32_t b = k == 0 ? rec.x : cbt_block(g.left, g.right, rec.x, k);
+            const uint32_t slots = min(g.B, fill - (k << g.logB));
+            const size_t base = (size_t)b << g.logB;
+            for (uint32_t i = 0; i < slots; ++i)
+                if (g.pool[base + i] != GV_TOMB) sacc += (double)g.wpool[base + i];
+        }
+        rinv[u] = sacc > 0.0 ? (float)(1.0 / sacc) : 0.f;
+    }
+}
+
+// Transposed snapshot: in-edges of every v with the raw weight.
+__global__ void k_indeg(DevGraph g, uint32_t *__restrict__ indeg) {
+    for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < g.n; u += gridDim.x * blockDim.x) {
+        const uint4 rec = g.vtx[u];
+        const uint32_t fill = rec.y, nb = blocks_for(fill, g.logB);
+        for (uint32_t k = 0; k < nb; ++k) {
+            const uint32_t b = k == 0 ? rec.x : cbt_block(g.left, g.right, rec.x, k);
+            const uint32_t slots = min(g.B, fill - (k << g.logB));
+            const size_t base = (size_t)b << g.logB;
+            for (uint32_t i = 0; i < slots; ++i) {
+                const uint32_t v = g.pool[base + i];
+                if (v != GV_TOMB) atomicAdd(&indeg[v], 1u);
+            }
+        }
+    }
+}
+
+__global__ void k_fill_transpose(DevGraph g, const unsigned long long *__restrict__ toff, uint32_t *__restrict__ cursor,
+                                 uint32_t *__restrict__ tsrc, float *__restrict__ tw) {
+    for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < g.n; u += gridDim.x * blockDim.x) {
+        const uint4 rec = g.vtx[u];
+        const uint32_t fill = rec.y, nb = blocks_for(fill, g.logB);
+        for (uint32_t k = 0; k < nb; ++k) {
+            const uint32_t b = k == 0 ? rec.x : cbt_block(g.left, g.right, rec.x, k);
+            const uint32_t slots = min(g.B, fill - (k << g.logB));
+            const size_t base = (size_t)b << g.logB;
+            for (uint32_t i = 0; i < slots; ++i) {
+                const uint32_t v = g.pool[base + i];
+                if (v == GV_TOMB) continue;
+                const unsigned long long p = toff[v] + atomicAdd(&cursor[v], 1u);
+                tsrc[p] = u;
+                tw[p] = g.wpool[base + i];
+            }
+        }
+    }
+}
+
+// Group per v over its in-edges: x'[v] = base + alpha * sum w_uv * contrib[u]
+template <int TPV>
+__global__ void __launch_bounds__(AN_THREADS) k_wpr_fwd(uint32_t n, const unsigned long long *__restrict__ toff,
+                                                        const uint32_t *__restrict__ tsrc, const float *__restrict__ tw,
+                                                        PullArgs a) {
+    __shared__ double red[AN_THREADS / 32];
+    if (a.state[0]) return;
+    constexpr int GPC = AN_THREADS / TPV;
+    Group<TPV> G;
+    double res = 0.0;
+    const uint32_t ngroups = gridDim.x * GPC;
+    for (uint32_t v = blockIdx.x * GPC + threadIdx.x / TPV; v < n; v += ngroups) {
+        float sum = 0.f;
+        for (unsigned long long i = toff[v] + G.gl; i < toff[v + 1]; i += TPV) sum += tw[i] * __ldg(a.gather + tsrc[i]);
+        sum = G.sum(sum);
+        if (G.gl == 0) pull_finish(a, v, sum, 0, res);
+    }
+    res = warp_sum(res);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = res;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int i = 0; i < AN_THREADS / 32; ++i) t += red[i];
+        a.partial[blockIdx.x] = t;
+    }
+}
+
+__global__ void k_mul(const float *__restrict__ x, const float *__restrict__ r, float *__restrict__ y, uint32_t n) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) y[v] = x[v] * r[v];
+}
+
+// Gradient per live entry, in export order (offsets = exclusive scan of live degrees).
+template <int TPV>
+__global__ void __launch_bounds__(AN_THREADS) k_wpr_grad(DevGraph g, const unsigned long long *__restrict__ off,
+                                                         const float *__restrict__ x, const float *__restrict__ lam,
+                                                         const float *__restrict__ c, const float *__restrict__ rinv,
+                                                         float alpha, int mode, float *__restrict__ grad) {
+    Group<TPV> G;
+    constexpr int GPC = AN_THREADS / TPV;
+    const uint32_t ngroups = gridDim.x * GPC;
+    for (uint32_t u = blockIdx.x * GPC + threadIdx.x / TPV; u < g.n; u += ngroups) {
+        const uint4 rec = g.vtx[u];
+        const uint32_t fill = rec.y, nb = blocks_for(fill, g.logB);
+        unsigned long long w = off[u];
+        const unsigned long long wend = off[u + 1];
+        const float xu = x[u];
+        const float ku = mode == 1 ? 0.f : (c[u] - lam[u]);
+        const float ru = rinv[u];
+        for (uint32_t k = 0; k < nb; ++k) {
+            const uint32_t b = (k == 0) ? rec.x : cbt_block(g.left, g.right, rec.x, k);
+            const uint32_t slots = min(g.B, fill - (k << g.logB));
+            for (uint32_t c0 = 0; c0 < slots; c0 += TPV) {
+                const uint32_t i = c0 + G.gl;
+                const uint32_t v = (i < slots) ? g.pool[((size_t)b << g.logB) + i] : GV_TOMB;
+                const uint32_t keep = v != GV_TOMB;
+                uint32_t tot;
+                const uint32_t pre = G.excl_scan(keep, tot);
+                if (keep && w + pre < wend) {
+                    const float lv = lam[v];
+                    grad[w + pre] = (mode == 1) ? alpha * xu * lv : xu * (alpha * lv + ku) * ru;
+                }
+                w += tot;
+            }
+        }
+    }
+}
+
+}  // namespace
+}  // namespace gv
+
+using namespace gv;
+
+extern "C" {
+
+gv_status gv_pagerank(gv_graph *g, float alpha, float epsilon, int32_t max_iter, float *x_out, int32_t *sweeps,
+                      int mem, void *stream) {
+    if (!g || !x_out || max_iter < 0) return GV_ERR_INVALID;
+    return pagerank_impl(g, alpha, epsilon, max_iter, nullptr, 0, GV_NIL, x_out, sweeps, mem, (cudaStream_t)stream);
+}
+
+gv_status gv_pagerank_dynamic(gv_graph *g, float alpha, float epsilon, int32_t max_iter, float *x_inout,
+                              int32_t *sweeps, int mem, void *stream) {
+    if (!g || !x_inout || max_iter < 0) return GV_ERR_INVALID;
+    return pagerank_impl(g, alpha, epsilon, max_iter, x_inout, mem, GV_NIL, x_inout, sweeps, mem, (cudaStream_t)stream);
+}
+
+gv_status gv_ppr(gv_graph *g, uint32_t source, float alpha, float epsilon, int32_t max_iter, float *x_out,
+                 int32_t *sweeps, int mem, void *stream) {
+    if (!g || !x_out || max_iter < 0 || source >= g->d.n) return GV_ERR_INVALID;
+    return pagerank_impl(g, alpha, epsilon, max_iter, nullptr, 0, source, x_out, sweeps, mem, (cudaStream_t)stream);
+}
+
+gv_status gv_tc(gv_graph *g, uint64_t *per_vertex, uint64_t *total, int mem, void *stream) {
+    if (!g || !total) return GV_ERR_INVALID;
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned long long *tc = nullptr;
+    gv_status st = tc_run(g, s, false, &tc);
+    if (st != GV_OK) return st;
+    const uint32_t n = g->d.n;
+    unsigned long long *dtot = (unsigned long long *)g->bs.tile_cnt;  // 8 bytes of batch scratch
+    cudaMemsetAsync(dtot, 0, 8, s);
+    GV_LAUNCH(k_sum_u64, grid_for(n, 256), 256, 0, s, (const unsigned long long *)tc, n, dtot);
+    unsigned long long h = 0;
+    cudaError_t e = cudaMemcpyAsync(&h, dtot, 8, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && per_vertex)
+        e = cudaMemcpyAsync(per_vertex, tc, (size_t)n * 8,
+                            mem == GV_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_status(e, "tc");
+    *total = h;
+    return GV_OK;
+}
+
+gv_status gv_tc_subset(gv_graph *g, const uint32_t *subset, uint64_t ns, uint64_t *out, int mem, void *stream) {
+    if (!g || (ns && (!subset || !out))) return GV_ERR_INVALID;
+    if (ns == 0) return GV_OK;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (mem == GV_MEM_HOST)
+        for (uint64_t i = 0; i < ns; ++i)
+            if (subset[i] >= g->d.n) { set_error("subset vertex out of range"); return GV_ERR_INVALID; }
+    unsigned long long *tc = nullptr;
+    gv_status st = tc_run(g, s, true, &tc);
+    if (st != GV_OK) return st;
+    uint32_t *didx = nullptr;
+    unsigned long long *dout = nullptr;
+    if (mem == GV_MEM_DEVICE) {
+        didx = const_cast<uint32_t *>(subset);
+        dout = (unsigned long long *)out;
+    } else {
+        if (cudaMalloc(&didx, ns * 4) != cudaSuccess || cudaMalloc(&dout, ns * 8) != cudaSuccess) {
+            cudaGetLastError();
+            if (didx) cudaFree(didx);
+            return GV_ERR_NOMEM;
+        }
+        cudaMemcpyAsync(didx, subset, ns * 4, cudaMemcpyHostToDevice, s);
+    }
+    GV_LAUNCH(k_gather_u64, grid_for(ns, 256), 256, 0, s, (const unsigned long long *)tc, (const uint32_t *)didx, ns, dout);
+    cudaError_t e = cudaSuccess;
+    if (mem != GV_MEM_DEVICE) e = cudaMemcpyAsync(out, dout, ns * 8, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (mem != GV_MEM_DEVICE) {
+        cudaFree(didx);
+        cudaFree(dout);
+    }
+    return cuda_status(e, "tc subset");
+}
+
+gv_status gv_bc(gv_graph *g, const uint32_t *sources, uint64_t ns, float *bc_out, int mem, void *stream) {
+    if (!g || !bc_out) return GV_ERR_INVALID;
+    return bc_impl(g, sources, ns, bc_out, mem, (cudaStream_t)stream);
+}
+
+gv_status gv_bfs_sigma(gv_graph *g, uint32_t source, int32_t *dist, uint64_t *sigma, int mem, void *stream) {
+    if (!g || !dist || !sigma || source >= g->d.n) return GV_ERR_INVALID;
+    cudaStream_t s = (cudaStream_t)stream;
+    const uint32_t n = g->d.n;
+    const size_t bytes = (size_t)n * (4 + 8 + 8 + 4) + (BC_MAXL + 1) * 8 + 256;
+    void *buf = analytics_scratch(g, bytes);
+    if (!buf) return GV_ERR_NOMEM;
+    char *p = (char *)buf;
+    BcBufs b;
+    b.bc = nullptr;
+    b.delta = nullptr;
+    b.sigma = (unsigned long long *)p; p += (size_t)n * 8;
+    b.lstart = (unsigned long long *)p; p += (BC_MAXL + 1) * 8;
+    b.qtail = (unsigned long long *)p; p += 8;
+    b.dist = (int32_t *)p; p += (size_t)n * 4;
+    b.queue = (uint32_t *)p; p += (size_t)n * 4;
+    b.active = (int *)p; p += 16;
+    uint32_t *dsrc = (uint32_t *)p;
+    cudaMemcpyAsync(dsrc, &source, 4, cudaMemcpyHostToDevice, s);
+    int *h_active = nullptr;
+    cudaMallocHost(&h_active, 16);
+    uint32_t depth = 0;
+    gv_status st = bfs_batch(g, s, b, dsrc, 1, &depth, h_active);
+    cudaFreeHost(h_active);
+    if (st != GV_OK) return st;
+    const cudaMemcpyKind k = mem == GV_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    cudaError_t e = cudaMemcpyAsync(dist, b.dist, (size_t)n * 4, k, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(sigma, b.sigma, (size_t)n * 8, k, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    return cuda_status(e, "bfs sigma");
+}
+
+gv_status gv_wpr_forward(gv_graph *g, float alpha, float tol, int32_t max_iter, float *x_out, int32_t *sweeps, int mem,
+                         void *stream) {
+    if (!g || !x_out || max_iter < 0) return GV_ERR_INVALID;
+    if (!g->cfg.weighted) { set_error("weighted PageRank needs a weighted store"); return GV_ERR_STATE; }
+    cudaStream_t s = (cudaStream_t)stream;
+    DevGraph d = g->d;
+    const uint32_t n = d.n;
+    uint64_t live = 0;
+    {
+        Ctl c;
+        gv_status st = read_ctl(g, &c, s);
+        if (st != GV_OK) return st;
+        live = c.live_edges;
+    }
+    const uint32_t parts = PULL_GRID + HEAVY_GRID;
+    const size_t bytes = iter_bytes(n, parts) + (size_t)n * 4 * 3 + ((size_t)n + 1) * 8 + (live + 1) * 8 + 512;
+    void *buf = analytics_scratch(g, bytes);
+    if (!buf) return GV_ERR_NOMEM;
+    IterBufs b = carve_iter(buf, n, parts);
+    char *p = (char *)buf + iter_bytes(n, parts);
+    float *rinv = (float *)p; p += (size_t)n * 4;
+    uint32_t *indeg = (uint32_t *)p; p += (size_t)n * 4;
+    uint32_t *cursor = (uint32_t *)p; p += (size_t)n * 4;
+    p = (char *)(((uintptr_t)p + 255) & ~(uintptr_t)255);
+    unsigned long long *toff = (unsigned long long *)p; p += ((size_t)n + 1) * 8;
+    uint32_t *tsrc = (uint32_t *)p; p += (live + 1) * 4;
+    float *tw = (float *)p;
+    GV_LAUNCH(k_row_sums, grid_for(n, 256), 256, 0, s, d, rinv);
+    cudaMemsetAsync(indeg, 0, (size_t)n * 4, s);
+    cudaMemsetAsync(cursor, 0, (size_t)n * 4, s);
+    GV_LAUNCH(k_indeg, grid_for(n, 256), 256, 0, s, d, indeg);
+    scan_exclusive_u32_to_u64(indeg, toff, n, toff + n, g->bs.scan_tmp, s);
+    GV_LAUNCH(k_fill_transpose, grid_for(n, 256), 256, 0, s, d, (const unsigned long long *)toff, cursor, tsrc, tw);
+    GV_LAUNCH(k_fill_f32, grid_for(n, 256), 256, 0, s, b.x0, n, 1.0f / (float)n, GV_NIL, 0.f);
+    cudaMemsetAsync(b.state, 0, 16, s);
+    const uint32_t nparts = PULL_GRID;
+    float *xa = b.x0, *xb = b.x1;
+    int h_state[2] = {0, 0};
+    int launched = 0;
+    PullArgs a{};
+    a.alpha = alpha;
+    a.base_all = (1.0f - alpha) / (float)n;
+    a.base_src = GV_NIL;
+    a.partial = b.partial;
+    a.state = b.state;
+    while (launched < max_iter) {
+        const int chunk = std::min(8, max_iter - launched);
+        for (int i = 0; i < chunk; ++i) {
+            GV_LAUNCH(k_mul, grid_for(n, 256), 256, 0, s, (const float *)xa, (const float *)rinv, b.c0, n);
+            a.gather = b.c0;
+            a.xold = xa;
+            a.xnew = xb;
+            dispatch_tpv(g->cfg.threads_per_vertex, [&](auto t) {
+                constexpr int T = decltype(t)::value;
+                GV_LAUNCH((k_wpr_fwd<T>), PULL_GRID, AN_THREADS, 0, s, n, (const unsigned long long *)toff,
+                          (const uint32_t *)tsrc, (const float *)tw, a);
+            });
+            GV_LAUNCH(k_iter_done, 1, 256, 0, s, b.partial, nparts, tol, b.state, b.res);
+            std::swap(xa, xb);
+        }
+        launched += chunk;
+        cudaError_t e = cudaMemcpyAsync(h_state, b.state, 8, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return cuda_status(e, "wpr forward");
+        if (h_state[0]) break;
+    }
+    if (sweeps) *sweeps = h_state[1];
+    return copy_out_f32((h_state[1] & 1) ? b.x1 : b.x0, x_out, n, mem, s);
+}
+
+gv_status gv_wpr_backward(gv_graph *g, float alpha, float tol, int32_t max_iter, const float *x, const float *c,
+                          int32_t mode, float *grad, uint64_t cap, float *lambda_out, int32_t *sweeps, int mem,
+                          void *stream) {
+    if (!g || !x || !c || max_iter < 0 || (mode != 0 && mode != 1)) return GV_ERR_INVALID;
+    if (!g->cfg.weighted) { set_error("weighted PageRank needs a weighted store"); return GV_ERR_STATE; }
+    cudaStream_t s = (cudaStream_t)stream;
+    DevGraph d = g->d;
+    const uint32_t n = d.n;
+    uint64_t live = 0;
+    {
+        Ctl cc;
+        gv_status st = read_ctl(g, &cc, s);
+        if (st != GV_OK) return st;
+        live = cc.live_edges;
+    }
+    if (grad && cap < live) { set_error("gradient capacity below the number of entries"); return GV_ERR_CAPACITY; }
+    const uint32_t parts = PULL_GRID + HEAVY_GRID;
+    const size_t bytes = iter_bytes(n, parts) + (size_t)n * 4 * 4 + ((size_t)n + 1) * 8 + (live + 1) * 4 + 512;
+    void *buf = analytics_scratch(g, bytes);
+    if (!buf) return GV_ERR_NOMEM;
+    IterBufs b = carve_iter(buf, n, parts);
+    char *p = (char *)buf + iter_bytes(n, parts);
+    float *rinv = (float *)p; p += (size_t)n * 4;
+    float *dx = (float *)p; p += (size_t)n * 4;
+    float *dc = (float *)p; p += (size_t)n * 4;
+    uint32_t *deg = (uint32_t *)p; p += (size_t)n * 4;
+    p = (char *)(((uintptr_t)p + 255) & ~(uintptr_t)255);
+    unsigned long long *off = (unsigned long long *)p; p += ((size_t)n + 1) * 8;
+    float *dgrad = (float *)p;
+    const cudaMemcpyKind kin = mem == GV_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    cudaMemcpyAsync(dx, x, (size_t)n * 4, kin, s);
+    cudaMemcpyAsync(dc, c, (size_t)n * 4, kin, s);
+    GV_LAUNCH(k_row_sums, grid_for(n, 256), 256, 0, s, d, rinv);
+    cudaMemcpyAsync(b.x0, dc, (size_t)n * 4, cudaMemcpyDeviceToDevice, s);  // lambda0 = c
+    PullArgs a{};
+    a.alpha = alpha;
+    a.base_all = 0.f;
+    a.base_src = GV_NIL;
+    a.cvec = dc;
+    a.rscale = rinv;
+    int sw = 0;
+    float *lam = nullptr;
+    gv_status st = run_sweeps(g, s, b, a, true, rinv, tol, max_iter, false, &sw, &lam);
+    if (st != GV_OK) return st;
+    if (sweeps) *sweeps = sw;
+    if (lambda_out) {
+        st = copy_out_f32(lam, lambda_out, n, mem, s);
+        if (st != GV_OK) return st;
+    }
+    if (!grad) return GV_OK;
+    launch_degrees(g, deg, s);
+    scan_exclusive_u32_to_u64(deg, off, n, off + n, g->bs.scan_tmp, s);
+    float *gout = mem == GV_MEM_DEVICE ? grad : dgrad;
+    dispatch_tpv(g->cfg.threads_per_vertex, [&](auto t) {
+        constexpr int T = decltype(t)::value;
+        GV_LAUNCH((k_wpr_grad<T>), grid_for(n, AN_THREADS / T), AN_THREADS, 0, s, d, (const unsigned long long *)off,
+                  (const float *)dx, (const float *)lam, (const float *)dc, (const float *)rinv, alpha, mode, gout);
+    });
+    cudaError_t e = cudaSuccess;
+    if (mem != GV_MEM_DEVICE) e = cudaMemcpyAsync(grad, dgrad, live * 4, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    return cuda_status(e, "wpr gradient");
+}
+
+}  // extern "C"

@@ -1,0 +1,85 @@
+// Host-side definition of a graph and the launch helpers the C ABI calls.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <cuda_runtime.h>
+#include "../../include/gv.h"
+#include "common.cuh"
+
+namespace gv {
+
+// Thresholds between the lane-group path and the CTA-per-vertex path.
+constexpr uint32_t BIG_BLOCKS = 64;    // vertices with more blocks go to a whole CTA
+constexpr uint32_t BIG_SEGMENT = 2048; // batch segments with more entries go to a whole CTA
+constexpr int BIG_THREADS = 512;
+
+struct BatchScratch {
+    uint64_t cap = 0;  // directed entries
+    unsigned long long *keys = nullptr, *keys_alt = nullptr;
+    uint32_t *vals = nullptr, *vals_alt = nullptr;
+    uint32_t *rs_counts = nullptr;
+    void *scan_tmp = nullptr;
+    unsigned long long *tile_cnt = nullptr;  // packed (uniq << 32 | heads) per tile
+    uint32_t *bdst = nullptr;
+    float *bw = nullptr;
+    uint8_t *found = nullptr;
+    uint32_t *seg_vertex = nullptr, *seg_start = nullptr, *seg_found = nullptr;
+    uint32_t *seg_newblocks = nullptr, *seg_blkbase = nullptr, *big_list = nullptr;
+    uint64_t in_cap = 0;  // pairs
+    uint32_t *in_src = nullptr, *in_dst = nullptr;
+    float *in_w = nullptr;
+};
+
+}  // namespace gv
+
+struct gv_graph {
+    gv_config cfg;
+    uint32_t bitsn = 1;
+    gv::DevGraph d{};
+    gv::BatchScratch bs;
+    bool weighted_alloc = false;
+    // lazily allocated analytics scratch
+    void *an_buf = nullptr;
+    size_t an_bytes = 0;
+    void *host_pinned = nullptr;
+    size_t host_pinned_bytes = 0;
+};
+
+namespace gv {
+
+void set_error(const std::string &msg);
+gv_status cuda_status(cudaError_t e, const char *what);
+gv_status ensure_batch_scratch(gv_graph *g, uint64_t entries, uint64_t pairs);
+void *analytics_scratch(gv_graph *g, size_t bytes);
+// Device-to-host copy of the control block (synchronises the stream).
+gv_status read_ctl(gv_graph *g, Ctl *out, cudaStream_t s);
+
+// Update pipeline stages (launch only).
+gv_status run_update(gv_graph *g, const uint32_t *dsrc, const uint32_t *ddst, const float *dw,
+                     uint64_t k, bool symmetric, bool is_delete, cudaStream_t s);
+gv_status run_compact(gv_graph *g, cudaStream_t s);
+gv_status run_export(gv_graph *g, unsigned long long *offsets, uint32_t *dst, float *w,
+                     cudaStream_t s);
+gv_status run_check(gv_graph *g, uint64_t *violations, uint32_t *code, uint32_t *vertex);
+void launch_degrees(gv_graph *g, uint32_t *deg, cudaStream_t s);
+
+template <int T>
+struct Tpv {
+    static constexpr int value = T;
+};
+
+// Calls f(Tpv<t>{}) for the configured threads-per-vertex t.
+template <typename F>
+void dispatch_tpv(uint32_t tpv, F &&f) {
+    switch (tpv) {
+        case 4: f(Tpv<4>{}); break;
+        case 8: f(Tpv<8>{}); break;
+        case 16: f(Tpv<16>{}); break;
+        default: f(Tpv<32>{}); break;
+    }
+}
+
+// Grid size for grid-stride kernels: a few CTAs per SM.
+unsigned grid_for(uint64_t work_items, unsigned per_cta, unsigned max_ctas = 148 * 8);
+
+}  // namespace gv

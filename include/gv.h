@@ -1,0 +1,209 @@
+/*
+ * gv.h — C ABI of libgv, a B200 (sm_100a) dynamic-graph store and the
+ * analytics that traverse it.
+ *
+ * The store is GraphVine's per-vertex edge-block complete binary tree (CBT):
+ * every vertex owns a tree of fixed-size edge blocks; block k of a vertex has
+ * children 2k+1 and 2k+2 and a level-order predecessor k-1.  Blocks come from
+ * one preallocated pool and return to it on compaction.
+ *
+ * Conventions (all entry points):
+ *   - vertex ids are 0-based uint32_t (the reference keeps 1-based ids inside
+ *     edge blocks; the C++ shim in graphvine.hpp converts);
+ *   - every call returns a gv_status and never aborts the process;
+ *   - device work is ordered on the caller's stream (`stream` is a
+ *     cudaStream_t passed as void*, NULL = legacy default stream);
+ *   - `mem` says where an input/output array lives: GV_MEM_HOST (pageable or
+ *     pinned host memory; the call copies through its own staging) or
+ *     GV_MEM_DEVICE (caller-owned device memory);
+ *   - errors found on the device (pool exhausted, vertex id out of range) are
+ *     latched in a device status word; gv_synchronize() waits for the stream
+ *     and returns it.  A batch that would exhaust the pool is rejected as a
+ *     whole and leaves the graph unchanged;
+ *   - a gv_graph is not safe for concurrent use from several host threads
+ *     without external locking.
+ */
+#ifndef GV_H
+#define GV_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct gv_graph gv_graph;
+
+typedef enum gv_status {
+    GV_OK = 0,
+    GV_ERR_INVALID = 1,     /* bad argument: null pointer, bad config, vertex id >= n */
+    GV_ERR_NOMEM = 2,       /* block pool / HBM budget exhausted; graph unchanged      */
+    GV_ERR_CUDA = 3,        /* CUDA runtime error; see gv_last_error_string()          */
+    GV_ERR_TIMEOUT = 4,     /* a bounded device-side wait expired                       */
+    GV_ERR_STATE = 5,       /* call not valid for this graph (e.g. TC on a directed store) */
+    GV_ERR_UNSUPPORTED = 6, /* feature not built into this library                      */
+    GV_ERR_CAPACITY = 7     /* batch larger than the scratch the graph was created with */
+} gv_status;
+
+enum { GV_MEM_HOST = 0, GV_MEM_DEVICE = 1 };
+
+/* Store configuration.  Replaces the reference's compile-time constants
+ * (include/dynamicStructure/constants.cuh:4-19: EDGE_BLOCK_SIZE,
+ * THREADS_PER_BLOCK, DIRECTED) and its "half of device memory" pool sizing
+ * (src/dynamicStructure/graphvine.cu:466-491). */
+typedef struct gv_config {
+    uint32_t num_vertices;       /* n; vertex ids are [0, n)                               */
+    uint32_t block_size;         /* entries per edge block: 32, 64 or 128                  */
+    uint32_t threads_per_vertex; /* lanes that walk one vertex's blocks: 4, 8, 16 or 32    */
+    uint32_t directed;           /* 0: gv_insert_edges/gv_delete_edges apply both (u,v),(v,u) */
+    uint32_t weighted;           /* 1: every entry carries a float weight                  */
+    int32_t device;              /* CUDA device ordinal                                    */
+    uint64_t pool_blocks;        /* block pool capacity; 0 = derive from hbm_budget_bytes  */
+    uint64_t hbm_budget_bytes;   /* bytes for pool + dictionary; 0 = half of free memory   */
+    uint64_t max_batch_pairs;    /* scratch sized for update batches of up to this size    */
+} gv_config;
+
+/* Fills defaults for n vertices: block 128, 8 threads/vertex, undirected,
+ * unweighted, device 0, budget = half of free memory, batches up to 2^22 pairs. */
+gv_status gv_config_init(gv_config *cfg, uint32_t num_vertices);
+
+/* Replaces GraphVine::GraphVine(CSR*) allocation half
+ * (src/dynamicStructure/graphvine.cu:5-35, :38-130). */
+gv_status gv_create(const gv_config *cfg, gv_graph **out);
+/* The reference never frees (include/dynamicStructure/graphvine.cuh:32). */
+gv_status gv_destroy(gv_graph *g);
+
+/* Bulk build from a CSR of directed entries: offsets[n+1] (uint64), dst[m].
+ * Self-loops and duplicates are dropped, every other entry is stored as
+ * given (no symmetrisation).  Replaces GraphVine::bulkBuild
+ * (src/dynamicStructure/graphvine.cu:181-220).  Valid on an empty graph only. */
+gv_status gv_bulk_build_csr(gv_graph *g, const uint64_t *offsets, const uint32_t *dst,
+                            const float *weights, int mem, void *stream);
+
+/* Set-union insert of k pairs (src[i], dst[i]); on an undirected graph both
+ * directions are inserted.  Self-loops and pairs already present are no-ops,
+ * and the first occurrence wins among duplicates in the batch (its weight is
+ * kept).  Replaces GraphVine::batchInsert
+ * (src/dynamicStructure/graphvine.cu:222-371). */
+gv_status gv_insert_edges(gv_graph *g, const uint32_t *src, const uint32_t *dst,
+                          const float *weights, uint64_t k, int mem, void *stream);
+
+/* Set-difference delete of k pairs (both directions on an undirected graph):
+ * matching entries are tombstoned until gv_compact.  Replaces
+ * GraphVine::batchDelete (src/dynamicStructure/graphvine.cu:373-451). */
+gv_status gv_delete_edges(gv_graph *g, const uint32_t *src, const uint32_t *dst,
+                          uint64_t k, int mem, void *stream);
+
+/* Fills tombstone holes, returns emptied tail blocks to the pool and unlinks
+ * them from their CBT parents; the neighbour set is unchanged.  Replaces
+ * GraphVine::compaction (src/dynamicStructure/graphvine.cu:453-464). */
+gv_status gv_compact(gv_graph *g, void *stream);
+
+/* Waits for `stream` and returns (then clears) the latched device status. */
+gv_status gv_synchronize(gv_graph *g, void *stream);
+
+/* Graph facts.  Synchronous. */
+gv_status gv_num_vertices(const gv_graph *g, uint32_t *n);
+gv_status gv_num_edges(gv_graph *g, uint64_t *live_entries);     /* stored directed entries */
+gv_status gv_pool_stats(gv_graph *g, uint64_t *capacity_blocks, uint64_t *free_blocks);
+gv_status gv_get_config(const gv_graph *g, gv_config *cfg);
+
+/* Per-vertex degree (live entries) into deg[n] (uint32). */
+gv_status gv_degrees(gv_graph *g, uint32_t *deg, int mem, void *stream);
+
+/* Snapshot of the live adjacency as CSR, each vertex's entries in storage
+ * order.  offsets[n+1] (uint64), dst[cap], weights[cap] (nullable).
+ * Synchronous; returns GV_ERR_CAPACITY if cap < live entries. */
+gv_status gv_export_csr(gv_graph *g, uint64_t *offsets, uint32_t *dst, float *weights,
+                        uint64_t cap, int mem, void *stream);
+
+/* Vertices touched by updates since the last gv_clear_affected (endpoints of
+ * every inserted or deleted entry, duplicates included).  affected[n] uint8.
+ * Replaces find_affected_nodes (src/dynamicStructure/kernels/insert_kernels.cu:182-198)
+ * and GraphVine::getAffectedNodesPointer (graphvine.cu:501-503). */
+gv_status gv_affected(gv_graph *g, uint8_t *affected, int mem, void *stream);
+gv_status gv_clear_affected(gv_graph *g, void *stream);
+
+/* Structural invariant check on the device: CBT child/predecessor links,
+ * per-block counts, owners, live counts, and that used + free blocks cover
+ * the pool exactly once.  Synchronous.  *violations = 0 on a sound store;
+ * *first_code names the first failed check. */
+gv_status gv_check(gv_graph *g, uint64_t *violations, uint32_t *first_code,
+                   uint32_t *first_vertex);
+
+/* ---- analytics ---------------------------------------------------------- */
+
+/* PageRank: x0 = 1/n; x <- (1-alpha)/n + alpha * sum_{u->v} x_u / deg(u);
+ * stops when sum|x' - x| < epsilon or after max_iter sweeps; no dangling-mass
+ * redistribution.  x_out[n] float.  *sweeps = sweeps performed.  Replaces
+ * static_pagerank (src/algorithm/pagerank/pagerank.cu:3-68,
+ * src/algorithm/pagerank/pr_kernel.cu:3-48).  Synchronous (reads *sweeps). */
+gv_status gv_pagerank(gv_graph *g, float alpha, float epsilon, int32_t max_iter,
+                      float *x_out, int32_t *sweeps, int mem, void *stream);
+
+/* Warm-started PageRank: starts from x_inout (the previous result) instead of
+ * 1/n and converges to the same fixed point.  Replaces dynamic_pagerank
+ * (src/algorithm/pagerank/pagerank.cu:70-132). */
+gv_status gv_pagerank_dynamic(gv_graph *g, float alpha, float epsilon, int32_t max_iter,
+                              float *x_inout, int32_t *sweeps, int mem, void *stream);
+
+/* Personalised PageRank from `source`: x0 = e_s;
+ * x <- (1-alpha) e_s + alpha * sum_{u->v} x_u / deg(u). */
+gv_status gv_ppr(gv_graph *g, uint32_t source, float alpha, float epsilon, int32_t max_iter,
+                 float *x_out, int32_t *sweeps, int mem, void *stream);
+
+/* Exact triangle count on an undirected store.  per_vertex[n] (nullable)
+ * gets t(u) = #triangles {u<v<w} owned by their smallest vertex u, as the
+ * reference counts them (src/algorithm/tc/tc_kernel.cu:3-74) but in uint64;
+ * *total = sum.  Synchronous. */
+gv_status gv_tc(gv_graph *g, uint64_t *per_vertex, uint64_t *total, int mem, void *stream);
+
+/* Incident-triangle counts for a vertex subset: out[i] = #triangles that
+ * contain subset[i].  Synchronous. */
+gv_status gv_tc_subset(gv_graph *g, const uint32_t *subset, uint64_t ns, uint64_t *out,
+                       int mem, void *stream);
+
+/* Betweenness centrality (Brandes): bc[v] = sum over the given sources s != v
+ * of delta_s(v), no halving for undirected graphs (as src/algorithm/bc/bc.cu:42-80
+ * sums).  sources == NULL or ns == 0 means every vertex.  Path counts are
+ * exact uint64, dependencies accumulate in fp64, bc_out[n] is fp32. */
+gv_status gv_bc(gv_graph *g, const uint32_t *sources, uint64_t ns, float *bc_out,
+                int mem, void *stream);
+
+/* Single-source BFS level and exact shortest-path counts (the forward half
+ * of gv_bc): dist[n] int32 (-1 unreachable), sigma[n] uint64. */
+gv_status gv_bfs_sigma(gv_graph *g, uint32_t source, int32_t *dist, uint64_t *sigma,
+                       int mem, void *stream);
+
+/* ---- differentiation: weighted PageRank ----------------------------------
+ * P_uv = w_uv / s_u with s_u = sum_v w_uv (row-normalised stored weights).
+ * forward:  x = (1-alpha)/n + alpha P^T x  (x0 = 1/n, until L1 step < tol)
+ * adjoint:  lambda = c + alpha P lambda    (lambda0 = c)
+ * gradient of J = sum_i c_i x_i:
+ *   mode 0 (raw weights):   dJ/dw_uv = x_u (alpha lambda_v - lambda_u + c_u) / s_u
+ *   mode 1 (normalised P):  dJ/dP_uv = alpha x_u lambda_v
+ * grad[] is aligned with gv_export_csr's entry order.  No reference
+ * counterpart: Edge::weight is commented out in the reference
+ * (include/dynamicStructure/graphStructures.cuh:21). */
+gv_status gv_wpr_forward(gv_graph *g, float alpha, float tol, int32_t max_iter,
+                         float *x_out, int32_t *sweeps, int mem, void *stream);
+gv_status gv_wpr_backward(gv_graph *g, float alpha, float tol, int32_t max_iter,
+                          const float *x, const float *c, int32_t mode,
+                          float *grad, uint64_t cap, float *lambda_out,
+                          int32_t *sweeps, int mem, void *stream);
+
+/* ---- misc --------------------------------------------------------------- */
+
+/* Number of kernels this library has launched in this process. */
+uint64_t gv_kernel_launches(void);
+/* Message for the last failing call on this host thread. */
+const char *gv_last_error_string(void);
+/* Library version string. */
+const char *gv_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GV_H */

@@ -1,0 +1,68 @@
+"""CPU tests of the boundary: libgv loads and exports every entry point that
+include/*.h declares; host-side argument validation needs no GPU."""
+import ctypes as C
+import re
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+DECL = re.compile(r"^\s*(?:gv_status|uint64_t|const\s+char\s*\*)\s*\**\s*(gv_\w+)\s*\(", re.M)
+
+
+def declared_symbols():
+    names = set()
+    for h in (ROOT / "include").glob("*.h"):
+        names.update(DECL.findall(h.read_text()))
+    return sorted(names)
+
+
+def test_headers_declare_entry_points():
+    names = declared_symbols()
+    for must in ("gv_create", "gv_insert_edges", "gv_delete_edges", "gv_compact", "gv_pagerank", "gv_tc", "gv_bc",
+                 "gv_wpr_forward", "gv_wpr_backward"):
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol():
+    from gv_b200 import _lib
+    L = C.CDLL(str(_lib.LIB_PATH))
+    missing = [n for n in declared_symbols() if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def test_python_binding_covers_every_symbol():
+    from gv_b200 import _lib
+    assert set(declared_symbols()) <= set(_lib.SIGNATURES)
+
+
+def test_version_and_launch_counter():
+    import gv_b200
+    assert "sm_100a" in gv_b200.version()
+    assert gv_b200.kernel_launches() >= 0
+
+
+def test_config_validation_without_gpu():
+    import gv_b200
+    from gv_b200 import _lib
+    L = _lib.lib()
+    cfg = _lib.gv_config()
+    assert L.gv_config_init(C.byref(cfg), 100) == 0
+    assert cfg.block_size == 128 and cfg.threads_per_vertex == 8
+    h = C.c_void_p()
+    cfg.block_size = 48
+    assert L.gv_create(C.byref(cfg), C.byref(h)) == _lib.GV_ERR_INVALID
+    cfg.block_size = 128
+    cfg.threads_per_vertex = 6
+    assert L.gv_create(C.byref(cfg), C.byref(h)) == _lib.GV_ERR_INVALID
+    assert L.gv_create(None, C.byref(h)) == _lib.GV_ERR_INVALID
+
+
+def test_no_gpu_fails_loudly():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("GPU present")
+    import gv_b200
+    with pytest.raises(gv_b200.GvError) as e:
+        gv_b200.GraphVine(64)
+    assert "no CUDA device" in str(e.value) or "GV_ERR_CUDA" in str(e.value)

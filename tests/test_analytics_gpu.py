@@ -1,0 +1,207 @@
+"""GPU parity tests of the analytics against the fp64 / exact oracle.
+
+Tolerances (stated per result):
+  PageRank, PPR: fp32 result within 1e-6 L1 of the fp64 oracle run for the
+                 same number of sweeps;
+  TC:            bit-exact per vertex (uint64);
+  BFS sigma:     exact uint64; BC fp32 within 1e-5 max-relative of fp64;
+  weighted PR:   forward within 1e-6 L1; gradient within 1e-4 relative
+                 (scaled by the largest entry) of the fp64 oracle.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from tests.helpers import rmat_graph, sample_existing
+
+gv_b200 = pytest.importorskip("gv_b200")
+pytestmark = pytest.mark.gpu
+
+PR_L1 = 1e-6
+BC_REL = 1e-5
+
+
+@pytest.fixture(scope="module")
+def graph12():
+    scale = 12
+    n = 1 << scale
+    s, d = rmat_graph(scale, 16, seed=21)
+    g = gv_b200.GraphVine(n, threads_per_vertex=8)
+    g.batch_insert(s, d)
+    g.synchronize()
+    o = oracle.OracleGraph(n)
+    o.insert(s, d)
+    return n, g, o
+
+
+def test_pagerank_matches_oracle(graph12):
+    n, g, o = graph12
+    x, sweeps = g.static_pagerank(0.85, 1e-6, 100)
+    xo, so = o.pagerank(0.85, 1e-6, 100, fixed_sweeps=sweeps)
+    err = np.abs(x.astype(np.float64) - xo).sum()
+    print(f"pagerank sweeps={sweeps} oracle_free_sweeps={o.pagerank(0.85, 1e-6, 100)[1]} L1={err:.3e}")
+    assert err < PR_L1
+    assert abs(sweeps - o.pagerank(0.85, 1e-6, 100)[1]) <= 1
+
+
+def test_pagerank_fixed_sweeps_and_tombstones(graph12):
+    n, _, _ = graph12
+    s, d = rmat_graph(12, 16, seed=21)
+    g = gv_b200.GraphVine(n, block_size=32, threads_per_vertex=4)
+    g.batch_insert(s, d)
+    o = oracle.OracleGraph(n)
+    o.insert(s, d)
+    off, dst, _ = o.export()
+    es, ed = sample_existing(off, dst, 3000, np.random.default_rng(4))
+    g.batch_delete(es, ed)  # tombstones stay until compaction; PageRank skips them
+    o.delete(es, ed)
+    g.synchronize()
+    x, sweeps = g.static_pagerank(0.85, 0.0, 20)
+    assert sweeps == 20
+    xo, _ = o.pagerank(0.85, 0.0, 20, fixed_sweeps=20)
+    assert np.abs(x - xo).sum() < PR_L1
+
+
+def test_dynamic_pagerank_reaches_static_fixed_point(graph12):
+    n, _, _ = graph12
+    s, d = rmat_graph(12, 16, seed=21)
+    g = gv_b200.GraphVine(n)
+    g.batch_insert(s, d)
+    x0, sw0 = g.static_pagerank(0.85, 1e-7, 200)
+    ui, vi = gv_b200.gen_uniform(n, 2000, seed=3)
+    g.batch_insert(ui, vi)
+    g.synchronize()
+    xs, sws = g.static_pagerank(0.85, 1e-7, 200)
+    xd, swd = g.dynamic_pagerank(x0, 0.85, 1e-7, 200)
+    print(f"static sweeps={sws} warm-start sweeps={swd} L1(static,dynamic)={np.abs(xs - xd).sum():.3e}")
+    assert swd < sws
+    assert np.abs(xs - xd).sum() < 2e-6
+
+
+def test_ppr_matches_oracle(graph12):
+    n, g, o = graph12
+    src = 5
+    x, sweeps = g.ppr(src, 0.85, 1e-6, 100)
+    xo, _ = o.ppr(src, 0.85, 1e-6, 100, fixed_sweeps=sweeps)
+    assert np.abs(x - xo).sum() < PR_L1
+
+
+@pytest.mark.parametrize("tpv", [4, 16])
+def test_triangle_count_bit_exact(tpv):
+    scale = 12
+    n = 1 << scale
+    s, d = rmat_graph(scale, 16, seed=31)
+    g = gv_b200.GraphVine(n, threads_per_vertex=tpv)
+    g.batch_insert(s, d)
+    o = oracle.OracleGraph(n)
+    o.insert(s, d)
+    pv, tot = g.static_tc()
+    opv, otot = o.tc()
+    assert tot == otot
+    assert np.array_equal(pv, opv)
+    # after deletes (tombstones) and compaction
+    off, dst, _ = o.export()
+    es, ed = sample_existing(off, dst, 5000, np.random.default_rng(7))
+    g.batch_delete(es, ed)
+    o.delete(es, ed)
+    pv, tot = g.static_tc()
+    assert np.array_equal(pv, o.tc()[0])
+    g.compaction()
+    pv, tot = g.static_tc()
+    assert np.array_equal(pv, o.tc()[0])
+
+
+def test_triangle_subset_incident(graph12):
+    n, g, o = graph12
+    sub = np.random.default_rng(1).choice(n, 300, replace=False).astype(np.uint32)
+    assert np.array_equal(g.tc_subset(sub), o.tc_incident(sub))
+
+
+def test_hub_triangles_use_cta_sort():
+    # a 1100-clique: its lowest-ranked member has an oriented list of 1099
+    # entries, above the 1024-entry warp sort, so the CTA sort runs
+    n = 1 << 13
+    K = 1100
+    iu, ju = np.triu_indices(K, 1)
+    perm = np.random.default_rng(5).permutation(n)[:K].astype(np.uint32)
+    rs, rd = rmat_graph(13, 4, seed=8)
+    s = np.concatenate([perm[iu], rs])
+    d = np.concatenate([perm[ju], rd])
+    g = gv_b200.GraphVine(n)
+    g.batch_insert(s, d)
+    o = oracle.OracleGraph(n)
+    o.insert(s, d)
+    pv, tot = g.static_tc()
+    opv, otot = o.tc()
+    assert tot == otot and np.array_equal(pv, opv)
+
+
+def test_bfs_sigma_exact(graph12):
+    n, g, o = graph12
+    for src in (0, 17, 1000):
+        dist, sigma = g.bfs_sigma(src)
+        od, osg = o.bfs_sigma(src)
+        assert np.array_equal(dist, od)
+        assert np.array_equal(sigma, osg)
+
+
+def test_bc_sampled_sources(graph12):
+    n, g, o = graph12
+    src = np.random.default_rng(3).choice(n, 64, replace=False).astype(np.uint32)
+    b = g.bc(src)
+    ob = o.bc(src)
+    rel = np.max(np.abs(b - ob) / np.maximum(np.abs(ob), 1e-300) * (ob != 0))
+    print(f"bc max relative error {rel:.3e}")
+    assert rel < BC_REL
+    assert np.all(b[ob == 0] == 0)
+
+
+def test_bc_all_sources_small():
+    scale = 9
+    n = 1 << scale
+    s, d = rmat_graph(scale, 16, seed=13)
+    g = gv_b200.GraphVine(n)
+    g.batch_insert(s, d)
+    o = oracle.OracleGraph(n)
+    o.insert(s, d)
+    b = g.bc()
+    ob = o.bc()
+    nz = ob != 0
+    assert np.max(np.abs(b[nz] - ob[nz]) / ob[nz]) < BC_REL
+
+
+def _weighted(scale, seed):
+    n = 1 << scale
+    s, d = rmat_graph(scale, 16, seed=seed)
+    rng = np.random.default_rng(seed)
+    w = rng.uniform(0.1, 1.0, len(s)).astype(np.float32)
+    g = gv_b200.GraphVine(n, directed=True, weighted=True)
+    g.batch_insert(s, d, w)
+    o = oracle.OracleGraph(n, directed=True, weighted=True)
+    o.insert(s, d, w)
+    return n, g, o, rng
+
+
+def test_wpr_forward_and_gradient():
+    n, g, o, rng = _weighted(11, 41)
+    x, sw = g.wpr_forward(0.85, 1e-9, 300)
+    xo, _ = o.wpr_forward(0.85)
+    assert np.abs(x - xo).sum() < PR_L1
+    c = rng.standard_normal(n)
+    lo, _ = o.wpr_adjoint(c)
+    for mode in (0, 1):
+        grad, lam, _ = g.wpr_backward(x, c.astype(np.float32), 0.85, 1e-9, 300, mode=mode)
+        go = o.wpr_gradient(xo, lo, c, mode=mode)
+        # align by (u, v): the GPU export order is storage order
+        off, dst, _ = g.export_csr()
+        ooff, odst, _ = o.export()
+        assert np.array_equal(off, ooff)
+        src = np.repeat(np.arange(n), np.diff(off).astype(np.int64))
+        key_g = src.astype(np.uint64) * n + dst
+        key_o = src.astype(np.uint64) * n + odst
+        gg = grad[np.argsort(key_g)]
+        gref = go[np.argsort(key_o)]
+        scale = np.abs(gref).max()
+        err = np.abs(gg - gref).max() / scale
+        print(f"mode {mode}: max |grad - fp64| / max|grad| = {err:.3e}")
+        assert err < 1e-4

@@ -1,0 +1,204 @@
+"""CPU tests: the oracle against independent implementations (networkx,
+scipy) and against the committed golden fixtures; the generator shared by
+libgv and the oracle."""
+import numpy as np
+import pytest
+
+import oracle
+from tests.helpers import rmat_graph
+
+nx = pytest.importorskip("networkx")
+
+
+def _nx_graph(ora, n):
+    off, dst, _ = ora.export()
+    G = nx.Graph()
+    G.add_nodes_from(range(n))
+    for u in range(n):
+        for v in dst[off[u]:off[u + 1]]:
+            G.add_edge(u, int(v))
+    return G
+
+
+@pytest.fixture(scope="module")
+def small():
+    n = 1 << 9
+    s, d = rmat_graph(9, 8, seed=11)
+    g = oracle.OracleGraph(n)
+    g.insert(s, d)
+    return n, g, s, d
+
+
+def test_insert_is_set_union(small):
+    n, g, s, d = small
+    pairs = {(int(a), int(b)) for a, b in zip(s, d) if a != b}
+    want = set()
+    for a, b in pairs:
+        want.add((a, b))
+        want.add((b, a))
+    off, dst, _ = g.export()
+    got = {(u, int(v)) for u in range(n) for v in dst[off[u]:off[u + 1]]}
+    assert got == want
+
+
+def test_delete_is_set_difference(small):
+    n, g0, s, d = small
+    g = oracle.OracleGraph(n)
+    g.insert(s, d)
+    rng = np.random.default_rng(3)
+    k = 200
+    ds, dd = s[:k], d[:k]
+    extra_s = rng.integers(0, n, 50).astype(np.uint32)
+    extra_d = rng.integers(0, n, 50).astype(np.uint32)
+    g.delete(np.concatenate([ds, extra_s]), np.concatenate([dd, extra_d]))
+    off, dst, _ = g.export()
+    got = {(u, int(v)) for u in range(n) for v in dst[off[u]:off[u + 1]]}
+    off0, dst0, _ = g0.export()
+    want = {(u, int(v)) for u in range(n) for v in dst0[off0[u]:off0[u + 1]]}
+    for a, b in zip(np.concatenate([ds, extra_s]), np.concatenate([dd, extra_d])):
+        want.discard((int(a), int(b)))
+        want.discard((int(b), int(a)))
+    assert got == want
+
+
+def test_tc_matches_networkx(small):
+    n, g, _, _ = small
+    pv, tot = g.tc()
+    G = _nx_graph(g, n)
+    assert tot == sum(nx.triangles(G).values()) // 3
+    # owner = smallest vertex of the triangle
+    want = np.zeros(n, np.uint64)
+    for a, b, c in (t for t in nx.enumerate_all_cliques(G) if len(t) == 3):
+        want[min(a, b, c)] += 1
+    assert np.array_equal(pv, want)
+
+
+def test_tc_literal_formula_agrees_on_symmetric_store(small):
+    n, g, s, d = small
+    gd = oracle.OracleGraph(n, directed=True)
+    gd.insert(np.concatenate([s, d]), np.concatenate([d, s]))
+    assert np.array_equal(gd.tc()[0], g.tc()[0])
+
+
+def test_tc_incident_matches_networkx(small):
+    n, g, _, _ = small
+    G = _nx_graph(g, n)
+    sub = np.arange(0, n, 7, dtype=np.uint32)
+    tri = nx.triangles(G)
+    assert np.array_equal(g.tc_incident(sub), np.array([tri[int(u)] for u in sub], np.uint64))
+
+
+def test_bc_matches_networkx(small):
+    n, g, _, _ = small
+    G = _nx_graph(g, n)
+    want = nx.betweenness_centrality(G, normalized=False)
+    got = g.bc()
+    # networkx halves undirected scores; the reference sums over ordered pairs
+    w = np.array([2 * want[i] for i in range(n)])
+    assert np.allclose(got, w, rtol=1e-9, atol=1e-9)
+
+
+def test_bc_subset_sources(small):
+    n, g, _, _ = small
+    G = _nx_graph(g, n)
+    src = [0, 5, 17, 100]
+    want = nx.betweenness_centrality_subset(G, sources=src, targets=list(G.nodes), normalized=False)
+    # subset BC in networkx also halves for undirected graphs
+    got = g.bc(np.array(src, np.uint32))
+    assert np.allclose(got, [2 * want[i] for i in range(n)], rtol=1e-9, atol=1e-9)
+
+
+def test_sigma_counts_shortest_paths(small):
+    n, g, _, _ = small
+    G = _nx_graph(g, n)
+    dist, sigma = g.bfs_sigma(3)
+    sp = nx.single_source_shortest_path_length(G, 3)
+    for v in range(n):
+        assert dist[v] == sp.get(v, -1)
+    for v in list(sp)[:40]:
+        assert sigma[v] == len(list(nx.all_shortest_paths(G, 3, v)))
+
+
+def test_pagerank_matches_scipy_power_iteration(small):
+    sp = pytest.importorskip("scipy.sparse")
+    n, g, _, _ = small
+    off, dst, _ = g.export()
+    deg = np.diff(off).astype(np.float64)
+    rows = np.repeat(np.arange(n), np.diff(off).astype(np.int64))
+    A = sp.csr_matrix((np.ones(len(dst)), (rows, dst.astype(np.int64))), shape=(n, n))
+    inv = np.where(deg > 0, 1.0 / np.maximum(deg, 1), 0.0)
+    x = np.full(n, 1.0 / n)
+    sweeps = 0
+    for _ in range(100):
+        xn = (1 - 0.85) / n + 0.85 * (A.T @ (x * inv))
+        diff = np.abs(xn - x).sum()
+        x = xn
+        sweeps += 1
+        if diff < 1e-6:
+            break
+    got, gs = g.pagerank(0.85, 1e-6, 100)
+    assert gs == sweeps
+    assert np.abs(got - x).sum() < 1e-12
+
+
+def test_wpr_gradient_matches_dense_solve():
+    n = 1 << 7
+    s, d = rmat_graph(7, 4, seed=5)
+    keep = s != d
+    s, d = s[keep], d[keep]
+    rng = np.random.default_rng(9)
+    w = rng.uniform(0.1, 1.0, len(s)).astype(np.float32)
+    g = oracle.OracleGraph(n, directed=True, weighted=True)
+    g.insert(s, d, w)
+    off, dst, wt = g.export()
+    W = np.zeros((n, n))
+    for u in range(n):
+        for v, ww in zip(dst[off[u]:off[u + 1]], wt[off[u]:off[u + 1]]):
+            W[u, v] = ww
+    rs = W.sum(1)
+    Pm = np.divide(W, rs[:, None], out=np.zeros_like(W), where=rs[:, None] > 0)
+    a = 0.85
+    x = np.linalg.solve(np.eye(n) - a * Pm.T, np.full(n, (1 - a) / n))
+    c = rng.standard_normal(n)
+    lam = np.linalg.solve(np.eye(n) - a * Pm, c)
+    gx, _ = g.wpr_forward(a)
+    gl, _ = g.wpr_adjoint(c, a)
+    assert np.allclose(gx, x, atol=1e-13)
+    assert np.allclose(gl, lam, atol=1e-11)
+    grad = g.wpr_gradient(gx, gl, c, a, mode=0)
+    k = 0
+    for u in range(n):
+        for v in dst[off[u]:off[u + 1]]:
+            gP = a * x[u] * lam
+            want = (gP[v] - (Pm[u] * gP).sum()) / rs[u]
+            assert abs(grad[k] - want) <= 1e-10 + 1e-8 * abs(want)
+            k += 1
+
+
+def test_wpr_gradient_matches_finite_differences():
+    n = 1 << 8
+    s, d = rmat_graph(8, 4, seed=6)
+    rng = np.random.default_rng(2)
+    w = rng.uniform(0.1, 1.0, len(s)).astype(np.float32)
+    g = oracle.OracleGraph(n, directed=True, weighted=True)
+    g.insert(s, d, w)
+    off, dst, _ = g.export()
+    c = rng.standard_normal(n)
+    x, _ = g.wpr_forward()
+    lam, _ = g.wpr_adjoint(c)
+    grad = g.wpr_gradient(x, lam, c, mode=0)
+    src = np.repeat(np.arange(n), np.diff(off).astype(np.int64))
+    h = 1e-6
+    for k in rng.choice(len(dst), 16, replace=False):
+        u, v = int(src[k]), int(dst[k])
+        fd = (g.wpr_objective(c, u, v, h) - g.wpr_objective(c, u, v, -h)) / (2 * h)
+        assert abs(fd - grad[k]) <= 1e-7 * max(1.0, abs(grad[k])) + 1e-9, (k, fd, grad[k])
+
+
+def test_generator_is_shared_with_libgv():
+    import gv_b200
+    s1, d1 = oracle.rmat_pairs(12, 5000, 77)
+    s2, d2 = gv_b200.gen_rmat(12, 5000, 77)
+    assert np.array_equal(s1, s2) and np.array_equal(d1, d2)
+    # R-MAT skew: vertex 0 is the densest quadrant corner
+    assert np.bincount(s1, minlength=1 << 12)[0] > 20
