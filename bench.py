@@ -1,0 +1,410 @@
+#!/usr/bin/env python3
+"""Benchmark of the GraphVine dynamic-graph hot path on B200.
+
+Workload (one step = one update batch of the plain method at scale):
+  undirected R-MAT scale 22, edge factor 16, a/b/c/d = 0.57/0.19/0.19/0.05,
+  seeded; each step applies 1M updates (500K inserts of uniform-random new
+  pairs + 500K deletes of existing edges), compacts, then runs PageRank
+  (fp32, alpha 0.85, L1 1e-6, <= 100 sweeps) and an exact triangle count;
+  every 5th step also runs betweenness centrality from 64 seeded sources.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl gv|reference]
+
+Prints one JSON line (rank 0).  `value` = edge updates/s over the timed
+steps with the batches already resident in HBM; `e2e` = the same through the
+C-ABI with pinned host buffers, copies inside the timed region.  For N > 1
+every rank runs an independent replica (the path does not shard).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "edge updates/s & PageRank GTEPS, plain vs batched/served, % of HBM peak"
+ALPHA, EPS, MAX_ITER = 0.85, 1e-6, 100
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["gv", "reference"], default="gv")
+    ap.add_argument("--scale", type=int, default=22)
+    ap.add_argument("--edge-factor", type=int, default=16)
+    ap.add_argument("--batch", type=int, default=1_000_000, help="updates per step (half inserts, half deletes)")
+    ap.add_argument("--bc-every", type=int, default=5)
+    ap.add_argument("--bc-sources", type=int, default=64)
+    ap.add_argument("--block", type=int, default=128)
+    ap.add_argument("--tpv", type=int, default=8)
+    ap.add_argument("--seed", type=int, default=2026)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-clocks", action="store_true")
+    return ap.parse_args()
+
+
+# --------------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict | None:
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 7:
+                continue
+            try:
+                sm.append(float(p[0]))
+                mx.append(float(p[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+# ------------------------------------------------------------------- workload
+def make_batches(n, off, dst, steps, half, seed):
+    """Per step: uniform new pairs to insert, existing undirected edges to delete."""
+    import gv_b200
+    deg = np.diff(off).astype(np.int64)
+    src_of = np.repeat(np.arange(n, dtype=np.uint32), deg)
+    und = np.nonzero(src_of < dst)[0]  # each undirected edge once
+    rng = np.random.default_rng(seed)
+    picks = rng.choice(len(und), size=min(len(und), steps * half), replace=False)
+    out = []
+    for b in range(steps):
+        ins_s, ins_d = gv_b200.gen_uniform(n, half, seed=seed * 1000 + b)
+        sel = und[picks[b * half:(b + 1) * half]]
+        out.append((ins_s, ins_d, src_of[sel].copy(), dst[sel].copy()))
+    return out
+
+
+def bc_sources(n, k, seed):
+    return np.random.default_rng(seed + 7).choice(n, size=k, replace=False).astype(np.uint32)
+
+
+# ----------------------------------------------------------------- CPU legs
+def cpu_sample(args, pairs, batches, n, threads, steps):
+    """Times the oracle (the reference's semantics restated on the CPU) on
+    `steps` steps of the same workload; BC is timed on 4 sources and scaled."""
+    import oracle
+    oracle.set_threads(threads)
+    g = oracle.OracleGraph(n)
+    g.insert(*pairs)
+    src = bc_sources(n, args.bc_sources, args.seed)
+    times = []
+    detail = {}
+    for b in range(steps):
+        ins_s, ins_d, del_s, del_d = batches[b % len(batches)]
+        t0 = time.perf_counter()
+        g.insert(ins_s, ins_d)
+        g.delete(del_s, del_d)
+        t1 = time.perf_counter()
+        g.pagerank(ALPHA, EPS, MAX_ITER)
+        t2 = time.perf_counter()
+        g.tc()
+        t3 = time.perf_counter()
+        g.bc(src[:4])
+        t4 = time.perf_counter()
+        bc_amortised = (t4 - t3) * (args.bc_sources / 4) / args.bc_every
+        times.append((t3 - t0) + bc_amortised)
+        detail = {"update_s": t1 - t0, "pagerank_s": t2 - t1, "tc_s": t3 - t2, "bc_4src_s": t4 - t3}
+    return sum(times) / len(times), detail
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    import gv_b200
+    n = 1 << args.scale
+    pairs = gv_b200.gen_rmat(args.scale, args.edge_factor << args.scale, args.seed)
+    import oracle
+    threads = os.cpu_count() or 1
+    oracle.set_threads(threads)
+    g = oracle.OracleGraph(n)
+    g.insert(*pairs)
+    off, dst, _ = g.export()
+    half = args.batch // 2
+    batches = make_batches(n, off, dst, args.warmup + args.steps, half, args.seed)
+    del g
+    step_s, detail = cpu_sample(args, pairs, batches, n, threads, args.warmup + args.steps)
+    value = args.batch / step_s
+    sample = (f"oracle port (C++/OpenMP, {threads} threads): {args.warmup + args.steps} full steps of the "
+              f"workload (insert+delete+PageRank+TC); BC timed on 4 of {args.bc_sources} sources, scaled "
+              f"and amortised over {args.bc_every} steps")
+    line = {"metric": METRIC, "value": value, "unit": "edge updates/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_s * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded R-MAT, uniform inserts, sampled deletes)",
+            "impl": "reference",
+            "config": workload_config(args, n, int(off[-1])),
+            "cpu_baseline": {"value": value, "unit": "edge updates/s", "cores": threads, "kind": "port",
+                             "sample": sample, "phases_s": detail},
+            "e2e": {"value": value, "unit": "edge updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def workload_config(args, n, m0):
+    return {"workload": (f"plain method at scale: undirected R-MAT scale {args.scale} ef {args.edge_factor}; "
+                         f"per step {args.batch} updates ({args.batch // 2} inserts + {args.batch // 2} deletes) "
+                         f"+ compaction + PageRank + exact TC; BC from {args.bc_sources} sources every "
+                         f"{args.bc_every} steps"),
+            "scale": args.scale, "n": n, "m_initial_entries": m0, "batch_updates": args.batch,
+            "block_size": args.block, "threads_per_vertex": args.tpv,
+            "l2": "working set larger than L2 (adjacency ~0.5 GB vs 126 MB); each step uses fresh batch buffers",
+            "parallelism": "replicas"}
+
+
+# ------------------------------------------------------------------ GPU leg
+def run_gv(args, rank, world, local_rank):
+    import torch
+    import gv_b200
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    n = 1 << args.scale
+    seed = args.seed + rank
+    g = gv_b200.GraphVine(n, block_size=args.block, threads_per_vertex=args.tpv, device=local_rank,
+                          max_batch_pairs=args.batch)
+    s_dev, d_dev = gv_b200.gen_rmat(args.scale, args.edge_factor << args.scale, seed, device=dev)
+    g.batch_insert(s_dev, d_dev)
+    g.synchronize()
+    del s_dev, d_dev
+    torch.cuda.empty_cache()
+    off, dst, _ = g.export_csr()
+    m0 = int(off[-1])
+    half = args.batch // 2
+    total_steps = args.warmup + args.steps + (0 if args.no_e2e else args.steps)
+    batches = make_batches(n, off, dst, total_steps, half, seed)
+    srcs = bc_sources(n, args.bc_sources, seed)
+    dev_batches = [tuple(torch.from_numpy(a.astype(np.int32)).to(dev) for a in b) for b in batches]
+    x_dev = torch.empty(n, dtype=torch.float32, device=dev)
+    bc_dev = torch.empty(n, dtype=torch.float32, device=dev)
+    src_dev = torch.from_numpy(srcs.astype(np.int32)).to(dev)
+
+    stats = {"pr_sweeps": [], "m": [], "tc_work": [], "triangles": []}
+
+    def step(b, inputs, host_out=None):
+        ins_s, ins_d, del_s, del_d = inputs
+        g.batch_insert(ins_s, ins_d)
+        g.batch_delete(del_s, del_d)
+        g.compaction()
+        if host_out is None:
+            _, sw = g.static_pagerank(ALPHA, EPS, MAX_ITER, out=x_dev)
+        else:
+            _, sw = g.static_pagerank(ALPHA, EPS, MAX_ITER, out=host_out["x"])
+        _, tri = g.static_tc(per_vertex=False)
+        stats["pr_sweeps"].append(sw)
+        stats["triangles"].append(tri)
+        if (b % args.bc_every) == args.bc_every - 1:
+            if host_out is None:
+                lib = gv_b200._lib.lib()
+                gv_b200._check(lib.gv_bc(g._h, src_dev.data_ptr(), len(srcs), bc_dev.data_ptr(),
+                                         gv_b200.GV_MEM_DEVICE, 0), "gv_bc")
+            else:
+                host_out["bc"][:] = g.bc(srcs)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # warm-up
+    for b in range(args.warmup):
+        step(b, dev_batches[b])
+    barrier()
+    for k in stats:
+        stats[k].clear()
+    sampler = ClockSampler(local_rank)
+    if not args.no_clocks:
+        sampler.start()
+    gv_b200.profile_reset()
+    gv_b200.profile_enable(True)
+    launches0 = gv_b200.kernel_launches()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    barrier()
+    t_start.record()
+    for i in range(args.steps):
+        b = args.warmup + i
+        step(b, dev_batches[b])
+        stats["m"].append(0)
+    t_end.record()
+    barrier()
+    gv_b200.profile_enable(False)
+    launches = gv_b200.kernel_launches() - launches0
+    clocks = sampler.stop()
+    elapsed_ms = t_start.elapsed_time(t_end)
+    m_now = g.num_edges()
+    try:
+        tc_work = g.last_stat("tc_work")
+    except Exception:
+        tc_work = None
+    prof = {s: gv_b200.profile_query(s) for s in gv_b200.PROFILE_SLOTS}
+
+    # e2e: same steps through the C-ABI with pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        pin = []
+        for b in range(args.warmup + args.steps, total_steps):
+            pin.append(tuple(torch.from_numpy(a.astype(np.uint32).view(np.int32)).pin_memory().numpy().view(np.uint32)
+                             for a in batches[b]))
+        host_out = {"x": torch.empty(n, dtype=torch.float32).pin_memory().numpy(),
+                    "bc": torch.empty(n, dtype=torch.float32).pin_memory().numpy()}
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for i, inputs in enumerate(pin):
+            step(args.warmup + args.steps + i, inputs, host_out)
+        e1.record()
+        barrier()
+        e2e_ms = e0.elapsed_time(e1)
+        n_bc = sum(1 for i in range(len(pin)) if ((args.warmup + args.steps + i) % args.bc_every) == args.bc_every - 1)
+        h2d = args.batch * 8  # (src, dst) uint32 per update
+        d2h = n * 4 + 8 + (n * 4 * n_bc) // max(1, len(pin))
+        e2e = {"ms": e2e_ms, "h2d": h2d, "d2h": d2h}
+
+    # max over ranks
+    t = torch.tensor([elapsed_ms, e2e["ms"] if e2e else 0.0], dtype=torch.float64, device=dev)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    elapsed_ms, e2e_ms = float(t[0]), float(t[1])
+    g.close()
+    if rank != 0:
+        return
+
+    updates = args.batch * args.steps * world
+    value = updates / (elapsed_ms / 1e3)
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    # dominant kernel and its roofline
+    dom = max(prof, key=lambda k: prof[k][0])
+    dom_ms, dom_n = prof[dom]
+    avg_sweeps = sum(stats["pr_sweeps"]) / max(1, len(stats["pr_sweeps"]))
+    alg = None
+    if dom == "pull":
+        alg = 4 * m_now + 12 * n  # neighbour ids + read x, read 1/deg, write x' per sweep
+        unit_note = "4*m + 12*n bytes per sweep"
+    elif dom == "tc_count" and tc_work:
+        alg = 4 * tc_work  # merged list entries, 4 B each
+        unit_note = "4 * sum over oriented edges of (|N+(u)| + |N+(v)|) bytes per launch"
+    roof = None
+    if alg and dom_n:
+        per_launch_s = dom_ms / dom_n / 1e3
+        achieved = alg / per_launch_s / 1e9
+        traffic = None
+        tfile = ROOT / "profiles" / "ncu_traffic.json"
+        if tfile.exists():
+            tj = json.loads(tfile.read_text())
+            if dom in tj and tj[dom].get("bytes_per_unit"):
+                units = m_now if dom == "pull" else tc_work
+                traffic = tj[dom]["bytes_per_unit"] * units
+        roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                "frac": achieved / hbm_peak, "traffic": traffic, "algorithmic_bytes": alg,
+                "avg_launch_ms": dom_ms / dom_n, "launches": dom_n, "peak_source": peak_src,
+                "note": unit_note + f"; fraction of {peak_src} HBM copy bandwidth"}
+    pr_ms = prof["pull"][0]
+    pr_gteps = (m_now * sum(stats["pr_sweeps"])) / (pr_ms / 1e3) / 1e9 if pr_ms else None
+    phases = {k: {"ms_total": v[0], "launches": v[1]} for k, v in prof.items() if v[1]}
+    line = {"metric": METRIC, "value": value, "unit": "edge updates/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic (seeded R-MAT graph, uniform-random inserts, deletes sampled from existing edges)",
+            "config": workload_config(args, n, m0),
+            "pagerank_gteps": pr_gteps, "pagerank_sweeps_avg": avg_sweeps, "m_entries": m_now,
+            "kernel_ms": phases, "roofline": roof, "gpu_launches": launches, "clocks": clocks}
+    if e2e:
+        line["e2e"] = {"value": updates / (e2e_ms / 1e3), "unit": "edge updates/s",
+                       "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"]}
+    if world == 1 and not args.no_cpu_baseline:
+        import gv_b200 as gvb
+        pairs = gvb.gen_rmat(args.scale, args.edge_factor << args.scale, seed)
+        threads = os.cpu_count() or 1
+        step_s, detail = cpu_sample(args, pairs, batches[:1], n, threads, 1)
+        line["cpu_baseline"] = {"value": args.batch / step_s, "unit": "edge updates/s", "cores": threads,
+                                "kind": "port",
+                                "sample": (f"oracle port (C++/OpenMP): 1 full step (1M updates, PageRank, TC) on the "
+                                           f"same graph; BC timed on 4 of {args.bc_sources} sources, scaled and "
+                                           f"amortised over {args.bc_every} steps"),
+                                "phases_s": detail}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        run_gv(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

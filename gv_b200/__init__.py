@@ -68,6 +68,25 @@ def version() -> str:
     return _lib.lib().gv_version().decode()
 
 
+PROFILE_SLOTS = ("radix", "segment", "member", "apply", "compact", "pull", "tc_snapshot", "tc_count",
+                 "bfs_level", "bc_dep")
+
+
+def profile_enable(on: bool = True) -> None:
+    _check(_lib.lib().gv_profile_enable(int(on)), "gv_profile_enable")
+
+
+def profile_reset() -> None:
+    _check(_lib.lib().gv_profile_reset(), "gv_profile_reset")
+
+
+def profile_query(slot: str) -> tuple[float, int]:
+    """(total device ms, launches) recorded for a kernel slot since the last reset."""
+    ms, n = C.c_double(), C.c_uint64()
+    _check(_lib.lib().gv_profile_query(slot.encode(), C.byref(ms), C.byref(n)), "gv_profile_query")
+    return ms.value, n.value
+
+
 def gen_rmat(scale: int, num_pairs: int, seed: int, first: int = 0, device=None, stream=None):
     """R-MAT pairs (src, dst) as numpy arrays, or torch CUDA tensors if device is given."""
     L = _lib.lib()
@@ -208,6 +227,11 @@ class GraphVine:
 
     def clear_affected(self, stream=None) -> None:
         _check(_lib.lib().gv_clear_affected(self._h, _stream(stream)), "gv_clear_affected")
+
+    def last_stat(self, key: str) -> float:
+        v = C.c_double()
+        _check(_lib.lib().gv_last_stat(self._h, key.encode(), C.byref(v)), "gv_last_stat")
+        return v.value
 
     def check(self) -> tuple[int, int, int]:
         v, code, vert = C.c_uint64(), C.c_uint32(), C.c_uint32()

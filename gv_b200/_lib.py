@@ -53,6 +53,7 @@ SIGNATURES = {
     "gv_affected": (C.c_int, [P, P, C.c_int, P]),
     "gv_clear_affected": (C.c_int, [P, P]),
     "gv_check": (C.c_int, [P, pu64, pu32, pu32]),
+    "gv_last_stat": (C.c_int, [P, C.c_char_p, C.POINTER(C.c_double)]),
     "gv_pagerank": (C.c_int, [P, f32, f32, i32, P, pi32, C.c_int, P]),
     "gv_pagerank_dynamic": (C.c_int, [P, f32, f32, i32, P, pi32, C.c_int, P]),
     "gv_ppr": (C.c_int, [P, u32, f32, f32, i32, P, pi32, C.c_int, P]),
@@ -63,6 +64,9 @@ SIGNATURES = {
     "gv_wpr_forward": (C.c_int, [P, f32, f32, i32, P, pi32, C.c_int, P]),
     "gv_wpr_backward": (C.c_int, [P, f32, f32, i32, P, P, i32, P, u64, P, pi32, C.c_int, P]),
     "gv_kernel_launches": (u64, []),
+    "gv_profile_enable": (C.c_int, [i32]),
+    "gv_profile_reset": (C.c_int, []),
+    "gv_profile_query": (C.c_int, [C.c_char_p, C.POINTER(C.c_double), pu64]),
     "gv_last_error_string": (C.c_char_p, []),
     "gv_version": (C.c_char_p, []),
     "gv_gen_rmat": (C.c_int, [u32, u64, u64, u64, P, P, C.c_int, P]),

@@ -22,12 +22,34 @@
 #include "group.cuh"
 #include "prims.cuh"
 #include "launch.hpp"
+#include "prof.hpp"
 
 namespace gv {
 namespace {
 
 constexpr int AN_THREADS = 256;
 constexpr int BIG_TAB_A = 1024;
+// Pull sweeps route vertices by used slots: lane groups up to LIGHT_FILL,
+// one CTA per vertex up to HUB_FILL, the whole grid above.
+constexpr uint32_t LIGHT_FILL = 256;
+constexpr uint32_t HUB_FILL = 16384;
+constexpr int HV_THREADS = 512;
+// BFS levels, BC dependencies and the TC snapshot expand vertices with more
+// used slots than this with every CTA (of their source slot) instead of one
+// lane group.
+constexpr uint32_t BFS_LIGHT_FILL = 2048;
+
+// Lanes per block and blocks per warp step for the grid-cooperative paths.
+struct WarpBlocks {
+    uint32_t lpb, bpw, sub, sl;
+    __device__ __forceinline__ explicit WarpBlocks(uint32_t B) {
+        const uint32_t lane = threadIdx.x & 31u;
+        lpb = min(32u, B >> 2);
+        bpw = 32u / lpb;
+        sub = lane / lpb;
+        sl = lane % lpb;
+    }
+};
 
 // ----------------------------------------------------------- pull sweeps
 // out[v] = base(v) + alpha * scale(v) * sum_{u in N(v)} w(v,u) * gather[u]
@@ -71,7 +93,7 @@ __global__ void __launch_bounds__(AN_THREADS) k_pull(DevGraph g, PullArgs a) {
     for (uint32_t v = blockIdx.x * GPC + threadIdx.x / TPV; v < g.n; v += ngroups) {
         const uint4 rec = g.vtx[v];
         const uint32_t fill = rec.y, nb = blocks_for(fill, g.logB);
-        if (nb > BIG_BLOCKS) continue;  // k_pull_heavy
+        if (fill > LIGHT_FILL) continue;  // chunked items (k_pull_items)
         float sum = 0.f;
         if (nb == 1) {
             const size_t base = (size_t)rec.x << g.logB;
@@ -116,49 +138,100 @@ __global__ void __launch_bounds__(AN_THREADS) k_pull(DevGraph g, PullArgs a) {
     }
 }
 
+// ---------------------------------------------------- chunked work items
+// Vertices above LIGHT_FILL are cut into items of 32 blocks; one warp takes
+// one item, so a hub of a million entries is spread over hundreds of warps
+// and every warp gets about the same work.  Items of a vertex are adjacent
+// and their partials are combined in item order (deterministic).
+struct Items {
+    const uint32_t *item_vertex;  // item -> vertex
+    const uint32_t *item_first;   // vertex -> its first item (n + 1)
+    const uint32_t *multi;        // vertices that have items
+    uint32_t nitems, nmulti;
+};
+
+__global__ void k_item_count(DevGraph g, uint32_t *__restrict__ cnt, uint32_t *__restrict__ multi,
+                             unsigned long long *nmulti) {
+    const uint32_t chunk_log = g.logB + 5;  // 32 blocks per item
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < g.n; v += gridDim.x * blockDim.x) {
+        const uint32_t fill = g.vtx[v].y;
+        uint32_t c = 0;
+        if (fill > LIGHT_FILL) {
+            c = (fill + (1u << chunk_log) - 1) >> chunk_log;
+            multi[atomicAdd(nmulti, 1ull)] = v;
+        }
+        cnt[v] = c;
+    }
+}
+
+__global__ void k_item_fill(uint32_t n, const uint32_t *__restrict__ first, uint32_t *__restrict__ item_vertex) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+        for (uint32_t i = first[v]; i < first[v + 1]; ++i) item_vertex[i] = v;
+}
+
+// Pool index of block (item block base + lane) for the lanes that have one.
+__device__ __forceinline__ uint32_t item_block(const DevGraph &g, uint4 rec, uint32_t kb0, uint32_t nb) {
+    const uint32_t k = kb0 + (threadIdx.x & 31u);
+    if (k >= nb) return GV_NIL;
+    return (k == 0) ? rec.x : cbt_block(g.left, g.right, rec.x, k);
+}
+
 template <bool W>
-__global__ void __launch_bounds__(BIG_THREADS) k_pull_heavy(DevGraph g, PullArgs a, const uint32_t *__restrict__ heavy,
-                                                            uint32_t nheavy, uint32_t part_base) {
-    __shared__ uint32_t tab[BIG_TAB_A];
-    __shared__ float wred[BIG_THREADS / 32];
+__global__ void __launch_bounds__(AN_THREADS) k_pull_items(DevGraph g, PullArgs a, Items it, float *__restrict__ ipart) {
     if (a.state[0]) return;
-    double res = 0.0;
-    for (uint32_t hi = blockIdx.x; hi < nheavy; hi += gridDim.x) {
-        const uint32_t v = heavy[hi];
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t nw = gridDim.x * (AN_THREADS / 32);
+    for (uint32_t i = blockIdx.x * (AN_THREADS / 32) + (threadIdx.x >> 5); i < it.nitems; i += nw) {
+        const uint32_t v = it.item_vertex[i];
+        const uint32_t c = i - it.item_first[v];
         const uint4 rec = g.vtx[v];
         const uint32_t fill = rec.y, nb = blocks_for(fill, g.logB);
+        const uint32_t kb0 = c << 5;
+        const uint32_t my_blk = item_block(g, rec, kb0, nb);
+        const uint32_t e0 = kb0 << g.logB;
+        const uint32_t e1 = min(fill, (kb0 + 32) << g.logB);
+        const uint32_t nq = (e1 - e0 + 3) >> 2;
         float sum = 0.f;
-        for (uint32_t k0 = 0; k0 < nb; k0 += BIG_TAB_A) {
-            const uint32_t kc = min((uint32_t)BIG_TAB_A, nb - k0);
-            fill_block_table(g, rec.x, k0, kc, tab, threadIdx.x, BIG_THREADS);
-            __syncthreads();
-            const uint32_t e0 = k0 << g.logB, e1 = min(fill, (k0 + kc) << g.logB);
-            const uint32_t nq = (e1 - e0 + 3) >> 2;
-            for (uint32_t qi = threadIdx.x; qi < nq; qi += BIG_THREADS) {
-                const uint32_t e = e0 + (qi << 2);
-                const size_t at = ((size_t)tab[(e >> g.logB) - k0] << g.logB) + (e & (g.B - 1));
-                const uint4 q = *reinterpret_cast<const uint4 *>(g.pool + at);
-                float4 wq = make_float4(1.f, 1.f, 1.f, 1.f);
-                if (W) wq = *reinterpret_cast<const float4 *>(g.wpool + at);
-                const uint32_t ev[4] = {q.x, q.y, q.z, q.w};
-                const float wv[4] = {wq.x, wq.y, wq.z, wq.w};
+#pragma unroll 4
+        for (uint32_t q0 = 0; q0 < nq; q0 += 32) {  // warp-uniform trip count
+            const uint32_t q = q0 + lane;
+            const uint32_t el = q << 2;  // entry offset within the item
+            const uint32_t pb = __shfl_sync(GV_FULL_MASK, my_blk, (el >> g.logB) & 31u);
+            if (q >= nq) continue;
+            const size_t at = ((size_t)pb << g.logB) + (el & (g.B - 1));
+            const uint4 qv = *reinterpret_cast<const uint4 *>(g.pool + at);
+            float4 wq = make_float4(1.f, 1.f, 1.f, 1.f);
+            if (W) wq = *reinterpret_cast<const float4 *>(g.wpool + at);
+            const uint32_t ev[4] = {qv.x, qv.y, qv.z, qv.w};
+            const float wv[4] = {wq.x, wq.y, wq.z, wq.w};
 #pragma unroll
-                for (int j = 0; j < 4; ++j)
-                    if (e + j < fill && ev[j] != GV_TOMB) sum += W ? wv[j] * __ldg(a.gather + ev[j]) : __ldg(a.gather + ev[j]);
-            }
-            __syncthreads();
+            for (int j = 0; j < 4; ++j)
+                if (e0 + el + j < e1 && ev[j] != GV_TOMB) sum += W ? wv[j] * __ldg(a.gather + ev[j]) : __ldg(a.gather + ev[j]);
         }
         sum = warp_sum(sum);
-        if ((threadIdx.x & 31) == 0) wred[threadIdx.x >> 5] = sum;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            float t = 0.f;
-            for (int i = 0; i < BIG_THREADS / 32; ++i) t += wred[i];
-            pull_finish(a, v, t, rec.z, res);
-        }
-        __syncthreads();
+        if (lane == 0) ipart[i] = sum;
     }
-    if (threadIdx.x == 0) a.partial[part_base + blockIdx.x] = res;
+}
+
+__global__ void __launch_bounds__(AN_THREADS) k_pull_items_fin(DevGraph g, PullArgs a, Items it,
+                                                               const float *__restrict__ ipart, uint32_t part_base) {
+    __shared__ double red[AN_THREADS / 32];
+    if (a.state[0]) return;
+    double res = 0.0;
+    for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < it.nmulti; m += gridDim.x * blockDim.x) {
+        const uint32_t v = it.multi[m];
+        float t = 0.f;
+        for (uint32_t i = it.item_first[v]; i < it.item_first[v + 1]; ++i) t += ipart[i];
+        pull_finish(a, v, t, g.vtx[v].z, res);
+    }
+    res = warp_sum(res);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = res;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int i = 0; i < AN_THREADS / 32; ++i) s += red[i];
+        a.partial[part_base + blockIdx.x] = s;
+    }
 }
 
 // Sums the per-CTA residuals in a fixed order; latches convergence.
@@ -177,13 +250,6 @@ __global__ void k_iter_done(const double *__restrict__ partial, uint32_t nparts,
         *last_res = s;
         state[1] += 1;
         if (s < (double)eps) state[0] = 1;
-    }
-}
-
-__global__ void k_heavy_list(DevGraph g, uint32_t *list, unsigned long long *cnt) {
-    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < g.n; v += gridDim.x * blockDim.x) {
-        const uint32_t nb = blocks_for(g.vtx[v].y, g.logB);
-        if (nb > BIG_BLOCKS) list[atomicAdd(cnt, 1ull)] = v;
     }
 }
 
@@ -211,11 +277,12 @@ struct IterBufs {
     int *state;  // [0] done, [1] sweeps
     double *res;
     uint32_t *heavy;
-    unsigned long long *nheavy;
+    unsigned long long *nheavy;  // [0] medium count, [1] hub count
+    uint32_t *hubs;
 };
 
 size_t iter_bytes(uint32_t n, uint32_t parts) {
-    return (size_t)n * 4 * 4 + (size_t)parts * 8 + 64 + (size_t)n * 4 + 64;
+    return (size_t)n * 4 * 4 + (size_t)parts * 8 + 64 + (size_t)n * 4 * 2 + 64;
 }
 
 IterBufs carve_iter(void *base, uint32_t n, uint32_t parts) {
@@ -229,12 +296,49 @@ IterBufs carve_iter(void *base, uint32_t n, uint32_t parts) {
     b.state = (int *)p; p += 16;
     b.res = (double *)p; p += 16;
     b.nheavy = (unsigned long long *)p; p += 32;
-    b.heavy = (uint32_t *)p;
+    b.heavy = (uint32_t *)p; p += (size_t)n * 4;
+    b.hubs = (uint32_t *)p;
     return b;
 }
 
 constexpr unsigned PULL_GRID = 148 * 8;
-constexpr unsigned HEAVY_GRID = 148;
+constexpr unsigned HUB_GRID = 148 * 2;
+constexpr unsigned FIN_GRID = 148;
+constexpr unsigned SWEEP_PARTS = PULL_GRID + FIN_GRID;
+
+// Builds the chunked item list of the current graph (aux scratch slots 1, 2);
+// *ipart gets one 4-byte slot per item.
+gv_status build_items(gv_graph *g, cudaStream_t s, unsigned long long *nmulti, Items *it, float **ipart) {
+    DevGraph d = g->d;
+    const uint32_t n = d.n;
+    uint32_t *first = (uint32_t *)aux_scratch(g, 1, ((size_t)n + 1) * 4 * 2 + 64);
+    if (!first) return GV_ERR_NOMEM;
+    uint32_t *multi = first + (n + 1);
+    cudaMemsetAsync(nmulti, 0, 8, s);
+    GV_LAUNCH(k_item_count, grid_for(n, 256), 256, 0, s, d, first, multi, nmulti);
+    scan_exclusive_u32(first, first, n, first + n, g->bs.scan_tmp, s);
+    uint32_t nitems = 0;
+    unsigned long long nm = 0;
+    cudaMemcpyAsync(&nitems, first + n, 4, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(&nm, nmulti, 8, cudaMemcpyDeviceToHost, s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_status(e, "items");
+    uint32_t *item_vertex = nullptr;
+    float *ip = nullptr;
+    if (nitems) {
+        item_vertex = (uint32_t *)aux_scratch(g, 2, (size_t)nitems * 8);
+        if (!item_vertex) return GV_ERR_NOMEM;
+        ip = (float *)(item_vertex + nitems);
+        GV_LAUNCH(k_item_fill, grid_for(n, 256), 256, 0, s, n, (const uint32_t *)first, item_vertex);
+    }
+    it->item_vertex = item_vertex;
+    it->item_first = first;
+    it->multi = multi;
+    it->nitems = nitems;
+    it->nmulti = (uint32_t)nm;
+    *ipart = ip;
+    return GV_OK;
+}
 
 // Runs pull sweeps until convergence or max_iter.  Result in *result (one of
 // x0/x1).  `weighted_rscale` non-null selects the weighted gather (adjoint).
@@ -242,14 +346,13 @@ gv_status run_sweeps(gv_graph *g, cudaStream_t s, IterBufs &b, PullArgs proto, b
                      const float *weighted_rscale, float eps, int max_iter, bool contrib_pr,
                      int *sweeps_out, float **result) {
     DevGraph d = g->d;
-    cudaMemsetAsync(b.nheavy, 0, 8, s);
-    GV_LAUNCH(k_heavy_list, grid_for(d.n, 256), 256, 0, s, d, b.heavy, b.nheavy);
-    unsigned long long nheavy = 0;
-    cudaMemcpyAsync(&nheavy, b.nheavy, 8, cudaMemcpyDeviceToHost, s);
+    Items it{};
+    float *ipart = nullptr;
+    gv_status st = build_items(g, s, b.nheavy, &it, &ipart);
+    if (st != GV_OK) return st;
     cudaMemsetAsync(b.state, 0, 16, s);
-    cudaError_t e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) return cuda_status(e, "sweeps");
-    const uint32_t nparts = PULL_GRID + HEAVY_GRID;
+    cudaError_t e = cudaSuccess;
+    const uint32_t nparts = SWEEP_PARTS;
     cudaMemsetAsync(b.partial, 0, (size_t)nparts * 8, s);
     int h_state[2] = {0, 0};
     float *xa = b.x0, *xb = b.x1, *ca = b.c0, *cb = b.c1;
@@ -265,14 +368,16 @@ gv_status run_sweeps(gv_graph *g, cudaStream_t s, IterBufs &b, PullArgs proto, b
             a.partial = b.partial;
             a.state = b.state;
             if (!contrib_pr && !weighted) a.gather = ca;
+            ProfScope ps(PROF_PULL, s);
             dispatch_tpv(g->cfg.threads_per_vertex, [&](auto t) {
                 constexpr int T = decltype(t)::value;
                 if (weighted) GV_LAUNCH((k_pull<T, true>), PULL_GRID, AN_THREADS, 0, s, d, a);
                 else GV_LAUNCH((k_pull<T, false>), PULL_GRID, AN_THREADS, 0, s, d, a);
             });
-            if (nheavy) {
-                if (weighted) GV_LAUNCH(k_pull_heavy<true>, HEAVY_GRID, BIG_THREADS, 0, s, d, a, b.heavy, (uint32_t)nheavy, PULL_GRID);
-                else GV_LAUNCH(k_pull_heavy<false>, HEAVY_GRID, BIG_THREADS, 0, s, d, a, b.heavy, (uint32_t)nheavy, PULL_GRID);
+            if (it.nitems) {
+                if (weighted) GV_LAUNCH(k_pull_items<true>, PULL_GRID, AN_THREADS, 0, s, d, a, it, ipart);
+                else GV_LAUNCH(k_pull_items<false>, PULL_GRID, AN_THREADS, 0, s, d, a, it, ipart);
+                GV_LAUNCH(k_pull_items_fin, FIN_GRID, AN_THREADS, 0, s, d, a, it, (const float *)ipart, PULL_GRID);
             }
             GV_LAUNCH(k_iter_done, 1, 256, 0, s, b.partial, nparts, eps, b.state, b.res);
             std::swap(xa, xb);
@@ -302,7 +407,7 @@ gv_status pagerank_impl(gv_graph *g, float alpha, float eps, int max_iter, const
                         uint32_t source, float *x_out, int32_t *sweeps, int mem, cudaStream_t s) {
     const uint32_t n = g->d.n;
     if (g->cfg.directed) { set_error("PageRank pull needs an undirected (symmetric) store"); return GV_ERR_STATE; }
-    const uint32_t parts = PULL_GRID + HEAVY_GRID;
+    const uint32_t parts = SWEEP_PARTS;
     void *buf = analytics_scratch(g, iter_bytes(n, parts));
     if (!buf) return GV_ERR_NOMEM;
     IterBufs b = carve_iter(buf, n, parts);
@@ -331,6 +436,7 @@ gv_status pagerank_impl(gv_graph *g, float alpha, float eps, int max_iter, const
     float *res = nullptr;
     gv_status st = run_sweeps(g, s, b, a, false, nullptr, eps, max_iter, true, &sw, &res);
     if (st != GV_OK) return st;
+    g->last_sweeps = sw;
     if (sweeps) *sweeps = sw;
     return copy_out_f32(res, x_out, n, mem, s);
 }
@@ -341,8 +447,11 @@ __device__ __forceinline__ bool rank_less(uint32_t du, uint32_t u, uint32_t dv, 
     return du < dv || (du == dv && u < v);
 }
 
+// Light vertices (fill <= LIGHT_FILL) count their oriented out-degree with
+// a lane group; heavier vertices go through the chunked items.
 template <int TPV>
-__global__ void __launch_bounds__(AN_THREADS) k_tc_outdeg(DevGraph g, uint32_t *__restrict__ dplus) {
+__global__ void __launch_bounds__(AN_THREADS) k_tc_outdeg(DevGraph g, const uint32_t *__restrict__ deg,
+                                                          uint32_t *__restrict__ dplus) {
     constexpr int GPC = AN_THREADS / TPV;
     __shared__ uint32_t tabs[GPC][BIG_BLOCKS];
     Group<TPV> G;
@@ -351,27 +460,104 @@ __global__ void __launch_bounds__(AN_THREADS) k_tc_outdeg(DevGraph g, uint32_t *
     for (uint32_t u = blockIdx.x * GPC + threadIdx.x / TPV; u < g.n; u += ngroups) {
         const uint4 rec = g.vtx[u];
         const uint32_t fill = rec.y, nb = blocks_for(fill, g.logB), du = rec.z;
+        if (fill > LIGHT_FILL) continue;  // k_tc_items / k_tc_multi
+        fill_block_table(g, rec.x, 0, nb, tab, G.gl, TPV);
+        G.sync();
         uint32_t c = 0;
-        for (uint32_t k0 = 0; k0 < nb; k0 += BIG_BLOCKS) {
-            const uint32_t kc = min((uint32_t)BIG_BLOCKS, nb - k0);
-            fill_block_table(g, rec.x, k0, kc, tab, G.gl, TPV);
-            G.sync();
-            const uint32_t e0 = k0 << g.logB, e1 = min(fill, (k0 + kc) << g.logB);
-            for (uint32_t e = e0 + G.gl; e < e1; e += TPV) {
-                const uint32_t v = g.pool[((size_t)tab[(e >> g.logB) - k0] << g.logB) + (e & (g.B - 1))];
-                if (v != GV_TOMB && rank_less(du, u, g.vtx[v].z, v)) ++c;
-            }
-            G.sync();
+        for (uint32_t e = G.gl; e < fill; e += TPV) {
+            const uint32_t v = g.pool[((size_t)tab[e >> g.logB] << g.logB) + (e & (g.B - 1))];
+            if (v != GV_TOMB && rank_less(du, u, __ldg(deg + v), v)) ++c;
         }
+        G.sync();
         c = G.sum(c);
         if (G.gl == 0) dplus[u] = c;
     }
 }
 
+// One warp per item of a heavy vertex.  WRITE = false counts the item's
+// oriented entries into icnt; WRITE = true writes them at off[u] + ioff[item].
+template <bool WRITE>
+__global__ void __launch_bounds__(AN_THREADS) k_tc_items(DevGraph g, const uint32_t *__restrict__ deg, Items it,
+                                                         uint32_t *__restrict__ icnt, const uint32_t *__restrict__ ioff,
+                                                         const unsigned long long *__restrict__ off,
+                                                         uint32_t *__restrict__ snap) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t nw = gridDim.x * (AN_THREADS / 32);
+    for (uint32_t i = blockIdx.x * (AN_THREADS / 32) + (threadIdx.x >> 5); i < it.nitems; i += nw) {
+        const uint32_t u = it.item_vertex[i];
+        const uint32_t c = i - it.item_first[u];
+        const uint4 rec = g.vtx[u];
+        const uint32_t fill = rec.y, nb = blocks_for(fill, g.logB), du = rec.z;
+        const uint32_t kb0 = c << 5;
+        const uint32_t my_blk = item_block(g, rec, kb0, nb);
+        const uint32_t e0 = kb0 << g.logB;
+        const uint32_t e1 = min(fill, (kb0 + 32) << g.logB);
+        const uint32_t nq = (e1 - e0 + 3) >> 2;
+        unsigned long long w = WRITE ? off[u] + ioff[i] : 0ull;
+        const unsigned long long wend = WRITE ? off[u + 1] : 0ull;
+        uint32_t total = 0;
+        for (uint32_t q0 = 0; q0 < nq; q0 += 32) {
+            const uint32_t q = q0 + lane;
+            const uint32_t el = q << 2;
+            const uint32_t pb = __shfl_sync(GV_FULL_MASK, my_blk, (el >> g.logB) & 31u);
+            uint32_t ev[4] = {GV_TOMB, GV_TOMB, GV_TOMB, GV_TOMB};
+            uint32_t k = 0;
+            if (q < nq) {
+                const uint4 qv = *reinterpret_cast<const uint4 *>(g.pool + ((size_t)pb << g.logB) + (el & (g.B - 1)));
+                ev[0] = qv.x; ev[1] = qv.y; ev[2] = qv.z; ev[3] = qv.w;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    if (e0 + el + j >= e1 || ev[j] == GV_TOMB || !rank_less(du, u, __ldg(deg + ev[j]), ev[j]))
+                        ev[j] = GV_TOMB;
+                    else
+                        ++k;
+                }
+            }
+            if (WRITE) {
+                uint32_t incl = k;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t t = __shfl_up_sync(GV_FULL_MASK, incl, o);
+                    if (lane >= (uint32_t)o) incl += t;
+                }
+                unsigned long long p = w + (incl - k);
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    if (ev[j] != GV_TOMB) {
+                        if (p < wend) snap[p] = ev[j];
+                        ++p;
+                    }
+                w += __shfl_sync(GV_FULL_MASK, incl, 31);
+            } else {
+                total += k;
+            }
+        }
+        if (!WRITE) {
+            total = warp_sum(total);
+            if (lane == 0) icnt[i] = total;
+        }
+    }
+}
+
+// Heavy vertices: dplus = sum of their items' counts; ioff = item prefix.
+__global__ void k_tc_multi(Items it, const uint32_t *__restrict__ icnt, uint32_t *__restrict__ ioff,
+                           uint32_t *__restrict__ dplus) {
+    for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < it.nmulti; m += gridDim.x * blockDim.x) {
+        const uint32_t v = it.multi[m];
+        uint32_t run = 0;
+        for (uint32_t i = it.item_first[v]; i < it.item_first[v + 1]; ++i) {
+            ioff[i] = run;
+            run += icnt[i];
+        }
+        dplus[v] = run;
+    }
+}
+
+// Light vertices write their oriented lists in storage order.
 template <int TPV>
-__global__ void __launch_bounds__(AN_THREADS) k_tc_write(DevGraph g, const unsigned long long *__restrict__ off,
-                                                         uint32_t *__restrict__ snap, uint32_t *__restrict__ mid_list,
-                                                         uint32_t *__restrict__ big_list, unsigned long long *cnts) {
+__global__ void __launch_bounds__(AN_THREADS) k_tc_write(DevGraph g, const uint32_t *__restrict__ deg,
+                                                         const unsigned long long *__restrict__ off,
+                                                         uint32_t *__restrict__ snap) {
     constexpr int GPC = AN_THREADS / TPV;
     __shared__ uint32_t tabs[GPC][BIG_BLOCKS];
     Group<TPV> G;
@@ -380,43 +566,42 @@ __global__ void __launch_bounds__(AN_THREADS) k_tc_write(DevGraph g, const unsig
     for (uint32_t u = blockIdx.x * GPC + threadIdx.x / TPV; u < g.n; u += ngroups) {
         const uint4 rec = g.vtx[u];
         const uint32_t fill = rec.y, nb = blocks_for(fill, g.logB), du = rec.z;
+        if (fill > LIGHT_FILL) continue;  // k_tc_items<true>
         unsigned long long w = off[u];
         const unsigned long long wend = off[u + 1];
-        const uint32_t len = (uint32_t)(wend - w);
-        for (uint32_t k0 = 0; k0 < nb; k0 += BIG_BLOCKS) {
-            const uint32_t kc = min((uint32_t)BIG_BLOCKS, nb - k0);
-            fill_block_table(g, rec.x, k0, kc, tab, G.gl, TPV);
-            G.sync();
-            const uint32_t e0 = k0 << g.logB, e1 = min(fill, (k0 + kc) << g.logB);
-            for (uint32_t c0 = e0; c0 < e1; c0 += TPV) {
-                const uint32_t e = c0 + G.gl;
-                uint32_t v = GV_TOMB;
-                if (e < e1) v = g.pool[((size_t)tab[(e >> g.logB) - k0] << g.logB) + (e & (g.B - 1))];
-                const uint32_t keep = (v != GV_TOMB && rank_less(du, u, g.vtx[v].z, v)) ? 1u : 0u;
-                uint32_t tot;
-                const uint32_t pre = G.excl_scan(keep, tot);
-                if (keep && w + pre < wend) snap[w + pre] = v;
-                w += tot;
-            }
-            G.sync();
-        }
-        if (G.gl == 0 && len > 16) {
-            if (len <= 1024) mid_list[atomicAdd(&cnts[0], 1ull)] = u;
-            else big_list[atomicAdd(&cnts[1], 1ull)] = u;
-        }
-        if (len > 1 && len <= 16) {
-            // tiny lists: one lane sorts (insertion sort)
-            if (G.gl == 0) {
-                uint32_t *a = snap + off[u];
-                for (uint32_t i = 1; i < len; ++i) {
-                    const uint32_t x = a[i];
-                    uint32_t j = i;
-                    while (j > 0 && a[j - 1] > x) { a[j] = a[j - 1]; --j; }
-                    a[j] = x;
-                }
-            }
+        fill_block_table(g, rec.x, 0, nb, tab, G.gl, TPV);
+        G.sync();
+        for (uint32_t c0 = 0; c0 < fill; c0 += TPV) {
+            const uint32_t e = c0 + G.gl;
+            uint32_t v = GV_TOMB;
+            if (e < fill) v = g.pool[((size_t)tab[e >> g.logB] << g.logB) + (e & (g.B - 1))];
+            const uint32_t keep = (v != GV_TOMB && rank_less(du, u, __ldg(deg + v), v)) ? 1u : 0u;
+            uint32_t tot;
+            const uint32_t pre = G.excl_scan(keep, tot);
+            if (keep && w + pre < wend) snap[w + pre] = v;
+            w += tot;
         }
         G.sync();
+    }
+}
+
+// Sorts tiny lists in place (one thread) and routes the rest to the sorts.
+__global__ void k_tc_classify(const unsigned long long *__restrict__ off, uint32_t n, uint32_t *__restrict__ snap,
+                              uint32_t *__restrict__ mid_list, uint32_t *__restrict__ big_list,
+                              unsigned long long *cnts) {
+    for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x) {
+        const uint32_t len = (uint32_t)(off[u + 1] - off[u]);
+        if (len > 1024) big_list[atomicAdd(&cnts[1], 1ull)] = u;
+        else if (len > 16) mid_list[atomicAdd(&cnts[0], 1ull)] = u;
+        else if (len > 1) {
+            uint32_t *a = snap + off[u];
+            for (uint32_t i = 1; i < len; ++i) {
+                const uint32_t x = a[i];
+                uint32_t j = i;
+                while (j > 0 && a[j - 1] > x) { a[j] = a[j - 1]; --j; }
+                a[j] = x;
+            }
+        }
     }
 }
 
@@ -491,49 +676,329 @@ template <int TPV, bool INCIDENT>
 __global__ void __launch_bounds__(AN_THREADS) k_tc_count(const unsigned long long *__restrict__ off,
                                                          const uint32_t *__restrict__ snap,
                                                          const uint32_t *__restrict__ esrc, uint64_t m_plus,
-                                                         unsigned long long *__restrict__ tcount) {
+                                                         unsigned long long *__restrict__ tcount,
+                                                         unsigned long long *__restrict__ work) {
     constexpr int GPC = AN_THREADS / TPV;
+    constexpr uint32_t HT = 2048;  // per-CTA credit table: hubs collect many credits
+    __shared__ unsigned long long wred[AN_THREADS / 32];
+    __shared__ uint32_t ht_key[HT];
+    __shared__ unsigned long long ht_val[HT];
+    for (uint32_t i = threadIdx.x; i < HT; i += blockDim.x) {
+        ht_key[i] = GV_NIL;
+        ht_val[i] = 0;
+    }
+    __syncthreads();
+    auto add = [&](uint32_t key, unsigned long long amount) {
+        uint32_t h = (key * 2654435761u) & (HT - 1);
+        for (int probe = 0; probe < 8; ++probe) {
+            uint32_t k = ht_key[h];
+            if (k == GV_NIL) k = atomicCAS(&ht_key[h], GV_NIL, key);
+            if (k == GV_NIL || k == key) {
+                atomicAdd(&ht_val[h], amount);
+                return;
+            }
+            h = (h + 1) & (HT - 1);
+        }
+        atomicAdd(&tcount[key], amount);
+    };
     Group<TPV> G;
     const uint64_t ngroups = (uint64_t)gridDim.x * GPC;
+    unsigned long long my_work = 0;  // list entries this group touched
     for (uint64_t ei = (uint64_t)blockIdx.x * GPC + threadIdx.x / TPV; ei < m_plus; ei += ngroups) {
         const uint32_t u = esrc[ei], v = snap[ei];
         const uint32_t *A = snap + off[u];
         const uint32_t la = (uint32_t)(off[u + 1] - off[u]);
         const uint32_t *Bv = snap + off[v];
         const uint32_t lb = (uint32_t)(off[v + 1] - off[v]);
-        const uint32_t tot = la + lb;
-        const uint32_t per = (tot + TPV - 1) / TPV;
-        const uint32_t d0 = min(tot, G.gl * per), d1 = min(tot, d0 + per);
-        uint32_t i = corank(A, la, Bv, lb, d0), j = d0 - i;
+        const uint32_t small = min(la, lb), large = max(la, lb);
+        if (small == 0) continue;  // group-uniform
         uint32_t cu = 0, cv = 0;
         const uint32_t uv_min = min(u, v);
-        for (uint32_t d = d0; d < d1; ++d) {
-            if (i < la && (j >= lb || A[i] <= Bv[j])) {
-                const uint32_t w = A[i];
-                if (j < lb && Bv[j] == w) {
-                    if (INCIDENT) {
-                        ++cu; ++cv;
-                        atomicAdd(&tcount[w], 1ull);
-                    } else if (w < uv_min) {
-                        atomicAdd(&tcount[w], 1ull);
-                    } else if (u < v) {
-                        ++cu;
-                    } else {
-                        ++cv;
-                    }
-                }
-                ++i;
+        auto credit = [&](uint32_t w) {
+            if (INCIDENT) {
+                ++cu; ++cv;
+                add(w, 1ull);
+            } else if (w < uv_min) {
+                add(w, 1ull);
+            } else if (u < v) {
+                ++cu;
             } else {
-                ++j;
+                ++cv;
             }
+        };
+        const uint32_t lg = 32 - __clz(large);
+        uint32_t touched;
+        if ((uint64_t)small * (lg + 1) < (uint64_t)la + lb) {
+            // skewed pair: binary-search each entry of the short list in the long one
+            const bool a_small = la <= lb;
+            const uint32_t *S = a_small ? A : Bv, *L = a_small ? Bv : A;
+            for (uint32_t i = G.gl; i < small; i += TPV) {
+                const uint32_t w = S[i];
+                const uint32_t pos = lower_bound_u32(L, large, w);
+                if (pos < large && L[pos] == w) credit(w);
+            }
+            touched = small * (lg + 1);
+        } else {
+            // balanced pair: merge path, one diagonal range per lane
+            const uint32_t tot = la + lb;
+            const uint32_t per = (tot + TPV - 1) / TPV;
+            const uint32_t d0 = min(tot, G.gl * per), d1 = min(tot, d0 + per);
+            uint32_t i = corank(A, la, Bv, lb, d0), j = d0 - i;
+            for (uint32_t d = d0; d < d1; ++d) {
+                if (i < la && (j >= lb || A[i] <= Bv[j])) {
+                    if (j < lb && Bv[j] == A[i]) credit(A[i]);
+                    ++i;
+                } else {
+                    ++j;
+                }
+            }
+            touched = tot;
         }
         cu = G.sum(cu);
         cv = G.sum(cv);
         if (G.gl == 0) {
-            if (cu) atomicAdd(&tcount[u], (unsigned long long)cu);
-            if (cv) atomicAdd(&tcount[v], (unsigned long long)cv);
+            if (cu) add(u, cu);
+            if (cv) add(v, cv);
+            my_work += touched;
         }
     }
+    my_work = warp_sum(my_work);
+    if ((threadIdx.x & 31) == 0) wred[threadIdx.x >> 5] = my_work;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long t = 0;
+        for (int i = 0; i < AN_THREADS / 32; ++i) t += wred[i];
+        if (t) atomicAdd(work, t);
+    }
+    for (uint32_t i = threadIdx.x; i < HT; i += blockDim.x)
+        if (ht_key[i] != GV_NIL && ht_val[i]) atomicAdd(&tcount[ht_key[i]], ht_val[i]);
+}
+
+// ------------------------------------------------ hash-probe intersection
+// u-centric: N+(u) goes into a shared-memory hash set; every v in N+(u)
+// streams N+(v) with coalesced loads and probes the set, so each entry costs
+// one independent probe instead of a dependent merge step.  Pairs where
+// N+(v) is much longer than N+(u) binary-search N+(u)'s entries in N+(v).
+constexpr uint32_t TC_WARP_TAB = 512;  // per-warp set: N+(u) up to 256 entries
+constexpr uint32_t TC_CREDIT_HT = 2048;
+
+struct TcCredit {
+    uint32_t *key;
+    unsigned long long *val;
+    unsigned long long *global;
+    __device__ __forceinline__ void add(uint32_t k, unsigned long long amount) {
+        uint32_t h = (k * 2654435761u) & (TC_CREDIT_HT - 1);
+        for (int probe = 0; probe < 8; ++probe) {
+            uint32_t cur = key[h];
+            if (cur == GV_NIL) cur = atomicCAS(&key[h], GV_NIL, k);
+            if (cur == GV_NIL || cur == k) {
+                atomicAdd(&val[h], amount);
+                return;
+            }
+            h = (h + 1) & (TC_CREDIT_HT - 1);
+        }
+        atomicAdd(&global[k], amount);
+    }
+    __device__ __forceinline__ void flush() {
+        for (uint32_t i = threadIdx.x; i < TC_CREDIT_HT; i += blockDim.x)
+            if (key[i] != GV_NIL && val[i]) atomicAdd(&global[key[i]], val[i]);
+    }
+};
+
+__device__ __forceinline__ uint32_t tc_hash(uint32_t x, uint32_t mask) { return (x * 2654435761u) & mask; }
+
+// Callers size the table to at least twice the entries, so a free slot is
+// always found; the probe count is bounded by the table size regardless.
+__device__ __forceinline__ void set_insert(uint32_t *tab, uint32_t mask, uint32_t x) {
+    uint32_t h = tc_hash(x, mask);
+    for (uint32_t p = 0; p <= mask; ++p) {
+        const uint32_t old = atomicCAS(&tab[h], GV_NIL, x);
+        if (old == GV_NIL || old == x) return;
+        h = (h + 1) & mask;
+    }
+}
+
+// Membership in a hash set (mask != 0) or in a sorted array of `mask_or_len`
+// entries (sorted == true).
+__device__ __forceinline__ bool set_has(const uint32_t *tab, uint32_t mask, uint32_t x, bool sorted) {
+    if (sorted) {
+        const uint32_t pos = lower_bound_u32(tab, mask, x);
+        return pos < mask && tab[pos] == x;
+    }
+    uint32_t h = tc_hash(x, mask);
+    for (uint32_t p = 0; p <= mask; ++p) {
+        const uint32_t k = tab[h];
+        if (k == x) return true;
+        if (k == GV_NIL) return false;
+        h = (h + 1) & mask;
+    }
+    return false;
+}
+
+template <bool INCIDENT>
+__device__ __forceinline__ void tc_credit(TcCredit &cr, uint32_t u, uint32_t v, uint32_t w, uint32_t &cu,
+                                          uint32_t &cv) {
+    if (INCIDENT) {
+        ++cu;
+        ++cv;
+        cr.add(w, 1ull);
+    } else {
+        const uint32_t m = min(u, v);
+        if (w < m) cr.add(w, 1ull);
+        else if (u < v) ++cu;
+        else ++cv;
+    }
+}
+
+// Probes all v in N+(u) against the set `tab` (threads t of nt cooperate on
+// each v; `sync` separates nothing: the set is read-only here).
+template <bool INCIDENT>
+__device__ __forceinline__ unsigned long long tc_probe_all(const unsigned long long *__restrict__ off,
+                                                           const uint32_t *__restrict__ snap, uint32_t u,
+                                                           const uint32_t *A, uint32_t la, const uint32_t *tab,
+                                                           uint32_t mask, bool sorted, uint32_t v_first,
+                                                           uint32_t v_step, uint32_t t, uint32_t nt, TcCredit &cr,
+                                                           uint32_t &cu_tot) {
+    unsigned long long work = 0;  // list entries touched (counted once per pair)
+    for (uint32_t j = v_first; j < la; j += v_step) {
+        const uint32_t v = A[j];
+        const uint32_t *Bv = snap + off[v];
+        const uint32_t lb = (uint32_t)(off[v + 1] - off[v]);
+        uint32_t cu = 0, cv = 0;
+        if (lb > 16u * la) {
+            // long N+(v): binary-search the entries of N+(u) in it
+            const uint32_t lgB = 32 - __clz(lb);
+            for (uint32_t i = t; i < la; i += nt) {
+                const uint32_t w = A[i];
+                const uint32_t pos = lower_bound_u32(Bv, lb, w);
+                if (pos < lb && Bv[pos] == w) tc_credit<INCIDENT>(cr, u, v, w, cu, cv);
+            }
+            if (t == 0) work += (unsigned long long)la * (lgB + 1);
+        } else {
+            for (uint32_t k = t; k < lb; k += nt) {
+                const uint32_t w = __ldg(Bv + k);
+                if (set_has(tab, mask, w, sorted)) tc_credit<INCIDENT>(cr, u, v, w, cu, cv);
+            }
+            if (t == 0) work += lb;
+        }
+        cu_tot += cu;
+        if (cv) cr.add(v, cv);
+    }
+    return work;
+}
+
+template <bool INCIDENT>
+__global__ void __launch_bounds__(AN_THREADS) k_tc_hash(const unsigned long long *__restrict__ off,
+                                                        const uint32_t *__restrict__ snap, uint32_t n,
+                                                        unsigned long long *__restrict__ tcount,
+                                                        uint32_t *__restrict__ big_u, unsigned long long *nbig,
+                                                        unsigned long long *__restrict__ work) {
+    __shared__ uint32_t wtab[AN_THREADS / 32][TC_WARP_TAB];
+    __shared__ uint32_t ck[TC_CREDIT_HT];
+    __shared__ unsigned long long cval[TC_CREDIT_HT];
+    __shared__ unsigned long long wred[AN_THREADS / 32];
+    for (uint32_t i = threadIdx.x; i < TC_CREDIT_HT; i += blockDim.x) {
+        ck[i] = GV_NIL;
+        cval[i] = 0;
+    }
+    __syncthreads();
+    TcCredit cr{ck, cval, tcount};
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint32_t *tab = wtab[warp];
+    const uint32_t mask = TC_WARP_TAB - 1;
+    unsigned long long my_work = 0;
+    const uint32_t nw = gridDim.x * (AN_THREADS / 32);
+    for (uint32_t u = blockIdx.x * (AN_THREADS / 32) + warp; u < n; u += nw) {
+        const uint32_t la = (uint32_t)(off[u + 1] - off[u]);
+        if (la < 2) continue;  // a triangle needs two out-neighbours of u
+        if (la > TC_WARP_TAB / 2) {
+            if (lane == 0) big_u[atomicAdd(nbig, 1ull)] = u;
+            continue;
+        }
+        const uint32_t *A = snap + off[u];
+        for (uint32_t i = lane; i < TC_WARP_TAB; i += 32) tab[i] = GV_NIL;
+        __syncwarp();
+        for (uint32_t i = lane; i < la; i += 32) set_insert(tab, mask, A[i]);
+        __syncwarp();
+        uint32_t cu = 0;
+        my_work += tc_probe_all<INCIDENT>(off, snap, u, A, la, tab, mask, false, 0, 1, lane, 32, cr, cu);
+        cu = warp_sum(cu);
+        if (lane == 0 && cu) cr.add(u, cu);
+        __syncwarp();
+    }
+    my_work = warp_sum(my_work);
+    if (lane == 0) wred[warp] = my_work;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long t = 0;
+        for (int i = 0; i < AN_THREADS / 32; ++i) t += wred[i];
+        if (t) atomicAdd(work, t);
+    }
+    cr.flush();
+}
+
+// Vertices with long N+(u): one CTA per vertex, set in dynamic shared memory.
+template <bool INCIDENT>
+__global__ void __launch_bounds__(512) k_tc_hash_big(const unsigned long long *__restrict__ off,
+                                                     const uint32_t *__restrict__ snap,
+                                                     unsigned long long *__restrict__ tcount,
+                                                     const uint32_t *__restrict__ big_u, const unsigned long long *nbig,
+                                                     uint32_t tab_size, unsigned long long *__restrict__ work) {
+    extern __shared__ uint32_t dyn[];
+    __shared__ uint32_t ck[TC_CREDIT_HT];
+    __shared__ unsigned long long cval[TC_CREDIT_HT];
+    __shared__ uint32_t cured[16];
+    __shared__ unsigned long long wred[16];
+    for (uint32_t i = threadIdx.x; i < TC_CREDIT_HT; i += blockDim.x) {
+        ck[i] = GV_NIL;
+        cval[i] = 0;
+    }
+    __syncthreads();
+    TcCredit cr{ck, cval, tcount};
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    const uint32_t nb = (uint32_t)*nbig;
+    unsigned long long my_work = 0;
+    for (uint32_t bi = blockIdx.x; bi < nb; bi += gridDim.x) {
+        const uint32_t u = big_u[bi];
+        const uint32_t la = (uint32_t)(off[u + 1] - off[u]);
+        const uint32_t *A = snap + off[u];
+        // hash set when it fits at half load, else a sorted copy (la <= tab_size
+        // is guaranteed by the host)
+        const bool sorted = 2 * la > tab_size;
+        uint32_t mask;
+        if (sorted) {
+            for (uint32_t i = threadIdx.x; i < la; i += blockDim.x) dyn[i] = A[i];
+            mask = la;
+        } else {
+            uint32_t size = 1024;
+            while (size < 2 * la) size <<= 1;
+            mask = size - 1;
+            for (uint32_t i = threadIdx.x; i < size; i += blockDim.x) dyn[i] = GV_NIL;
+            __syncthreads();
+            for (uint32_t i = threadIdx.x; i < la; i += blockDim.x) set_insert(dyn, mask, A[i]);
+        }
+        __syncthreads();
+        uint32_t cu = 0;
+        my_work += tc_probe_all<INCIDENT>(off, snap, u, A, la, dyn, mask, sorted, warp, nwarps, lane, 32, cr, cu);
+        cu = warp_sum(cu);
+        if (lane == 0) cured[warp] = cu;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t t = 0;
+            for (uint32_t i = 0; i < nwarps; ++i) t += cured[i];
+            if (t) cr.add(u, t);
+        }
+        __syncthreads();
+    }
+    my_work = warp_sum(my_work);
+    if (lane == 0) wred[warp] = my_work;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long t = 0;
+        for (uint32_t i = 0; i < nwarps; ++i) t += wred[i];
+        if (t) atomicAdd(work, t);
+    }
+    cr.flush();
 }
 
 __global__ void k_tc_esrc(const unsigned long long *__restrict__ off, uint32_t n, uint32_t *__restrict__ esrc) {
@@ -557,9 +1022,10 @@ __global__ void k_gather_u64(const unsigned long long *__restrict__ x, const uin
 struct TcBufs {
     uint32_t *dplus;
     unsigned long long *off;
-    uint32_t *snap, *esrc, *mid, *big;
-    unsigned long long *cnts;
+    uint32_t *snap, *esrc, *mid, *big, *hubs;
+    unsigned long long *cnts;  // [0] mid lists, [1] big lists, [2] hubs
     unsigned long long *tcount;
+    unsigned long long *hcur;  // per-hub write cursors
 };
 
 // Builds the oriented sorted snapshot and counts.  tcount[n] receives the
@@ -568,60 +1034,82 @@ gv_status tc_run(gv_graph *g, cudaStream_t s, bool incident, unsigned long long 
     if (g->cfg.directed) { set_error("triangle counting needs an undirected store"); return GV_ERR_STATE; }
     DevGraph d = g->d;
     const uint32_t n = d.n;
-    // Phase 1: oriented out-degrees and offsets, then size the snapshot exactly.
-    const size_t head = ((size_t)n + 1) * 8 + (size_t)n * 8 + 64 + (size_t)n * 4 * 3;
-    void *buf = analytics_scratch(g, head + 256);
+    uint64_t live = 0;
+    {
+        Ctl c;
+        gv_status st = read_ctl(g, &c, s);
+        if (st != GV_OK) return st;
+        live = c.live_edges;
+    }
+    // An oriented snapshot holds at most one entry per live entry.
+    const size_t head = ((size_t)n + 1) * 8 + (size_t)n * 8 * 2 + 64 + (size_t)n * 4 * 4;
+    void *buf = analytics_scratch(g, head + 2 * (live + 1) * 4 + 256);
     if (!buf) return GV_ERR_NOMEM;
     TcBufs b;
-    auto carve = [&](void *base, uint64_t mp) {
-        char *p = (char *)base;
+    {
+        char *p = (char *)buf;
         b.off = (unsigned long long *)p; p += ((size_t)n + 1) * 8;
         b.tcount = (unsigned long long *)p; p += (size_t)n * 8;
+        b.hcur = (unsigned long long *)p; p += (size_t)n * 8;
         b.cnts = (unsigned long long *)p; p += 64;
         b.dplus = (uint32_t *)p; p += (size_t)n * 4;
         b.mid = (uint32_t *)p; p += (size_t)n * 4;
         b.big = (uint32_t *)p; p += (size_t)n * 4;
-        b.snap = (uint32_t *)p; p += mp * 4;
+        b.hubs = (uint32_t *)p; p += (size_t)n * 4;
+        b.snap = (uint32_t *)p; p += (live + 1) * 4;
         b.esrc = (uint32_t *)p;
-    };
-    carve(buf, 0);
+    }
     const uint32_t tpv = g->cfg.threads_per_vertex;
-    dispatch_tpv(tpv, [&](auto t) {
-        constexpr int T = decltype(t)::value;
-        GV_LAUNCH((k_tc_outdeg<T>), grid_for(n, AN_THREADS / T), AN_THREADS, 0, s, d, b.dplus);
-    });
-    scan_exclusive_u32_to_u64(b.dplus, b.off, n, b.off + n, g->bs.scan_tmp, s);
     unsigned long long mplus = 0;
     {
-        cudaError_t e = cudaMemcpyAsync(&mplus, b.off + n, 8, cudaMemcpyDeviceToHost, s);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        ProfScope ps(PROF_TC_SNAPSHOT, s);
+        uint32_t *deg = b.hubs;  // live degree per vertex (4 B, stays in L2)
+        launch_degrees(g, deg, s);
+        cudaMemsetAsync(b.cnts, 0, 64, s);
+        Items it{};
+        float *ip = nullptr;
+        gv_status st = build_items(g, s, b.cnts + 3, &it, &ip);
+        if (st != GV_OK) return st;
+        uint32_t *icnt = (uint32_t *)ip;
+        uint32_t *ioff = nullptr;
+        if (it.nitems) {
+            ioff = (uint32_t *)aux_scratch(g, 3, (size_t)it.nitems * 4);
+            if (!ioff) return GV_ERR_NOMEM;
+        }
+        dispatch_tpv(tpv, [&](auto t) {
+            constexpr int T = decltype(t)::value;
+            GV_LAUNCH((k_tc_outdeg<T>), grid_for(n, AN_THREADS / T), AN_THREADS, 0, s, d, (const uint32_t *)deg, b.dplus);
+        });
+        if (it.nitems) {
+            GV_LAUNCH(k_tc_items<false>, PULL_GRID, AN_THREADS, 0, s, d, (const uint32_t *)deg, it, icnt,
+                      (const uint32_t *)nullptr, (const unsigned long long *)nullptr, (uint32_t *)nullptr);
+            GV_LAUNCH(k_tc_multi, grid_for(it.nmulti, 256), 256, 0, s, it, (const uint32_t *)icnt, ioff, b.dplus);
+        }
+        scan_exclusive_u32_to_u64(b.dplus, b.off, n, b.off + n, g->bs.scan_tmp, s);
+        cudaMemcpyAsync(&mplus, b.off + n, 8, cudaMemcpyDeviceToHost, s);
+        cudaError_t e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) return cuda_status(e, "tc");
+        if (mplus > live) { set_error("oriented snapshot larger than the store"); return GV_ERR_STATE; }
+        cudaMemsetAsync(b.tcount, 0, (size_t)n * 8, s);
+        dispatch_tpv(tpv, [&](auto t) {
+            constexpr int T = decltype(t)::value;
+            GV_LAUNCH((k_tc_write<T>), grid_for(n, AN_THREADS / T), AN_THREADS, 0, s, d, (const uint32_t *)deg,
+                      (const unsigned long long *)b.off, b.snap);
+        });
+        if (it.nitems)
+            GV_LAUNCH(k_tc_items<true>, PULL_GRID, AN_THREADS, 0, s, d, (const uint32_t *)deg, it, icnt,
+                      (const uint32_t *)ioff, (const unsigned long long *)b.off, b.snap);
+        GV_LAUNCH(k_tc_classify, grid_for(n, 256), 256, 0, s, (const unsigned long long *)b.off, n, b.snap, b.mid, b.big,
+                  b.cnts);
+        GV_LAUNCH(k_tc_sort_mid, 148 * 4, AN_THREADS, 0, s, (const unsigned long long *)b.off, b.snap,
+                  (const uint32_t *)b.mid, (const unsigned long long *)b.cnts);
     }
-    if (g->an_bytes < head + 2 * (mplus + 1) * 4 + 256) {
-        // grow the scratch and keep the offsets computed so far
-        std::vector<unsigned long long> hoff((size_t)n + 1);
-        cudaMemcpy(hoff.data(), b.off, hoff.size() * 8, cudaMemcpyDeviceToHost);
-        buf = analytics_scratch(g, head + 2 * (mplus + 1) * 4 + 256);
-        if (!buf) return GV_ERR_NOMEM;
-        carve(buf, mplus + 1);
-        cudaMemcpyAsync(b.off, hoff.data(), hoff.size() * 8, cudaMemcpyHostToDevice, s);
-    } else {
-        carve(buf, mplus + 1);
-    }
-    cudaMemsetAsync(b.cnts, 0, 64, s);
-    cudaMemsetAsync(b.tcount, 0, (size_t)n * 8, s);
-    dispatch_tpv(tpv, [&](auto t) {
-        constexpr int T = decltype(t)::value;
-        GV_LAUNCH((k_tc_write<T>), grid_for(n, AN_THREADS / T), AN_THREADS, 0, s, d, (const unsigned long long *)b.off,
-                  b.snap, b.mid, b.big, b.cnts);
-    });
-    GV_LAUNCH(k_tc_sort_mid, 148 * 4, AN_THREADS, 0, s, (const unsigned long long *)b.off, b.snap,
-              (const uint32_t *)b.mid, (const unsigned long long *)b.cnts);
     // longest list bounds the CTA sort's shared memory
     unsigned long long h[2] = {0, 0};
     cudaMemcpyAsync(h, b.cnts, 16, cudaMemcpyDeviceToHost, s);
     cudaError_t e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_status(e, "tc");
+    uint64_t max_len = 1024;  // lists up to 1024 entries are sorted by warps
     if (h[1]) {
         std::vector<uint32_t> bl(h[1]);
         std::vector<unsigned long long> hoff(n + 1);
@@ -629,6 +1117,7 @@ gv_status tc_run(gv_graph *g, cudaStream_t s, bool incident, unsigned long long 
         cudaMemcpy(bl.data(), b.big, h[1] * 4, cudaMemcpyDeviceToHost);
         uint64_t mx = 0;
         for (uint32_t u : bl) mx = std::max<uint64_t>(mx, hoff[u + 1] - hoff[u]);
+        max_len = std::max<uint64_t>(max_len, mx);
         uint32_t P = 1024;
         while (P < mx) P <<= 1;
         const size_t smem = (size_t)P * 4;
@@ -637,10 +1126,43 @@ gv_status tc_run(gv_graph *g, cudaStream_t s, bool incident, unsigned long long 
         GV_LAUNCH(k_tc_sort_big, 148, 1024, smem, s, (const unsigned long long *)b.off, b.snap,
                   (const uint32_t *)b.big, (const unsigned long long *)b.cnts, P);
     }
-    GV_LAUNCH(k_tc_esrc, grid_for(n, 256), 256, 0, s, (const unsigned long long *)b.off, n, b.esrc);
-    const unsigned cgrid = grid_for(mplus, AN_THREADS / 8, 148 * 16);
-    if (incident) GV_LAUNCH((k_tc_count<8, true>), cgrid, AN_THREADS, 0, s, (const unsigned long long *)b.off, b.snap, b.esrc, mplus, b.tcount);
-    else GV_LAUNCH((k_tc_count<8, false>), cgrid, AN_THREADS, 0, s, (const unsigned long long *)b.off, b.snap, b.esrc, mplus, b.tcount);
+    unsigned long long *work = &d.ctl->scratch1;
+    cudaMemsetAsync(work, 0, 8, s);
+    const char *merge_env = std::getenv("GV_TC_MERGE");
+    if (merge_env && merge_env[0] == '1') {
+        // merge-path intersection per oriented edge (kept for comparison)
+        GV_LAUNCH(k_tc_esrc, grid_for(n, 256), 256, 0, s, (const unsigned long long *)b.off, n, b.esrc);
+        const unsigned cgrid = grid_for(mplus, AN_THREADS / 8, 148 * 16);
+        ProfScope ps(PROF_TC_COUNT, s);
+        if (incident) GV_LAUNCH((k_tc_count<8, true>), cgrid, AN_THREADS, 0, s, (const unsigned long long *)b.off, b.snap, b.esrc, mplus, b.tcount, work);
+        else GV_LAUNCH((k_tc_count<8, false>), cgrid, AN_THREADS, 0, s, (const unsigned long long *)b.off, b.snap, b.esrc, mplus, b.tcount, work);
+    } else {
+        // hash-probe intersection; lists above 256 entries go to one CTA each
+        constexpr uint32_t TAB = 48 * 1024;  // entries of the CTA's shared set
+        if (max_len > TAB) { set_error("oriented out-degree exceeds the shared-memory set"); return GV_ERR_UNSUPPORTED; }
+        const size_t tab_bytes = (size_t)TAB * 4;
+        static bool attr = false;
+        if (!attr) {
+            cudaFuncSetAttribute(k_tc_hash_big<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tab_bytes);
+            cudaFuncSetAttribute(k_tc_hash_big<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tab_bytes);
+            attr = true;
+        }
+        unsigned long long *nbig = b.cnts + 4;
+        cudaMemsetAsync(nbig, 0, 8, s);
+        ProfScope ps(PROF_TC_COUNT, s);
+        if (incident) {
+            GV_LAUNCH(k_tc_hash<true>, PULL_GRID, AN_THREADS, 0, s, (const unsigned long long *)b.off, (const uint32_t *)b.snap,
+                      n, b.tcount, b.mid, nbig, work);
+            GV_LAUNCH(k_tc_hash_big<true>, 148, 512, tab_bytes, s, (const unsigned long long *)b.off,
+                      (const uint32_t *)b.snap, b.tcount, (const uint32_t *)b.mid, (const unsigned long long *)nbig, TAB, work);
+        } else {
+            GV_LAUNCH(k_tc_hash<false>, PULL_GRID, AN_THREADS, 0, s, (const unsigned long long *)b.off, (const uint32_t *)b.snap,
+                      n, b.tcount, b.mid, nbig, work);
+            GV_LAUNCH(k_tc_hash_big<false>, 148, 512, tab_bytes, s, (const unsigned long long *)b.off,
+                      (const uint32_t *)b.snap, b.tcount, (const uint32_t *)b.mid, (const unsigned long long *)nbig, TAB, work);
+        }
+    }
+    g->last_tc_oriented = mplus;
     *tcount_out = b.tcount;
     return cuda_status(cudaGetLastError(), "tc launch");
 }
@@ -658,9 +1180,24 @@ struct BcBufs {
     unsigned long long *qtail;    // per slot
     int *active;                  // any slot still expanding
     double *bc;                   // fp64 accumulator (n)
+    uint32_t *hv;                 // [slot][n] frontier vertices routed to the hub kernels
+    unsigned long long *hv_cnt;   // per slot
 };
 
 constexpr int BC_MAXL = 4096;
+
+__device__ __forceinline__ void bfs_visit(uint32_t w, int32_t nl, unsigned long long sv, int32_t *dist,
+                                          unsigned long long *sigma, uint32_t *queue, unsigned long long *qtail) {
+    int32_t dw = dist[w];
+    if (dw < 0) {
+        dw = atomicCAS(&dist[w], -1, nl);
+        if (dw < 0) {
+            dw = nl;
+            queue[atomicAdd(qtail, 1ull)] = w;
+        }
+    }
+    if (dw == nl) atomicAdd(&sigma[w], sv);
+}
 
 template <int TPV>
 __global__ void __launch_bounds__(AN_THREADS) k_bfs_level(DevGraph g, BcBufs b, uint32_t level) {
@@ -682,26 +1219,50 @@ __global__ void __launch_bounds__(AN_THREADS) k_bfs_level(DevGraph g, BcBufs b, 
         const unsigned long long sv = sigma[v];
         const uint4 rec = g.vtx[v];
         const uint32_t fill = rec.y, nb = blocks_for(fill, g.logB);
-        for (uint32_t k0 = 0; k0 < nb; k0 += BIG_BLOCKS) {
-            const uint32_t kc = min((uint32_t)BIG_BLOCKS, nb - k0);
-            fill_block_table(g, rec.x, k0, kc, tab, G.gl, TPV);
-            G.sync();
-            const uint32_t e0 = k0 << g.logB, e1 = min(fill, (k0 + kc) << g.logB);
-            for (uint32_t e = e0 + G.gl; e < e1; e += TPV) {
-                const uint32_t w = g.pool[((size_t)tab[(e >> g.logB) - k0] << g.logB) + (e & (g.B - 1))];
-                if (w == GV_TOMB) continue;
-                int32_t dw = dist[w];
-                if (dw < 0) {
-                    dw = atomicCAS(&dist[w], -1, nl);
-                    if (dw < 0) {
-                        dw = nl;
-                        const unsigned long long p = atomicAdd(&b.qtail[slot], 1ull);
-                        queue[p] = w;
-                    }
-                }
-                if (dw == nl) atomicAdd(&sigma[w], sv);
+        if (fill > BFS_LIGHT_FILL) {
+            if (G.gl == 0) b.hv[(size_t)slot * n + atomicAdd(&b.hv_cnt[slot], 1ull)] = v;
+            continue;
+        }
+        fill_block_table(g, rec.x, 0, nb, tab, G.gl, TPV);
+        G.sync();
+        for (uint32_t e = G.gl; e < fill; e += TPV) {
+            const uint32_t w = g.pool[((size_t)tab[e >> g.logB] << g.logB) + (e & (g.B - 1))];
+            if (w != GV_TOMB) bfs_visit(w, nl, sv, dist, sigma, queue, &b.qtail[slot]);
+        }
+        G.sync();
+    }
+}
+
+// Heavy frontier vertices of one level: all CTAs of the slot split their blocks.
+__global__ void __launch_bounds__(HV_THREADS) k_bfs_hub(DevGraph g, BcBufs b, uint32_t level) {
+    const uint32_t slot = blockIdx.y, n = g.n;
+    const uint32_t cnt = (uint32_t)b.hv_cnt[slot];
+    if (cnt == 0) return;
+    int32_t *dist = b.dist + (size_t)slot * n;
+    unsigned long long *sigma = b.sigma + (size_t)slot * n;
+    uint32_t *queue = b.queue + (size_t)slot * n;
+    const uint32_t *hv = b.hv + (size_t)slot * n;
+    const int32_t nl = (int32_t)level + 1;
+    WarpBlocks W(g.B);
+    const uint32_t gw = blockIdx.x * (HV_THREADS / 32) + (threadIdx.x >> 5), nw = gridDim.x * (HV_THREADS / 32);
+    for (uint32_t h = 0; h < cnt; ++h) {
+        const uint32_t v = hv[h];
+        const unsigned long long sv = sigma[v];
+        const uint4 rec = g.vtx[v];
+        const uint32_t fill = rec.y, nb = blocks_for(fill, g.logB);
+        for (uint32_t k0 = gw * W.bpw; k0 < nb; k0 += nw * W.bpw) {
+            const uint32_t k = k0 + W.sub;
+            if (k >= nb) continue;
+            const uint32_t blk = (k == 0) ? rec.x : cbt_block(g.left, g.right, rec.x, k);
+            const uint32_t slots = min(g.B, fill - (k << g.logB));
+            const size_t base = (size_t)blk << g.logB;
+            for (uint32_t e = W.sl * 4; e < slots; e += W.lpb * 4) {
+                const uint4 q = *reinterpret_cast<const uint4 *>(g.pool + base + e);
+                const uint32_t ev[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    if (e + j < slots && ev[j] != GV_TOMB) bfs_visit(ev[j], nl, sv, dist, sigma, queue, &b.qtail[slot]);
             }
-            G.sync();
         }
     }
 }
@@ -713,6 +1274,7 @@ __global__ void k_bfs_close(BcBufs b, uint32_t nslots, uint32_t level) {
     unsigned long long *ls = b.lstart + (size_t)slot * (BC_MAXL + 1);
     const unsigned long long t = b.qtail[slot];
     ls[level + 2] = t;
+    b.hv_cnt[slot] = 0;
     if (t > ls[level + 1]) atomicOr(b.active, 1);
 }
 
@@ -750,21 +1312,64 @@ __global__ void __launch_bounds__(AN_THREADS) k_bc_dep(DevGraph g, BcBufs b, uin
         const double sv = (double)sigma[v];
         const uint4 rec = g.vtx[v];
         const uint32_t fill = rec.y, nb = blocks_for(fill, g.logB);
-        double acc = 0.0;
-        for (uint32_t k0 = 0; k0 < nb; k0 += BIG_BLOCKS) {
-            const uint32_t kc = min((uint32_t)BIG_BLOCKS, nb - k0);
-            fill_block_table(g, rec.x, k0, kc, tab, G.gl, TPV);
-            G.sync();
-            const uint32_t e0 = k0 << g.logB, e1 = min(fill, (k0 + kc) << g.logB);
-            for (uint32_t e = e0 + G.gl; e < e1; e += TPV) {
-                const uint32_t w = g.pool[((size_t)tab[(e >> g.logB) - k0] << g.logB) + (e & (g.B - 1))];
-                if (w == GV_TOMB) continue;
-                if (dist[w] == nl) acc += (sv / (double)sigma[w]) * (1.0 + delta[w]);
-            }
-            G.sync();
+        if (fill > BFS_LIGHT_FILL) {
+            if (G.gl == 0) b.hv[(size_t)slot * n + atomicAdd(&b.hv_cnt[slot], 1ull)] = v;
+            continue;
         }
+        double acc = 0.0;
+        fill_block_table(g, rec.x, 0, nb, tab, G.gl, TPV);
+        G.sync();
+        for (uint32_t e = G.gl; e < fill; e += TPV) {
+            const uint32_t w = g.pool[((size_t)tab[e >> g.logB] << g.logB) + (e & (g.B - 1))];
+            if (w != GV_TOMB && dist[w] == nl) acc += (sv / (double)sigma[w]) * (1.0 + delta[w]);
+        }
+        G.sync();
         acc = G.sum(acc);
         if (G.gl == 0) delta[v] = acc;
+    }
+}
+
+// Heavy vertices of one dependency level: every CTA of the slot adds a warp
+// partial per block share into delta[v] (fp64 atomics; delta of heavy
+// vertices starts at zero).
+__global__ void __launch_bounds__(HV_THREADS) k_bc_dep_hub(DevGraph g, BcBufs b, uint32_t level) {
+    const uint32_t slot = blockIdx.y, n = g.n;
+    const uint32_t cnt = (uint32_t)b.hv_cnt[slot];
+    if (cnt == 0) return;
+    const int32_t *dist = b.dist + (size_t)slot * n;
+    const unsigned long long *sigma = b.sigma + (size_t)slot * n;
+    double *delta = b.delta + (size_t)slot * n;
+    const uint32_t *hv = b.hv + (size_t)slot * n;
+    const int32_t nl = (int32_t)level + 1;
+    WarpBlocks W(g.B);
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t gw = blockIdx.x * (HV_THREADS / 32) + (threadIdx.x >> 5), nw = gridDim.x * (HV_THREADS / 32);
+    for (uint32_t h = 0; h < cnt; ++h) {
+        const uint32_t v = hv[h];
+        const double sv = (double)sigma[v];
+        const uint4 rec = g.vtx[v];
+        const uint32_t fill = rec.y, nb = blocks_for(fill, g.logB);
+        double acc = 0.0;
+        bool any = false;
+        for (uint32_t k0 = gw * W.bpw; k0 < nb; k0 += nw * W.bpw) {
+            any = true;
+            const uint32_t k = k0 + W.sub;
+            if (k >= nb) continue;
+            const uint32_t blk = (k == 0) ? rec.x : cbt_block(g.left, g.right, rec.x, k);
+            const uint32_t slots = min(g.B, fill - (k << g.logB));
+            const size_t base = (size_t)blk << g.logB;
+            for (uint32_t e = W.sl * 4; e < slots; e += W.lpb * 4) {
+                const uint4 q = *reinterpret_cast<const uint4 *>(g.pool + base + e);
+                const uint32_t ev[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    if (e + j < slots && ev[j] != GV_TOMB && dist[ev[j]] == nl)
+                        acc += (sv / (double)sigma[ev[j]]) * (1.0 + delta[ev[j]]);
+            }
+        }
+        if (!any) continue;  // warp-uniform
+        acc = warp_sum(acc);
+        if (lane == 0 && acc != 0.0) atomicAdd(&delta[v], acc);
     }
 }
 
@@ -789,18 +1394,24 @@ gv_status bfs_batch(gv_graph *g, cudaStream_t s, BcBufs &b, const uint32_t *dsrc
     const uint32_t n = d.n;
     cudaMemsetAsync(b.dist, 0xFF, (size_t)nslots * n * 4, s);
     cudaMemsetAsync(b.sigma, 0, (size_t)nslots * n * 8, s);
+    cudaMemsetAsync(b.hv_cnt, 0, (size_t)nslots * 8, s);
     GV_LAUNCH(k_bfs_init, (nslots + 63) / 64, 64, 0, s, b, n, dsrc, nslots);
     uint32_t level = 0;
     const unsigned gx = grid_for((uint64_t)n, AN_THREADS, 148 * 8 / std::max(1u, nslots) + 1);
+    const unsigned hx = std::max(1u, 148u * 2 / std::max(1u, nslots));
     while (true) {
         const int chunk = 4;
         cudaMemsetAsync(b.active, 0, 4, s);
         for (int i = 0; i < chunk; ++i) {
             if (level + 2 > BC_MAXL) { set_error("BFS deeper than the level table"); return GV_ERR_UNSUPPORTED; }
-            dispatch_tpv(g->cfg.threads_per_vertex, [&](auto t) {
-                constexpr int T = decltype(t)::value;
-                GV_LAUNCH((k_bfs_level<T>), dim3(gx, nslots), AN_THREADS, 0, s, d, b, level);
-            });
+            {
+                ProfScope ps(PROF_BFS_LEVEL, s);
+                dispatch_tpv(g->cfg.threads_per_vertex, [&](auto t) {
+                    constexpr int T = decltype(t)::value;
+                    GV_LAUNCH((k_bfs_level<T>), dim3(gx, nslots), AN_THREADS, 0, s, d, b, level);
+                });
+                GV_LAUNCH(k_bfs_hub, dim3(hx, nslots), HV_THREADS, 0, s, d, b, level);
+            }
             GV_LAUNCH(k_bfs_close, (nslots + 63) / 64, 64, 0, s, b, nslots, level);
             ++level;
         }
@@ -832,7 +1443,7 @@ gv_status bc_impl(gv_graph *g, const uint32_t *sources, uint64_t ns, float *bc_o
         if (hs[i] >= n) { set_error("BC source out of range"); return GV_ERR_INVALID; }
     // slots per batch: bounded by memory (~24 B per vertex per slot)
     uint64_t slots = 64;
-    const uint64_t per_slot = (uint64_t)n * (4 + 8 + 8 + 4) + (BC_MAXL + 1) * 8 + 16;
+    const uint64_t per_slot = (uint64_t)n * (4 + 8 + 8 + 4 + 4) + (BC_MAXL + 1) * 8 + 16 + 8;
     size_t fr = 0, tot = 0;
     cudaMemGetInfo(&fr, &tot);
     while (slots > 1 && slots * per_slot > fr / 4) slots >>= 1;
@@ -847,8 +1458,10 @@ gv_status bc_impl(gv_graph *g, const uint32_t *sources, uint64_t ns, float *bc_o
     b.sigma = (unsigned long long *)p; p += slots * n * 8;
     b.lstart = (unsigned long long *)p; p += slots * (BC_MAXL + 1) * 8;
     b.qtail = (unsigned long long *)p; p += slots * 8;
+    b.hv_cnt = (unsigned long long *)p; p += slots * 8;
     b.dist = (int32_t *)p; p += slots * n * 4;
     b.queue = (uint32_t *)p; p += slots * n * 4;
+    b.hv = (uint32_t *)p; p += slots * n * 4;
     b.active = (int *)p; p += 16;
     uint32_t *dsrc = (uint32_t *)p;
     cudaMemsetAsync(b.bc, 0, (size_t)n * 8, s);
@@ -863,12 +1476,17 @@ gv_status bc_impl(gv_graph *g, const uint32_t *sources, uint64_t ns, float *bc_o
         st = bfs_batch(g, s, b, dsrc, nsl, &depth, h_active);
         if (st != GV_OK) break;
         cudaMemsetAsync(b.delta, 0, (size_t)nsl * n * 8, s);
+        cudaMemsetAsync(b.hv_cnt, 0, (size_t)nsl * 8, s);
         const unsigned gx = grid_for((uint64_t)n, AN_THREADS, 148 * 8 / std::max(1u, nsl) + 1);
+        const unsigned hx = std::max(1u, 148u * 2 / std::max(1u, nsl));
         for (int32_t lv = (int32_t)depth; lv >= 0; --lv) {
+            ProfScope ps(PROF_BC_DEP, s);
             dispatch_tpv(g->cfg.threads_per_vertex, [&](auto t) {
                 constexpr int T = decltype(t)::value;
                 GV_LAUNCH((k_bc_dep<T>), dim3(gx, nsl), AN_THREADS, 0, s, d, b, (uint32_t)lv);
             });
+            GV_LAUNCH(k_bc_dep_hub, dim3(hx, nsl), HV_THREADS, 0, s, d, b, (uint32_t)lv);
+            cudaMemsetAsync(b.hv_cnt, 0, (size_t)nsl * 8, s);
         }
         GV_LAUNCH(k_bc_reduce, grid_for(n, 256), 256, 0, s, b, n, nsl, (const uint32_t *)dsrc);
     }
@@ -1089,7 +1707,7 @@ gv_status gv_bfs_sigma(gv_graph *g, uint32_t source, int32_t *dist, uint64_t *si
     if (!g || !dist || !sigma || source >= g->d.n) return GV_ERR_INVALID;
     cudaStream_t s = (cudaStream_t)stream;
     const uint32_t n = g->d.n;
-    const size_t bytes = (size_t)n * (4 + 8 + 8 + 4) + (BC_MAXL + 1) * 8 + 256;
+    const size_t bytes = (size_t)n * (4 + 8 + 8 + 4 + 4) + (BC_MAXL + 1) * 8 + 256;
     void *buf = analytics_scratch(g, bytes);
     if (!buf) return GV_ERR_NOMEM;
     char *p = (char *)buf;
@@ -1099,8 +1717,10 @@ gv_status gv_bfs_sigma(gv_graph *g, uint32_t source, int32_t *dist, uint64_t *si
     b.sigma = (unsigned long long *)p; p += (size_t)n * 8;
     b.lstart = (unsigned long long *)p; p += (BC_MAXL + 1) * 8;
     b.qtail = (unsigned long long *)p; p += 8;
+    b.hv_cnt = (unsigned long long *)p; p += 8;
     b.dist = (int32_t *)p; p += (size_t)n * 4;
     b.queue = (uint32_t *)p; p += (size_t)n * 4;
+    b.hv = (uint32_t *)p; p += (size_t)n * 4;
     b.active = (int *)p; p += 16;
     uint32_t *dsrc = (uint32_t *)p;
     cudaMemcpyAsync(dsrc, &source, 4, cudaMemcpyHostToDevice, s);
@@ -1131,7 +1751,7 @@ gv_status gv_wpr_forward(gv_graph *g, float alpha, float tol, int32_t max_iter, 
         if (st != GV_OK) return st;
         live = c.live_edges;
     }
-    const uint32_t parts = PULL_GRID + HEAVY_GRID;
+    const uint32_t parts = SWEEP_PARTS;
     const size_t bytes = iter_bytes(n, parts) + (size_t)n * 4 * 3 + ((size_t)n + 1) * 8 + (live + 1) * 8 + 512;
     void *buf = analytics_scratch(g, bytes);
     if (!buf) return GV_ERR_NOMEM;
@@ -1203,7 +1823,7 @@ gv_status gv_wpr_backward(gv_graph *g, float alpha, float tol, int32_t max_iter,
         live = cc.live_edges;
     }
     if (grad && cap < live) { set_error("gradient capacity below the number of entries"); return GV_ERR_CAPACITY; }
-    const uint32_t parts = PULL_GRID + HEAVY_GRID;
+    const uint32_t parts = SWEEP_PARTS;
     const size_t bytes = iter_bytes(n, parts) + (size_t)n * 4 * 4 + ((size_t)n + 1) * 8 + (live + 1) * 4 + 512;
     void *buf = analytics_scratch(g, bytes);
     if (!buf) return GV_ERR_NOMEM;

@@ -2,12 +2,15 @@
 // update entry points.  Replaces the host orchestration of class GraphVine
 // (src/dynamicStructure/graphvine.cu:5-527) with stream-ordered calls that
 // return status codes instead of exiting (include/util/cudaError.cuh:8-26).
+#include <atomic>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 #include "store.cuh"
 #include "prims.cuh"
+#include "prof.hpp"
 #include "launch.hpp"
 
 namespace gv {
@@ -164,10 +167,81 @@ void *analytics_scratch(gv_graph *g, size_t bytes) {
     return g->an_buf;
 }
 
+void *aux_scratch(gv_graph *g, int slot, size_t bytes) {
+    if (bytes > g->aux_bytes[slot]) {
+        if (g->aux[slot]) cudaFree(g->aux[slot]);
+        g->aux[slot] = nullptr;
+        g->aux_bytes[slot] = 0;
+        const size_t want = bytes + bytes / 4;
+        if (cudaMalloc(&g->aux[slot], want) != cudaSuccess) {
+            cudaGetLastError();
+            t_err = "auxiliary scratch allocation of " + std::to_string(want) + " B failed";
+            return nullptr;
+        }
+        g->aux_bytes[slot] = want;
+    }
+    return g->aux[slot];
+}
+
 gv_status read_ctl(gv_graph *g, Ctl *out, cudaStream_t s) {
     cudaError_t e = cudaMemcpyAsync(out, g->d.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     return cuda_status(e, "read control block");
+}
+
+// ----------------------------------------------------------------- profiler
+namespace {
+const char *const kProfNames[PROF_NSLOTS] = {"radix", "segment", "member", "apply", "compact",
+                                             "pull", "tc_snapshot", "tc_count", "bfs_level", "bc_dep"};
+struct ProfRec {
+    int slot;
+    cudaEvent_t a, b;
+};
+std::mutex prof_mu;
+std::atomic<bool> prof_on{false};
+std::vector<ProfRec> prof_recs;
+std::vector<cudaEvent_t> prof_pool;
+double prof_ms[PROF_NSLOTS];
+unsigned long long prof_n[PROF_NSLOTS];
+
+cudaEvent_t prof_event() {
+    if (!prof_pool.empty()) {
+        cudaEvent_t e = prof_pool.back();
+        prof_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+}
+
+void prof_collect_locked() {
+    for (ProfRec &r : prof_recs) {
+        float ms = 0.f;
+        if (cudaEventSynchronize(r.b) == cudaSuccess && cudaEventElapsedTime(&ms, r.a, r.b) == cudaSuccess) {
+            prof_ms[r.slot] += ms;
+            prof_n[r.slot] += 1;
+        }
+        prof_pool.push_back(r.a);
+        prof_pool.push_back(r.b);
+    }
+    prof_recs.clear();
+}
+}  // namespace
+
+int prof_begin(int slot, cudaStream_t s) {
+    if (!prof_on.load(std::memory_order_relaxed)) return -1;
+    std::lock_guard<std::mutex> lk(prof_mu);
+    ProfRec r{slot, prof_event(), prof_event()};
+    cudaEventRecord(r.a, s);
+    prof_recs.push_back(r);
+    return (int)prof_recs.size() - 1;
+}
+
+void prof_end(int token, cudaStream_t s) {
+    if (token < 0) return;
+    std::lock_guard<std::mutex> lk(prof_mu);
+    if (token < (int)prof_recs.size()) cudaEventRecord(prof_recs[token].b, s);
 }
 
 }  // namespace gv
@@ -181,6 +255,37 @@ const char *gv_version(void) { return "gv-b200 0.1 (sm_100a)"; }
 const char *gv_last_error_string(void) { return t_err.c_str(); }
 
 uint64_t gv_kernel_launches(void) { return g_launches.load(); }
+
+gv_status gv_profile_enable(int32_t on) {
+    std::lock_guard<std::mutex> lk(prof_mu);
+    if (!on) prof_collect_locked();
+    prof_on.store(on != 0);
+    return GV_OK;
+}
+
+gv_status gv_profile_reset(void) {
+    std::lock_guard<std::mutex> lk(prof_mu);
+    prof_collect_locked();
+    for (int i = 0; i < PROF_NSLOTS; ++i) {
+        prof_ms[i] = 0.0;
+        prof_n[i] = 0;
+    }
+    return GV_OK;
+}
+
+gv_status gv_profile_query(const char *name, double *total_ms, uint64_t *launches) {
+    if (!name) return GV_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(prof_mu);
+    prof_collect_locked();
+    for (int i = 0; i < PROF_NSLOTS; ++i)
+        if (std::strcmp(name, kProfNames[i]) == 0) {
+            if (total_ms) *total_ms = prof_ms[i];
+            if (launches) *launches = prof_n[i];
+            return GV_OK;
+        }
+    set_error(std::string("unknown profile slot ") + name);
+    return GV_ERR_INVALID;
+}
 
 gv_status gv_config_init(gv_config *cfg, uint32_t num_vertices) {
     if (!cfg) return GV_ERR_INVALID;
@@ -283,6 +388,8 @@ gv_status gv_destroy(gv_graph *g) {
     free_batch_entries(g->bs);
     free_batch_inputs(g->bs);
     if (g->an_buf) cudaFree(g->an_buf);
+    for (int i = 0; i < 4; ++i)
+        if (g->aux[i]) cudaFree(g->aux[i]);
     if (g->host_pinned) cudaFreeHost(g->host_pinned);
     delete g;
     return GV_OK;
@@ -504,6 +611,27 @@ gv_status gv_clear_affected(gv_graph *g, void *stream) {
     if (!g) return GV_ERR_INVALID;
     DeviceGuard dg(g->cfg.device);
     return cuda_status(cudaMemsetAsync(g->d.affected, 0, g->d.n, (cudaStream_t)stream), "clear affected");
+}
+
+gv_status gv_last_stat(gv_graph *g, const char *key, double *value) {
+    if (!g || !key || !value) return GV_ERR_INVALID;
+    DeviceGuard dg(g->cfg.device);
+    if (std::strcmp(key, "tc_work") == 0 || std::strcmp(key, "tc_oriented_edges") == 0) {
+        if (key[3] == 'o') {
+            *value = (double)g->last_tc_oriented;
+            return GV_OK;
+        }
+        Ctl c;
+        gv_status st = read_ctl(g, &c, 0);
+        if (st == GV_OK) *value = (double)c.scratch1;
+        return st;
+    }
+    if (std::strcmp(key, "sweeps") == 0) {
+        *value = (double)g->last_sweeps;
+        return GV_OK;
+    }
+    set_error(std::string("unknown stat ") + key);
+    return GV_ERR_INVALID;
 }
 
 gv_status gv_check(gv_graph *g, uint64_t *violations, uint32_t *first_code, uint32_t *first_vertex) {

@@ -43,6 +43,12 @@ struct gv_graph {
     size_t an_bytes = 0;
     void *host_pinned = nullptr;
     size_t host_pinned_bytes = 0;
+    // facts about the last analytics calls (gv_last_stat)
+    uint64_t last_tc_oriented = 0;
+    int32_t last_sweeps = 0;
+    // independent auxiliary device buffers, grown on demand
+    void *aux[4] = {nullptr, nullptr, nullptr, nullptr};
+    size_t aux_bytes[4] = {0, 0, 0, 0};
 };
 
 namespace gv {
@@ -51,6 +57,8 @@ void set_error(const std::string &msg);
 gv_status cuda_status(cudaError_t e, const char *what);
 gv_status ensure_batch_scratch(gv_graph *g, uint64_t entries, uint64_t pairs);
 void *analytics_scratch(gv_graph *g, size_t bytes);
+// Auxiliary buffer `slot` (0..3) of at least `bytes`, kept across calls.
+void *aux_scratch(gv_graph *g, int slot, size_t bytes);
 // Device-to-host copy of the control block (synchronises the stream).
 gv_status read_ctl(gv_graph *g, Ctl *out, cudaStream_t s);
 

@@ -26,6 +26,7 @@
 #include "group.cuh"
 #include "prims.cuh"
 #include "launch.hpp"
+#include "prof.hpp"
 
 namespace gv {
 
@@ -763,42 +764,51 @@ gv_status run_update(gv_graph *g, const uint32_t *dsrc, const uint32_t *ddst, co
     BatchScratch &bs = g->bs;
     const uint64_t E = symmetric ? 2 * k : k;
     const bool vals = (dw != nullptr) && !is_delete;
-    GV_LAUNCH(k_expand, grid_for(k, 256), 256, 0, s, dsrc, ddst, k, symmetric ? 1 : 0, g->d.n,
-              g->bitsn, bs.keys, vals ? bs.vals : nullptr, g->d.ctl);
-    const int nbits = 2 * (int)g->bitsn;
-    const int which = radix_sort_u64(bs.keys, bs.keys_alt, vals ? bs.vals : nullptr,
-                                     vals ? bs.vals_alt : nullptr, E, nbits, bs.rs_counts, bs.scan_tmp, s);
+    int which = 0;
+    {
+        ProfScope ps(PROF_RADIX, s);
+        GV_LAUNCH(k_expand, grid_for(k, 256), 256, 0, s, dsrc, ddst, k, symmetric ? 1 : 0, g->d.n,
+                  g->bitsn, bs.keys, vals ? bs.vals : nullptr, g->d.ctl);
+        which = radix_sort_u64(bs.keys, bs.keys_alt, vals ? bs.vals : nullptr, vals ? bs.vals_alt : nullptr,
+                               E, 2 * (int)g->bitsn, bs.rs_counts, bs.scan_tmp, s);
+    }
     const unsigned long long *K = which ? bs.keys_alt : bs.keys;
     const uint32_t *V = which ? bs.vals_alt : bs.vals;
     const unsigned long long sent = (g->bitsn >= 32) ? ~0ull : ((1ull << (2 * g->bitsn)) - 1ull);
     const unsigned ntiles = (unsigned)((E + SEG_TILE - 1) / SEG_TILE);
-    GV_LAUNCH(k_seg_count, ntiles, SEG_THREADS, 0, s, K, E, sent, g->bitsn, bs.tile_cnt);
-    scan_exclusive_u64(bs.tile_cnt, bs.tile_cnt, ntiles, &g->d.ctl->scratch0, bs.scan_tmp, s);
-    GV_LAUNCH(k_seg_write, ntiles, SEG_THREADS, 0, s, K, V, E, sent, g->bitsn, symmetric ? 1 : 0,
-              (const unsigned long long *)bs.tile_cnt, dw, bs.bdst, vals ? bs.bw : nullptr, bs.found,
-              bs.seg_vertex, bs.seg_start, g->d.affected, g->d.ctl);
+    {
+        ProfScope ps(PROF_SEGMENT, s);
+        GV_LAUNCH(k_seg_count, ntiles, SEG_THREADS, 0, s, K, E, sent, g->bitsn, bs.tile_cnt);
+        scan_exclusive_u64(bs.tile_cnt, bs.tile_cnt, ntiles, &g->d.ctl->scratch0, bs.scan_tmp, s);
+        GV_LAUNCH(k_seg_write, ntiles, SEG_THREADS, 0, s, K, V, E, sent, g->bitsn, symmetric ? 1 : 0,
+                  (const unsigned long long *)bs.tile_cnt, dw, bs.bdst, vals ? bs.bw : nullptr, bs.found,
+                  bs.seg_vertex, bs.seg_start, g->d.affected, g->d.ctl);
+    }
     // Segments <= unique entries <= E.
     const unsigned gsmall = grid_for(E, 64);
     const unsigned gbig = 148 * 2;
     const uint32_t tpv = g->cfg.threads_per_vertex;
     DevGraph d = g->d;
-    if (is_delete) {
+    {
+        ProfScope ps(PROF_MEMBER, s);
         dispatch_tpv(tpv, [&](auto t) {
             constexpr int T = decltype(t)::value;
-            GV_LAUNCH((k_member<T, true>), gsmall, UPD_THREADS, 0, s, d, bs.seg_vertex, bs.seg_start,
-                      bs.bdst, bs.found, bs.seg_found, bs.big_list);
+            if (is_delete)
+                GV_LAUNCH((k_member<T, true>), gsmall, UPD_THREADS, 0, s, d, bs.seg_vertex, bs.seg_start,
+                          bs.bdst, bs.found, bs.seg_found, bs.big_list);
+            else
+                GV_LAUNCH((k_member<T, false>), gsmall, UPD_THREADS, 0, s, d, bs.seg_vertex, bs.seg_start,
+                          bs.bdst, bs.found, bs.seg_found, bs.big_list);
         });
-        GV_LAUNCH(k_member_big<true>, gbig, BIG_THREADS, 0, s, d, bs.seg_vertex, bs.seg_start, bs.bdst,
-                  bs.found, bs.seg_found, bs.big_list);
-        GV_LAUNCH(k_finish, 1, 1, 0, s, d.ctl);
-    } else {
-        dispatch_tpv(tpv, [&](auto t) {
-            constexpr int T = decltype(t)::value;
-            GV_LAUNCH((k_member<T, false>), gsmall, UPD_THREADS, 0, s, d, bs.seg_vertex, bs.seg_start,
-                      bs.bdst, bs.found, bs.seg_found, bs.big_list);
-        });
-        GV_LAUNCH(k_member_big<false>, gbig, BIG_THREADS, 0, s, d, bs.seg_vertex, bs.seg_start, bs.bdst,
-                  bs.found, bs.seg_found, bs.big_list);
+        if (is_delete)
+            GV_LAUNCH(k_member_big<true>, gbig, BIG_THREADS, 0, s, d, bs.seg_vertex, bs.seg_start, bs.bdst,
+                      bs.found, bs.seg_found, bs.big_list);
+        else
+            GV_LAUNCH(k_member_big<false>, gbig, BIG_THREADS, 0, s, d, bs.seg_vertex, bs.seg_start, bs.bdst,
+                      bs.found, bs.seg_found, bs.big_list);
+    }
+    if (!is_delete) {
+        ProfScope ps(PROF_APPLY, s);
         GV_LAUNCH(k_plan, grid_for(E, UPD_THREADS), UPD_THREADS, 0, s, d, bs.seg_vertex, bs.seg_start,
                   bs.seg_found, bs.seg_newblocks, bs.seg_blkbase);
         GV_LAUNCH(k_admit, 1, 1, 0, s, d.ctl);
@@ -810,13 +820,14 @@ gv_status run_update(gv_graph *g, const uint32_t *dsrc, const uint32_t *ddst, co
         GV_LAUNCH(k_apply_big, gbig, BIG_THREADS, 0, s, d, bs.seg_vertex, bs.seg_start, bs.bdst,
                   vals ? bs.bw : nullptr, bs.found, bs.seg_found, bs.seg_newblocks, bs.seg_blkbase,
                   bs.big_list);
-        GV_LAUNCH(k_finish, 1, 1, 0, s, d.ctl);
     }
+    GV_LAUNCH(k_finish, 1, 1, 0, s, d.ctl);
     return cuda_status(cudaGetLastError(), "update launch");
 }
 
 gv_status run_compact(gv_graph *g, cudaStream_t s) {
     DevGraph d = g->d;
+    ProfScope ps(PROF_COMPACT, s);
     // The dirty list holds at most n vertices; size the grid for it.
     const unsigned grid = grid_for(g->d.n, 64);
     dispatch_tpv(g->cfg.threads_per_vertex, [&](auto t) {

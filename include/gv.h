@@ -132,6 +132,11 @@ gv_status gv_clear_affected(gv_graph *g, void *stream);
 gv_status gv_check(gv_graph *g, uint64_t *violations, uint32_t *first_code,
                    uint32_t *first_vertex);
 
+/* Facts about the last analytics call on this graph: "tc_work" = sum over
+ * oriented edges (u->v) of |N+(u)| + |N+(v)| merged by the last triangle
+ * count, "tc_oriented_edges", "sweeps" (last PageRank).  Synchronous. */
+gv_status gv_last_stat(gv_graph *g, const char *key, double *value);
+
 /* ---- analytics ---------------------------------------------------------- */
 
 /* PageRank: x0 = 1/n; x <- (1-alpha)/n + alpha * sum_{u->v} x_u / deg(u);
@@ -197,6 +202,15 @@ gv_status gv_wpr_backward(gv_graph *g, float alpha, float tol, int32_t max_iter,
 
 /* Number of kernels this library has launched in this process. */
 uint64_t gv_kernel_launches(void);
+
+/* Per-kernel device timing with CUDA events recorded on the launching
+ * stream (replaces the reference's wall-clock Profiler,
+ * src/util/profiler.cu:20-40).  Slots: "radix", "segment", "member",
+ * "apply", "compact", "pull", "tc_snapshot", "tc_count", "bfs_level",
+ * "bc_dep".  gv_profile_query synchronises the recorded events. */
+gv_status gv_profile_enable(int32_t on);
+gv_status gv_profile_reset(void);
+gv_status gv_profile_query(const char *name, double *total_ms, uint64_t *launches);
 /* Message for the last failing call on this host thread. */
 const char *gv_last_error_string(void);
 /* Library version string. */

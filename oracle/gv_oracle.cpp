@@ -4,8 +4,11 @@
 #include "gv_oracle.h"
 
 #include <omp.h>
+#include <parallel/algorithm>
 
 #include <algorithm>
+#include <atomic>
+#include <iterator>
 #include <cmath>
 #include <cstring>
 #include <numeric>
@@ -62,8 +65,41 @@ std::vector<std::pair<size_t, size_t>> groups(const std::vector<Entry> &e) {
     return r;
 }
 
+// Unweighted insert: duplicates are identical, so a parallel sort of packed
+// (src << 32 | dst) keys states the same set union.
+int insert_keys(or_graph *g, const uint32_t *src, const uint32_t *dst, uint64_t k, bool sym) {
+    std::vector<uint64_t> keys;
+    keys.reserve(sym ? 2 * k : k);
+    for (uint64_t i = 0; i < k; ++i) {
+        if (src[i] == dst[i]) continue;
+        keys.push_back(((uint64_t)src[i] << 32) | dst[i]);
+        if (sym) keys.push_back(((uint64_t)dst[i] << 32) | src[i]);
+    }
+    __gnu_parallel::sort(keys.begin(), keys.end());
+    keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
+    std::vector<size_t> starts;
+    for (size_t i = 0; i < keys.size(); ++i)
+        if (i == 0 || (keys[i] >> 32) != (keys[i - 1] >> 32)) starts.push_back(i);
+    starts.push_back(keys.size());
+    const long ngroups = (long)starts.size() - 1;
+#pragma omp parallel for schedule(dynamic, 256)
+    for (long gi = 0; gi < ngroups; ++gi) {
+        const uint32_t s = (uint32_t)(keys[starts[gi]] >> 32);
+        std::vector<uint32_t> &a = g->adj[s];
+        std::vector<uint32_t> add;
+        add.reserve(starts[gi + 1] - starts[gi]);
+        for (size_t q = starts[gi]; q < starts[gi + 1]; ++q) add.push_back((uint32_t)keys[q]);
+        std::vector<uint32_t> na;
+        na.reserve(a.size() + add.size());
+        std::set_union(a.begin(), a.end(), add.begin(), add.end(), std::back_inserter(na));
+        a.swap(na);
+    }
+    return 0;
+}
+
 int insert_impl(or_graph *g, const uint32_t *src, const uint32_t *dst, const float *w, uint64_t k, bool sym) {
     if (!in_range(g, src, dst, k)) return -1;
+    if (!g->weighted) return insert_keys(g, src, dst, k, sym);
     std::vector<Entry> e = expand(src, dst, w, k, sym);
     std::stable_sort(e.begin(), e.end(), [](const Entry &a, const Entry &b) {
         return a.s != b.s ? a.s < b.s : (a.d != b.d ? a.d < b.d : a.order < b.order);
@@ -264,27 +300,57 @@ static bool has(const std::vector<uint32_t> &a, uint32_t x) {
     return std::binary_search(a.begin(), a.end(), x);
 }
 
+// Symmetric store: every triangle {a, b, c} is found once from its two
+// lowest-ranked vertices under the order (degree, id) and credited to its
+// smallest id, which is the reference's owner (tc_kernel.cu:25-30).
+static uint64_t tc_symmetric(const or_graph *g, uint64_t *per_vertex) {
+    const long n = g->n;
+    auto less = [&](uint32_t a, uint32_t b) {
+        const size_t da = g->adj[a].size(), db = g->adj[b].size();
+        return da < db || (da == db && a < b);
+    };
+    std::vector<std::vector<uint32_t>> out(n);
+#pragma omp parallel for schedule(dynamic, 256)
+    for (long u = 0; u < n; ++u)
+        for (uint32_t v : g->adj[u])
+            if (less((uint32_t)u, v)) out[u].push_back(v);  // adj is sorted, so out[u] is sorted
+    std::vector<std::atomic<uint64_t>> cnt(n);
+    for (long u = 0; u < n; ++u) cnt[u].store(0, std::memory_order_relaxed);
+    uint64_t total = 0;
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : total)
+    for (long u = 0; u < n; ++u) {
+        const auto &A = out[u];
+        for (uint32_t v : A) {
+            const auto &Bv = out[v];
+            auto a = A.begin();
+            auto b = Bv.begin();
+            while (a != A.end() && b != Bv.end()) {
+                if (*a < *b) ++a;
+                else if (*b < *a) ++b;
+                else {
+                    const uint32_t o = std::min<uint32_t>(std::min<uint32_t>((uint32_t)u, v), *a);
+                    cnt[o].fetch_add(1, std::memory_order_relaxed);
+                    ++total;
+                    ++a;
+                    ++b;
+                }
+            }
+        }
+    }
+    if (per_vertex)
+        for (long u = 0; u < n; ++u) per_vertex[u] = cnt[u].load();
+    return total;
+}
+
 uint64_t or_tc(const or_graph *g, uint64_t *per_vertex) {
+    if (!g->directed) return tc_symmetric(g, per_vertex);
     const long n = g->n;
     uint64_t total = 0;
 #pragma omp parallel for schedule(dynamic, 64) reduction(+ : total)
     for (long u = 0; u < n; ++u) {
         uint64_t c = 0;
         const auto &Nu = g->adj[u];
-        if (!g->directed) {
-            // symmetric store: |{w in N(u) & N(v) : w > v}| for v in N(u), v > u
-            for (uint32_t v : Nu) {
-                if (v <= (uint32_t)u) continue;
-                const auto &Nv = g->adj[v];
-                auto a = std::upper_bound(Nu.begin(), Nu.end(), v);
-                auto b = std::upper_bound(Nv.begin(), Nv.end(), v);
-                while (a != Nu.end() && b != Nv.end()) {
-                    if (*a < *b) ++a;
-                    else if (*b < *a) ++b;
-                    else { ++c; ++a; ++b; }
-                }
-            }
-        } else {
+        {
             // literal reference formula (tc_kernel.cu:25-65)
             for (uint32_t v : Nu) {
                 if (v <= (uint32_t)u) continue;

@@ -6,6 +6,17 @@ import numpy as np
 import oracle
 
 
+TEST_BUDGET = 2 << 30  # bytes of HBM per test graph (keeps the device mostly free)
+
+
+def make_graph(n: int, **kw):
+    """A libgv graph with a modest HBM budget unless the test sets one."""
+    import gv_b200
+    if "pool_blocks" not in kw and "hbm_budget_bytes" not in kw:
+        kw["hbm_budget_bytes"] = TEST_BUDGET
+    return gv_b200.GraphVine(n, **kw)
+
+
 def rmat_graph(scale: int, edge_factor: int, seed: int):
     """Seeded R-MAT pairs (the generator libgv and the oracle share)."""
     return oracle.rmat_pairs(scale, edge_factor << scale, seed)

@@ -5,14 +5,14 @@ import numpy as np
 import pytest
 
 import oracle
-from tests.helpers import assert_same_adjacency, assert_sound, rmat_graph, sample_existing
+from tests.helpers import assert_same_adjacency, assert_sound, make_graph, rmat_graph, sample_existing
 
 gv_b200 = pytest.importorskip("gv_b200")
 pytestmark = pytest.mark.gpu
 
 
 def build_pair(n, s, d, **kw):
-    g = gv_b200.GraphVine(n, **kw)
+    g = make_graph(n, **kw)
     g.batch_insert(s, d)
     g.synchronize()
     o = oracle.OracleGraph(n, directed=kw.get("directed", False), weighted=kw.get("weighted", False))
@@ -75,8 +75,9 @@ def test_hub_paths_and_block_multiples():
     B = 32
     hub = np.full(9000, 7, np.uint32)
     hub_d = np.setdiff1d(np.arange(n, dtype=np.uint32), [7])[:9000]
-    mult_s = np.repeat(np.arange(100, 110, dtype=np.uint32), 64)
-    mult_d = (np.tile(np.arange(64, dtype=np.uint32), 10) + 1000)
+    # vertices 100..109 get exactly 64 = 2 blocks of neighbours, none shared with the hub
+    mult_s = np.repeat(np.arange(100, 110, dtype=np.uint32), 64) + 12000
+    mult_d = (np.tile(np.arange(64, dtype=np.uint32), 10) + 13000)
     s = np.concatenate([hub, mult_s])
     d = np.concatenate([hub_d, mult_d])
     g, o = build_pair(n, s, d, block_size=B, threads_per_vertex=8)
@@ -85,7 +86,7 @@ def test_hub_paths_and_block_multiples():
     rng = np.random.default_rng(0)
     # delete a random half of the hub plus every edge of vertex 100
     pick = rng.choice(9000, 4500, replace=False)
-    ds = np.concatenate([hub[pick], np.full(64, 100, np.uint32)])
+    ds = np.concatenate([hub[pick], np.full(64, 12100, np.uint32)])
     dd = np.concatenate([hub_d[pick], mult_d[:64]])
     g.batch_delete(ds, dd)
     o.delete(ds, dd)
@@ -93,7 +94,7 @@ def test_hub_paths_and_block_multiples():
     g.synchronize()
     assert_same_adjacency(g, o)
     assert_sound(g)
-    assert g.degrees()[100] == 0
+    assert g.degrees()[12100] == 0
     # a big insert batch into the hub (CTA path of apply)
     add = np.setdiff1d(np.arange(n, dtype=np.uint32), [7])[9000:12000]
     g.batch_insert(np.full(len(add), 7, np.uint32), add)
@@ -121,7 +122,7 @@ def test_weighted_first_occurrence_and_compaction():
     s, d = rmat_graph(9, 8, seed=2)
     rng = np.random.default_rng(1)
     w = rng.uniform(0.1, 1.0, len(s)).astype(np.float32)
-    g = gv_b200.GraphVine(n, directed=True, weighted=True)
+    g = make_graph(n, directed=True, weighted=True)
     g.batch_insert(s, d, w)
     o = oracle.OracleGraph(n, directed=True, weighted=True)
     o.insert(s, d, w)
@@ -144,7 +145,7 @@ def test_bulk_build_from_csr_matches_insert():
     o = oracle.OracleGraph(n)
     o.insert(s, d)
     off, dst, _ = o.export()
-    g = gv_b200.GraphVine(n)
+    g = make_graph(n)
     g.bulk_build(off, dst)
     g.synchronize()
     assert_same_adjacency(g, o)
@@ -153,7 +154,7 @@ def test_bulk_build_from_csr_matches_insert():
 
 def test_empty_and_degenerate_batches():
     n = 256
-    g = gv_b200.GraphVine(n)
+    g = make_graph(n)
     g.batch_insert(np.zeros(0, np.uint32), np.zeros(0, np.uint32))
     loops = np.arange(n, dtype=np.uint32)
     g.batch_insert(loops, loops)
@@ -166,7 +167,7 @@ def test_empty_and_degenerate_batches():
 
 def test_pool_exhaustion_rejects_batch_and_keeps_graph():
     n = 1 << 10
-    g = gv_b200.GraphVine(n, block_size=32, pool_blocks=200)
+    g = make_graph(n, block_size=32, pool_blocks=200)
     s = np.arange(0, 100, dtype=np.uint32)
     d = s + 1
     g.batch_insert(s, d)
@@ -186,7 +187,7 @@ def test_pool_exhaustion_rejects_batch_and_keeps_graph():
 def test_bad_ids_rejected():
     import torch
     n = 64
-    g = gv_b200.GraphVine(n)
+    g = make_graph(n)
     with pytest.raises(gv_b200.GvError) as e:
         g.batch_insert(np.array([1, 70], np.uint32), np.array([2, 3], np.uint32))
     assert "INVALID" in str(e.value)
@@ -202,7 +203,7 @@ def test_bad_ids_rejected():
 
 def test_affected_flags():
     n = 128
-    g = gv_b200.GraphVine(n)
+    g = make_graph(n)
     g.batch_insert(np.array([1, 2], np.uint32), np.array([3, 4], np.uint32))
     a = g.affected()
     assert set(np.nonzero(a)[0]) == {1, 2, 3, 4}
