@@ -744,13 +744,16 @@ __global__ void __launch_bounds__(AN_THREADS) k_tc_count(const unsigned long lon
             const uint32_t per = (tot + TPV - 1) / TPV;
             const uint32_t d0 = min(tot, G.gl * per), d1 = min(tot, d0 + per);
             uint32_t i = corank(A, la, Bv, lb, d0), j = d0 - i;
+            // branch-free merge step: lanes stay converged, only matches diverge
+            uint32_t a = (i < la) ? __ldg(A + i) : 0xFFFFFFFFu;
+            uint32_t bb = (j < lb) ? __ldg(Bv + j) : 0xFFFFFFFFu;
             for (uint32_t d = d0; d < d1; ++d) {
-                if (i < la && (j >= lb || A[i] <= Bv[j])) {
-                    if (j < lb && Bv[j] == A[i]) credit(A[i]);
-                    ++i;
-                } else {
-                    ++j;
-                }
+                const uint32_t ta = (a <= bb) ? 1u : 0u;  // ties consume A first
+                if (a == bb && a != 0xFFFFFFFFu) credit(a);
+                i += ta;
+                j += 1u - ta;
+                a = (i < la) ? __ldg(A + i) : 0xFFFFFFFFu;
+                bb = (j < lb) ? __ldg(Bv + j) : 0xFFFFFFFFu;
             }
             touched = tot;
         }
@@ -805,7 +808,11 @@ struct TcCredit {
     }
 };
 
-__device__ __forceinline__ uint32_t tc_hash(uint32_t x, uint32_t mask) { return (x * 2654435761u) & mask; }
+// Multiplicative hash taking the high bits of the product (the low bits of
+// x * odd depend only on the low bits of x and cluster sorted id lists).
+__device__ __forceinline__ uint32_t tc_hash(uint32_t x, uint32_t mask) {
+    return (uint32_t)(((unsigned long long)(x * 2654435761u) * (mask + 1ull)) >> 32);
+}
 
 // Callers size the table to at least twice the entries, so a free slot is
 // always found; the probe count is bounded by the table size regardless.
@@ -1128,9 +1135,10 @@ gv_status tc_run(gv_graph *g, cudaStream_t s, bool incident, unsigned long long 
     }
     unsigned long long *work = &d.ctl->scratch1;
     cudaMemsetAsync(work, 0, 8, s);
-    const char *merge_env = std::getenv("GV_TC_MERGE");
-    if (merge_env && merge_env[0] == '1') {
-        // merge-path intersection per oriented edge (kept for comparison)
+    const char *hash_env = std::getenv("GV_TC_HASH");
+    if (!(hash_env && hash_env[0] == '1')) {
+        // merge-path intersection per oriented edge (default; hash probe kept
+        // behind GV_TC_HASH=1 for comparison)
         GV_LAUNCH(k_tc_esrc, grid_for(n, 256), 256, 0, s, (const unsigned long long *)b.off, n, b.esrc);
         const unsigned cgrid = grid_for(mplus, AN_THREADS / 8, 148 * 16);
         ProfScope ps(PROF_TC_COUNT, s);
