@@ -56,6 +56,7 @@ SIGNATURES = {
     "gv_last_stat": (C.c_int, [P, C.c_char_p, C.POINTER(C.c_double)]),
     "gv_pagerank": (C.c_int, [P, f32, f32, i32, P, pi32, C.c_int, P]),
     "gv_pagerank_dynamic": (C.c_int, [P, f32, f32, i32, P, pi32, C.c_int, P]),
+    "gv_pagerank_noalloc": (C.c_int, [P, f32, f32, i32, P, pi32, P]),
     "gv_ppr": (C.c_int, [P, u32, f32, f32, i32, P, pi32, C.c_int, P]),
     "gv_tc": (C.c_int, [P, P, pu64, C.c_int, P]),
     "gv_tc_subset": (C.c_int, [P, P, u64, P, C.c_int, P]),
