@@ -1,0 +1,152 @@
+"""Pins the oracle (and libgv) against the reference implementation itself.
+
+oracle/_ref/gv_ref_harness is the reference's own CUDA sources (sajidanis/GV)
+compiled with a small driver (oracle/ref_harness.cu, built by
+oracle/ref_build.py).  It is fed only inputs inside the regime where the
+reference is well defined and stays in bounds:
+  * every vertex keeps fewer than 128 entries (one edge block, never full),
+    so compaction never frees a block and never meets a full last block;
+  * batches have no self-loops, no duplicates, no pair already in the graph,
+    and never touch vertex n-1 (find_affected_nodes indexes by 1-based id);
+  * deletes never remove a vertex's last edge;
+  * compaction runs last; PageRank and TC run on delete-free or compacted graphs.
+BC is not compared: the reference's BC indexes with 1-based ids.
+The reference reserves half of the GPU's memory for its pool with an
+unchecked cudaMalloc, so the test needs that much free memory first.
+"""
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oracle
+from tests.helpers import make_graph, sorted_adjacency
+
+ROOT = Path(__file__).resolve().parent.parent
+HARNESS = ROOT / "oracle" / "_ref" / "gv_ref_harness"
+
+pytestmark = pytest.mark.gpu
+
+
+def _write_mtx(path, n, pairs):
+    with open(path, "w") as f:
+        f.write(f"{n} {n} {len(pairs)}\n")
+        for a, b in pairs:
+            f.write(f"{a + 1} {b + 1}\n")
+
+
+def _read_csr(path):
+    with open(path, "rb") as f:
+        n = int(np.frombuffer(f.read(8), np.uint64)[0])
+        off = np.frombuffer(f.read(8 * (n + 1)), np.uint64).copy()
+        dst = np.frombuffer(f.read(4 * int(off[-1])), np.uint32).copy()
+    return off, dst
+
+
+def _read_vec(path, dtype):
+    with open(path, "rb") as f:
+        n = int(np.frombuffer(f.read(8), np.uint64)[0])
+        return np.frombuffer(f.read(np.dtype(dtype).itemsize * n), dtype).copy()
+
+
+def _workload(n, rng):
+    """Uniform base graph, an insert batch of new pairs, a delete batch of
+    existing pairs, all inside the regime above."""
+    usable = n - 1  # vertex n-1 is never touched
+    edges = set()
+    while len(edges) < 8 * n:
+        a, b = rng.integers(0, usable, 2)
+        if a != b:
+            edges.add((min(a, b), max(a, b)))
+    deg = np.zeros(n, np.int64)
+    for a, b in edges:
+        deg[a] += 1
+        deg[b] += 1
+    ins = set()
+    while len(ins) < n // 2:
+        a, b = rng.integers(0, usable, 2)
+        p = (min(a, b), max(a, b))
+        if a != b and p not in edges and p not in ins and deg[a] < 100 and deg[b] < 100:
+            ins.add(p)
+            deg[a] += 1
+            deg[b] += 1
+    allp = sorted(edges | ins)
+    dele = []
+    for i in rng.permutation(len(allp))[: n // 4]:
+        a, b = allp[i]
+        if deg[a] > 1 and deg[b] > 1:
+            dele.append((a, b))
+            deg[a] -= 1
+            deg[b] -= 1
+    assert deg.max() < 128
+    return sorted(edges), sorted(ins), sorted(dele)
+
+
+def _same_sets(off, dst, ooff, odst):
+    assert np.array_equal(off, ooff), "degrees differ"
+    assert np.array_equal(sorted_adjacency(off, dst)[0], odst), "neighbour sets differ"
+
+
+def test_reference_matches_oracle_and_libgv(tmp_path):
+    if not HARNESS.exists():
+        pytest.skip("reference harness not built (oracle/ref_build.py)")
+    import torch
+    free, total = torch.cuda.mem_get_info()
+    if free < 0.55 * total:
+        pytest.skip("the reference needs half of the GPU's memory free")
+    n = 2048
+    rng = np.random.default_rng(20261203)
+    base, ins, dele = _workload(n, rng)
+    _write_mtx(tmp_path / "g.mtx", n, base)
+    _write_mtx(tmp_path / "i.mtx", n, ins)
+    _write_mtx(tmp_path / "d.mtx", n, dele)
+    t = tmp_path
+    (t / "script").write_text(
+        f"graph {t}/g.mtx\ninsert {t}/i.mtx\ndump {t}/a1.bin\npagerank 0.85 1e-6 100 {t}/pr1.bin\ntc {t}/tc1.bin\n"
+        f"delete {t}/d.mtx\ncompact\ndump {t}/a2.bin\npagerank 0.85 1e-6 100 {t}/pr2.bin\ntc {t}/tc2.bin\n")
+    r = subprocess.run([str(HARNESS), str(t / "script")], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+
+    o = oracle.OracleGraph(n)
+    g = make_graph(n)
+    bs, bd = np.array(base, np.uint32).T
+    is_, id_ = np.array(ins, np.uint32).T
+    ds, dd = np.array(dele, np.uint32).T
+    for gr in (o, g):
+        getattr(gr, "insert" if gr is o else "batch_insert")(bs, bd)
+        getattr(gr, "insert" if gr is o else "batch_insert")(is_, id_)
+
+    # adjacency after the insert batch: reference == oracle == libgv
+    off, dst = _read_csr(t / "a1.bin")
+    ooff, odst, _ = o.export()
+    _same_sets(off, dst, ooff, odst)
+    goff, gdst, _ = g.export_csr()
+    _same_sets(goff, gdst, ooff, odst)
+    # PageRank: each side stops on its own fp residual, so compare within the
+    # distance of an eps-converged iterate to the fixed point
+    pr_ref = _read_vec(t / "pr1.bin", np.float32)
+    xo, _ = o.pagerank(0.85, 1e-6, 100)
+    assert np.abs(pr_ref - xo).sum() < 2 * 1e-6 * 0.85 / 0.15
+    # triangle counts: the reference counts in float, owner = smallest id
+    tc_ref = _read_vec(t / "tc1.bin", np.float32)
+    opv, _ = o.tc()
+    assert np.array_equal(tc_ref.astype(np.uint64), opv)
+    gpv, _ = g.static_tc()
+    assert np.array_equal(gpv, opv)
+
+    o.delete(ds, dd)
+    g.batch_delete(ds, dd)
+    g.compaction()
+    g.synchronize()
+    off, dst = _read_csr(t / "a2.bin")
+    ooff, odst, _ = o.export()
+    _same_sets(off, dst, ooff, odst)
+    goff, gdst, _ = g.export_csr()
+    _same_sets(goff, gdst, ooff, odst)
+    pr_ref = _read_vec(t / "pr2.bin", np.float32)
+    xo, _ = o.pagerank(0.85, 1e-6, 100)
+    assert np.abs(pr_ref - xo).sum() < 2 * 1e-6 * 0.85 / 0.15
+    tc_ref = _read_vec(t / "tc2.bin", np.float32)
+    assert np.array_equal(tc_ref.astype(np.uint64), o.tc()[0])
+    g.close()
