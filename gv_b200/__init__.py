@@ -118,6 +118,36 @@ def gen_uniform(n: int, count: int, seed: int, device=None, stream=None):
     return src, dst
 
 
+def autotune(num_vertices: int, src0, dst0, batches, *, device: int = 0, hbm_budget_bytes: int = 0,
+             max_batch_pairs: int = 1 << 20):
+    """Times edge-block size {32, 64, 128} x threads-per-vertex {4, 8, 16, 32}
+    on a sample workload (build from src0/dst0, one window of `batches` as in
+    GraphVine.batch_run, one PageRank).  Returns (best dict, [results])."""
+    L = _lib.lib()
+    cfg = gv_config()
+    _check(L.gv_config_init(C.byref(cfg), num_vertices), "gv_config_init")
+    cfg.device = device
+    cfg.hbm_budget_bytes = hbm_budget_bytes
+    cfg.max_batch_pairs = max_batch_pairs
+    descs, srcs, dsts, off = [], [], [], 0
+    for ins_s, ins_d, del_s, del_d in batches:
+        descs.append((off, len(ins_s), len(del_s)))
+        srcs += [np.asarray(ins_s, np.uint32), np.asarray(del_s, np.uint32)]
+        dsts += [np.asarray(ins_d, np.uint32), np.asarray(del_d, np.uint32)]
+        off += len(ins_s) + len(del_s)
+    bs, bd = np.concatenate(srcs), np.concatenate(dsts)
+    s0, d0 = np.ascontiguousarray(src0, np.uint32), np.ascontiguousarray(dst0, np.uint32)
+    arr = (_lib.gv_batch_desc * len(descs))(*[_lib.gv_batch_desc(o, i, d) for o, i, d in descs])
+    res = (_lib.gv_tune_result * 12)()
+    nres = C.c_uint32(12)
+    best = gv_config()
+    _check(L.gv_autotune(C.byref(cfg), s0.ctypes.data, d0.ctypes.data, len(s0), arr, len(descs), bs.ctypes.data,
+                         bd.ctypes.data, GV_MEM_HOST, res, C.byref(nres), C.byref(best)), "gv_autotune")
+    results = [{"block_size": r.block_size, "threads_per_vertex": r.threads_per_vertex, "update_ms": r.update_ms,
+                "pagerank_ms": r.pagerank_ms} for r in res[:nres.value]]
+    return {"block_size": best.block_size, "threads_per_vertex": best.threads_per_vertex}, results
+
+
 class GraphVine:
     """A dynamic graph resident on one GPU (edge-block CBT store)."""
 
@@ -193,6 +223,45 @@ class GraphVine:
 
     def synchronize(self, stream=None) -> None:
         _check(_lib.lib().gv_synchronize(self._h, _stream(stream)), "gv_synchronize")
+
+    # -- batched updates and queries ----------------------------------------
+    def batch_run(self, batches, compact: bool = True, graph: bool = False, stream=None) -> None:
+        """Apply a window of batches [(ins_src, ins_dst, del_src, del_dst), ...]
+        or (descs, src, dst) already laid out; equal to applying them in order."""
+        if isinstance(batches, tuple) and len(batches) == 3 and not isinstance(batches[0], tuple):
+            descs, src, dst = batches
+        else:
+            descs, srcs, dsts, off = [], [], [], 0
+            for ins_s, ins_d, del_s, del_d in batches:
+                descs.append((off, len(ins_s), len(del_s)))
+                srcs += [np.asarray(ins_s, np.uint32), np.asarray(del_s, np.uint32)]
+                dsts += [np.asarray(ins_d, np.uint32), np.asarray(del_d, np.uint32)]
+                off += len(ins_s) + len(del_s)
+            src, dst = np.concatenate(srcs), np.concatenate(dsts)
+        arr = (_lib.gv_batch_desc * len(descs))(*[_lib.gv_batch_desc(o, i, d) for o, i, d in descs])
+        ps, mem, k1 = _ptr(src, np.uint32)
+        pd, _, k2 = _ptr(dst, np.uint32)
+        flags = (_lib.GV_BATCH_COMPACT if compact else 0) | (_lib.GV_BATCH_GRAPH if graph else 0)
+        _check(_lib.lib().gv_batch_run(self._h, arr, len(descs), ps, pd, mem, flags, _stream(stream)), "gv_batch_run")
+        self._keep = (k1, k2, arr)
+
+    def ppr_batch(self, sources, alpha: float = 0.85, epsilon: float = 1e-6, max_iter: int = 100, out=None,
+                  stream=None):
+        """k <= 32 personalised PageRank queries at once; returns (x[n, k], sweeps)."""
+        s = np.ascontiguousarray(sources, dtype=np.uint32)
+        k = len(s)
+        x = np.empty((self.n, k), np.float32) if out is None else out
+        px, mem, _ = _ptr(x, np.float32)
+        sw = C.c_int32()
+        if mem == GV_MEM_DEVICE:
+            import torch
+            sd = torch.from_numpy(s.view(np.int32)).to(x.device)
+            ps = sd.data_ptr()
+        else:
+            ps = s.ctypes.data
+        _check(_lib.lib().gv_ppr_batch(self._h, ps, k, alpha, epsilon, max_iter, px, C.byref(sw), mem,
+                                       _stream(stream)), "gv_ppr_batch")
+        return x, sw.value
 
     # -- facts -------------------------------------------------------------
     def num_edges(self) -> int:

@@ -30,6 +30,17 @@ class gv_config(C.Structure):
     ]
 
 
+class gv_batch_desc(C.Structure):
+    _fields_ = [("offset", C.c_uint64), ("n_insert", C.c_uint32), ("n_delete", C.c_uint32)]
+
+
+class gv_tune_result(C.Structure):
+    _fields_ = [("block_size", C.c_uint32), ("threads_per_vertex", C.c_uint32), ("update_ms", C.c_float),
+                ("pagerank_ms", C.c_float)]
+
+
+GV_BATCH_COMPACT, GV_BATCH_GRAPH = 1, 2
+
 P = C.c_void_p
 u32, u64, i32, f32 = C.c_uint32, C.c_uint64, C.c_int32, C.c_float
 pu32, pu64, pi32, pf32, pu8 = C.POINTER(C.c_uint32), C.POINTER(C.c_uint64), C.POINTER(C.c_int32), C.POINTER(C.c_float), C.POINTER(C.c_uint8)
@@ -70,6 +81,10 @@ SIGNATURES = {
     "gv_profile_query": (C.c_int, [C.c_char_p, C.POINTER(C.c_double), pu64]),
     "gv_last_error_string": (C.c_char_p, []),
     "gv_version": (C.c_char_p, []),
+    "gv_batch_run": (C.c_int, [P, C.POINTER(gv_batch_desc), u32, P, P, C.c_int, u32, P]),
+    "gv_ppr_batch": (C.c_int, [P, P, u32, f32, f32, i32, P, pi32, C.c_int, P]),
+    "gv_autotune": (C.c_int, [C.POINTER(gv_config), P, P, u64, C.POINTER(gv_batch_desc), u32, P, P, C.c_int,
+                              C.POINTER(gv_tune_result), pu32, C.POINTER(gv_config)]),
     "gv_gen_rmat": (C.c_int, [u32, u64, u64, u64, P, P, C.c_int, P]),
     "gv_gen_uniform": (C.c_int, [u32, u64, u64, P, P, C.c_int, P]),
 }

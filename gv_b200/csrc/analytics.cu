@@ -18,6 +18,7 @@
 #include <cmath>
 #include <cstring>
 #include <vector>
+#include "../../include/gv_batch.h"
 #include "store.cuh"
 #include "group.cuh"
 #include "prims.cuh"
@@ -1626,12 +1627,220 @@ __global__ void __launch_bounds__(AN_THREADS) k_wpr_grad(DevGraph g, const unsig
     }
 }
 
+// ------------------------------------------------------ batched PPR queries
+// k <= 32 personalised PageRank queries share every adjacency read: lane j
+// of a warp owns query j, values are vertex-major (x[v * k + j]), and one
+// coalesced load of a neighbour's k contributions serves all queries.
+struct PprBatch {
+    uint32_t k;
+    const uint32_t *sources;  // device, k
+    float alpha;
+    const float *gather;      // contributions (n * k)
+    const float *xold;
+    float *xnew, *cnew;
+    double *partial;          // [grid][32]
+    const int *state;
+};
+
+__device__ __forceinline__ void ppr_finish(const DevGraph &g, const PprBatch &a, uint32_t v, float acc, uint32_t lane,
+                                           double &res) {
+    if (lane >= a.k) return;
+    const float base = (a.sources[lane] == v) ? (1.0f - a.alpha) : 0.f;
+    const float xv = base + a.alpha * acc;
+    const size_t at = (size_t)v * a.k + lane;
+    a.xnew[at] = xv;
+    const uint32_t d = g.vtx[v].z;
+    a.cnew[at] = d ? xv / (float)d : 0.f;
+    res += (double)fabsf(xv - a.xold[at]);
+}
+
+__global__ void __launch_bounds__(AN_THREADS) k_ppr_light(DevGraph g, PprBatch a) {
+    __shared__ double red[AN_THREADS / 32][32];
+    if (a.state[0]) return;
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double res = 0.0;
+    const uint32_t nw = gridDim.x * (AN_THREADS / 32);
+    for (uint32_t v = blockIdx.x * (AN_THREADS / 32) + warp; v < g.n; v += nw) {
+        const uint4 rec = g.vtx[v];
+        const uint32_t fill = rec.y;
+        if (fill > LIGHT_FILL) continue;  // items path
+        const uint32_t nb = blocks_for(fill, g.logB);
+        const uint32_t my_blk = item_block(g, rec, 0, nb);  // lane k holds block k (nb <= 8)
+        float acc = 0.f;
+        for (uint32_t e0 = 0; e0 < fill; e0 += 32) {
+            const uint32_t e = e0 + lane;
+            const uint32_t pb = __shfl_sync(GV_FULL_MASK, my_blk, (e >> g.logB) & 31u);
+            const uint32_t u = (e < fill) ? g.pool[((size_t)pb << g.logB) + (e & (g.B - 1))] : GV_TOMB;
+            const uint32_t cnt = min(32u, fill - e0);
+#pragma unroll 8
+            for (uint32_t j = 0; j < cnt; ++j) {
+                const uint32_t w = __shfl_sync(GV_FULL_MASK, u, j);
+                if (w != GV_TOMB && lane < a.k) acc += __ldg(a.gather + (size_t)w * a.k + lane);
+            }
+        }
+        ppr_finish(g, a, v, acc, lane, res);
+    }
+    red[warp][lane] = res;
+    __syncthreads();
+    if (warp == 0) {
+        double t = 0.0;
+        for (int w = 0; w < AN_THREADS / 32; ++w) t += red[w][lane];
+        a.partial[(size_t)blockIdx.x * 32 + lane] = t;
+    }
+}
+
+__global__ void __launch_bounds__(AN_THREADS) k_ppr_items(DevGraph g, PprBatch a, Items it, float *__restrict__ ipart) {
+    if (a.state[0]) return;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t nw = gridDim.x * (AN_THREADS / 32);
+    for (uint32_t i = blockIdx.x * (AN_THREADS / 32) + (threadIdx.x >> 5); i < it.nitems; i += nw) {
+        const uint32_t v = it.item_vertex[i];
+        const uint32_t c = i - it.item_first[v];
+        const uint4 rec = g.vtx[v];
+        const uint32_t fill = rec.y, nb = blocks_for(fill, g.logB);
+        const uint32_t kb0 = c << 5;
+        const uint32_t my_blk = item_block(g, rec, kb0, nb);
+        const uint32_t e0 = kb0 << g.logB, e1 = min(fill, (kb0 + 32) << g.logB);
+        float acc = 0.f;
+        for (uint32_t q0 = e0; q0 < e1; q0 += 32) {
+            const uint32_t el = q0 - e0 + lane;
+            const uint32_t pb = __shfl_sync(GV_FULL_MASK, my_blk, (el >> g.logB) & 31u);
+            const uint32_t u = (q0 + lane < e1) ? g.pool[((size_t)pb << g.logB) + (el & (g.B - 1))] : GV_TOMB;
+            const uint32_t cnt = min(32u, e1 - q0);
+#pragma unroll 8
+            for (uint32_t j = 0; j < cnt; ++j) {
+                const uint32_t w = __shfl_sync(GV_FULL_MASK, u, j);
+                if (w != GV_TOMB && lane < a.k) acc += __ldg(a.gather + (size_t)w * a.k + lane);
+            }
+        }
+        ipart[(size_t)i * 32 + lane] = acc;
+    }
+}
+
+__global__ void __launch_bounds__(AN_THREADS) k_ppr_items_fin(DevGraph g, PprBatch a, Items it,
+                                                              const float *__restrict__ ipart, uint32_t part_base) {
+    __shared__ double red[AN_THREADS / 32][32];
+    if (a.state[0]) return;
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double res = 0.0;
+    const uint32_t nw = gridDim.x * (AN_THREADS / 32);
+    for (uint32_t m = blockIdx.x * (AN_THREADS / 32) + warp; m < it.nmulti; m += nw) {
+        const uint32_t v = it.multi[m];
+        float acc = 0.f;
+        for (uint32_t i = it.item_first[v]; i < it.item_first[v + 1]; ++i) acc += ipart[(size_t)i * 32 + lane];
+        ppr_finish(g, a, v, acc, lane, res);
+    }
+    red[warp][lane] = res;
+    __syncthreads();
+    if (warp == 0) {
+        double t = 0.0;
+        for (int w = 0; w < AN_THREADS / 32; ++w) t += red[w][lane];
+        a.partial[(size_t)(part_base + blockIdx.x) * 32 + lane] = t;
+    }
+}
+
+// Per query: sum of its residual partials; converged when every query is.
+__global__ void k_ppr_done(const double *__restrict__ partial, uint32_t nparts, uint32_t k, float eps, int *state) {
+    __shared__ int all_ok;
+    if (state[0]) return;
+    if (threadIdx.x == 0) all_ok = 1;
+    __syncthreads();
+    if (threadIdx.x < k) {
+        double t = 0.0;
+        for (uint32_t p = 0; p < nparts; ++p) t += partial[(size_t)p * 32 + threadIdx.x];
+        if (!(t < (double)eps)) atomicAnd(&all_ok, 0);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        state[1] += 1;
+        if (all_ok) state[0] = 1;
+    }
+}
+
+__global__ void k_ppr_init(DevGraph g, const uint32_t *__restrict__ sources, uint32_t k, float *__restrict__ x,
+                           float *__restrict__ c) {
+    const size_t total = (size_t)g.n * k;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        const uint32_t v = (uint32_t)(i / k), j = (uint32_t)(i % k);
+        const float xv = (sources[j] == v) ? 1.f : 0.f;
+        x[i] = xv;
+        const uint32_t d = g.vtx[v].z;
+        c[i] = d ? xv / (float)d : 0.f;
+    }
+}
+
+gv_status ppr_batch_impl(gv_graph *g, const uint32_t *sources, uint32_t k, float alpha, float eps, int max_iter,
+                         float *x_out, int32_t *sweeps, int mem, cudaStream_t s) {
+    DevGraph d = g->d;
+    const uint32_t n = d.n;
+    const size_t vec = (size_t)n * k * sizeof(float);
+    const uint32_t nparts = PULL_GRID + FIN_GRID;
+    const size_t bytes = 4 * vec + (size_t)nparts * 32 * 8 + 64 + 128 + 256 * 3;
+    char *p = (char *)analytics_scratch(g, bytes);
+    if (!p) return GV_ERR_NOMEM;
+    float *x[2] = {(float *)p, (float *)(p + vec)};
+    float *c[2] = {(float *)(p + 2 * vec), (float *)(p + 3 * vec)};
+    double *partial = (double *)(p + 4 * vec);
+    int *state = (int *)(p + 4 * vec + (size_t)nparts * 32 * 8);
+    uint32_t *dsrc = (uint32_t *)(p + 4 * vec + (size_t)nparts * 32 * 8 + 64);
+    unsigned long long *nmulti = (unsigned long long *)(dsrc + 32);
+    cudaMemcpyAsync(dsrc, sources, k * 4, mem == GV_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s);
+    Items it{};
+    float *ip_unused = nullptr;
+    gv_status st = build_items(g, s, nmulti, &it, &ip_unused);
+    if (st != GV_OK) return st;
+    float *ipart = nullptr;
+    if (it.nitems) {
+        ipart = (float *)aux_scratch(g, 3, (size_t)it.nitems * 32 * sizeof(float));
+        if (!ipart) return GV_ERR_NOMEM;
+    }
+    cudaMemsetAsync(state, 0, 16, s);
+    cudaMemsetAsync(partial, 0, (size_t)nparts * 32 * 8, s);
+    GV_LAUNCH(k_ppr_init, grid_for((uint64_t)n * k, 256, 148 * 16), 256, 0, s, d, (const uint32_t *)dsrc, k, x[0], c[0]);
+    int h_state[2] = {0, 0};
+    int launched = 0, cur = 0;
+    cudaError_t e = cudaSuccess;
+    while (launched < max_iter) {
+        const int chunk = std::min(8, max_iter - launched);
+        for (int i = 0; i < chunk; ++i) {
+            PprBatch a{k, dsrc, alpha, c[cur], x[cur], x[cur ^ 1], c[cur ^ 1], partial, state};
+            ProfScope ps(PROF_PULL, s);
+            GV_LAUNCH(k_ppr_light, PULL_GRID, AN_THREADS, 0, s, d, a);
+            if (it.nitems) {
+                GV_LAUNCH(k_ppr_items, PULL_GRID, AN_THREADS, 0, s, d, a, it, ipart);
+                GV_LAUNCH(k_ppr_items_fin, FIN_GRID, AN_THREADS, 0, s, d, a, it, (const float *)ipart, PULL_GRID);
+            }
+            GV_LAUNCH(k_ppr_done, 1, 32, 0, s, (const double *)partial, nparts, k, eps, state);
+            cur ^= 1;
+        }
+        launched += chunk;
+        e = cudaMemcpyAsync(h_state, state, 8, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return cuda_status(e, "ppr batch");
+        if (h_state[0]) break;
+    }
+    if (sweeps) *sweeps = h_state[1];
+    e = cudaMemcpyAsync(x_out, x[h_state[1] & 1], vec, mem == GV_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    return cuda_status(e, "ppr batch");
+}
+
 }  // namespace
 }  // namespace gv
 
 using namespace gv;
 
 extern "C" {
+
+gv_status gv_ppr_batch(gv_graph *g, const uint32_t *sources, uint32_t k, float alpha, float epsilon, int32_t max_iter,
+                       float *x_out, int32_t *sweeps, int mem, void *stream) {
+    if (!g || !sources || !x_out || k == 0 || k > 32 || max_iter < 0) { set_error("bad argument"); return GV_ERR_INVALID; }
+    if (g->cfg.directed) { set_error("PageRank pull needs an undirected (symmetric) store"); return GV_ERR_STATE; }
+    if (mem == GV_MEM_HOST)
+        for (uint32_t j = 0; j < k; ++j)
+            if (sources[j] >= g->d.n) { set_error("source out of range"); return GV_ERR_INVALID; }
+    return ppr_batch_impl(g, sources, k, alpha, epsilon, max_iter, x_out, sweeps, mem, (cudaStream_t)stream);
+}
 
 gv_status gv_pagerank(gv_graph *g, float alpha, float epsilon, int32_t max_iter, float *x_out, int32_t *sweeps,
                       int mem, void *stream) {

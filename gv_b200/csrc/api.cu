@@ -231,6 +231,8 @@ void prof_collect_locked() {
 
 int prof_begin(int slot, cudaStream_t s) {
     if (!prof_on.load(std::memory_order_relaxed)) return -1;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return -1;
     std::lock_guard<std::mutex> lk(prof_mu);
     ProfRec r{slot, prof_event(), prof_event()};
     cudaEventRecord(r.a, s);
@@ -381,6 +383,7 @@ fail:
 gv_status gv_destroy(gv_graph *g) {
     if (!g) return GV_OK;
     DeviceGuard dg(g->cfg.device);
+    release_window(g);
     DevGraph &d = g->d;
     dfree(d.vtx); dfree(d.left); dfree(d.right); dfree(d.pred); dfree(d.bcount); dfree(d.owner);
     dfree(d.pool); dfree(d.wpool); dfree(d.free_stack); dfree(d.affected); dfree(d.dirty);

@@ -1,0 +1,339 @@
+// Batched updates: many update batches of uneven size applied as one window.
+//
+// Under set semantics the presence of a pair after a sequence of updates is
+// decided by the last update that names it.  A window of batches is
+// therefore expanded into keys in window order, stable-sorted once, reduced
+// to the last operation per pair, and applied as one set-union insert of the
+// net inserts plus one set-difference delete of the net deletes (the two
+// sets are disjoint, so their order does not matter).  Every touched
+// vertex's blocks are scanned once per window instead of once per batch and
+// per operation type, and compaction runs once at the end.  The final graph
+// equals applying the batches one by one; tests/test_batch_gpu.py checks it.
+//
+// With GV_BATCH_GRAPH the window's device work is captured into a CUDA graph
+// and launched as one graph.
+//
+// The reference applies one batch per host call with several host round
+// trips each (src/dynamicStructure/graphvine.cu:222-451).
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <vector>
+#include "../../include/gv_batch.h"
+#include "store.cuh"
+#include "group.cuh"
+#include "prims.cuh"
+#include "launch.hpp"
+
+namespace gv {
+namespace {
+
+constexpr int NET_THREADS = 256;
+constexpr int NET_ITEMS = 8;
+constexpr int NET_TILE = NET_THREADS * NET_ITEMS;
+
+// Window expansion: op i is an insert when it lies in its batch's insert
+// slice.  Keys as k_expand; the value carries the op type (1 = insert).
+__global__ void k_window_expand(const uint32_t *__restrict__ src, const uint32_t *__restrict__ dst, uint64_t total,
+                                const unsigned long long *__restrict__ bstart,
+                                const unsigned long long *__restrict__ bsplit, uint32_t nb, int sym, uint32_t n,
+                                uint32_t bitsn, unsigned long long *__restrict__ keys, uint32_t *__restrict__ vals,
+                                uint8_t *__restrict__ affected, Ctl *ctl) {
+    const unsigned long long sent = (bitsn >= 32) ? ~0ull : ((1ull << (2 * bitsn)) - 1ull);
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t lo = 0, hi = nb;  // last batch with bstart <= i
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (bstart[mid] <= i) lo = mid; else hi = mid;
+        }
+        const uint32_t type = (i < bsplit[lo]) ? 1u : 0u;
+        const uint32_t s = src[i], d = dst[i];
+        const bool bad = (s >= n) || (d >= n);
+        if (bad) {
+            atomicOr(&ctl->status, GV_DEV_ERR_RANGE);
+            ctl->batch_abort = 1;
+        }
+        const bool drop = bad || (s == d);
+        if (!drop) {
+            affected[s] = 1;
+            affected[d] = 1;
+        }
+        if (sym) {
+            keys[2 * i] = drop ? sent : (((unsigned long long)s << bitsn) | d);
+            keys[2 * i + 1] = drop ? sent : (((unsigned long long)d << bitsn) | s);
+            vals[2 * i] = type;
+            vals[2 * i + 1] = type;
+        } else {
+            keys[i] = drop ? sent : (((unsigned long long)s << bitsn) | d);
+            vals[i] = type;
+        }
+    }
+}
+
+// keep = last of its run of equal keys, not the sentinel, and of type `want`
+__device__ __forceinline__ bool net_keep(const unsigned long long *K, const uint32_t *V, uint64_t i, uint64_t N,
+                                         unsigned long long sent, uint32_t want) {
+    if (i >= N) return false;
+    const unsigned long long k = K[i];
+    if (k == sent) return false;
+    if (i + 1 < N && K[i + 1] == k) return false;
+    return V[i] == want;
+}
+
+__global__ void __launch_bounds__(NET_THREADS) k_net_count(const unsigned long long *__restrict__ K,
+                                                           const uint32_t *__restrict__ V, uint64_t N,
+                                                           unsigned long long sent, uint32_t want,
+                                                           uint32_t *__restrict__ tile_cnt) {
+    __shared__ uint32_t wt[33];
+    const uint64_t base = (uint64_t)blockIdx.x * NET_TILE + (uint64_t)threadIdx.x * NET_ITEMS;
+    uint32_t c = 0;
+#pragma unroll
+    for (int j = 0; j < NET_ITEMS; ++j) c += net_keep(K, V, base + j, N, sent, want) ? 1u : 0u;
+    const uint32_t tot = cta_sum<uint32_t, NET_THREADS>(c, wt);
+    if (threadIdx.x == 0) tile_cnt[blockIdx.x] = tot;
+}
+
+__global__ void __launch_bounds__(NET_THREADS) k_net_write(const unsigned long long *__restrict__ K,
+                                                           const uint32_t *__restrict__ V, uint64_t N,
+                                                           unsigned long long sent, uint32_t want,
+                                                           const uint32_t *__restrict__ tile_off,
+                                                           unsigned long long *__restrict__ out) {
+    __shared__ uint32_t wt[33];
+    const uint64_t base = (uint64_t)blockIdx.x * NET_TILE + (uint64_t)threadIdx.x * NET_ITEMS;
+    bool keep[NET_ITEMS];
+    uint32_t c = 0;
+#pragma unroll
+    for (int j = 0; j < NET_ITEMS; ++j) {
+        keep[j] = net_keep(K, V, base + j, N, sent, want);
+        c += keep[j] ? 1u : 0u;
+    }
+    uint32_t tot;
+    uint32_t p = cta_excl_scan<uint32_t, NET_THREADS>(c, wt, tot) + tile_off[blockIdx.x];
+#pragma unroll
+    for (int j = 0; j < NET_ITEMS; ++j)
+        if (keep[j]) out[p++] = K[base + j];
+}
+
+// Fills out[count, N) with the sentinel so the compacted keys stay sorted.
+__global__ void k_fill_sent(unsigned long long *__restrict__ out, const uint32_t *__restrict__ count, uint64_t N,
+                            unsigned long long sent) {
+    const uint64_t c = *count;
+    for (uint64_t i = c + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (uint64_t)gridDim.x * blockDim.x)
+        out[i] = sent;
+}
+
+struct WindowBufs {
+    uint64_t cap_src = 0, cap_dst = 0, cap_vals = 0, cap_vals_alt = 0, cap_bstart = 0, cap_bsplit = 0, cap_tiles = 0;
+    uint32_t *src = nullptr, *dst = nullptr;  // device copies of host windows
+    uint32_t *vals = nullptr, *vals_alt = nullptr;
+    unsigned long long *bstart = nullptr, *bsplit = nullptr;
+    uint32_t *tile_cnt = nullptr;  // tiles + 1 (the last slot holds the count)
+    cudaStream_t cap_stream = nullptr;
+};
+
+std::mutex win_mu;
+std::vector<std::pair<gv_graph *, std::unique_ptr<WindowBufs>>> g_windows;
+
+WindowBufs &window_bufs(gv_graph *g) {
+    std::lock_guard<std::mutex> lk(win_mu);
+    for (auto &w : g_windows)
+        if (w.first == g) return *w.second;
+    g_windows.emplace_back(g, std::make_unique<WindowBufs>());
+    return *g_windows.back().second;
+}
+
+template <typename T>
+gv_status grow(T **p, uint64_t &cap, uint64_t want, size_t elem, const char *what) {
+    if (want <= cap && *p) return GV_OK;
+    if (*p) cudaFree((void *)*p);
+    *p = nullptr;
+    cap = 0;
+    cudaError_t e = cudaMalloc((void **)p, want * elem);
+    if (e != cudaSuccess) return cuda_status(e, what);
+    cap = want;
+    return GV_OK;
+}
+
+}  // namespace
+
+void release_window(gv_graph *g) {
+    std::lock_guard<std::mutex> lk(win_mu);
+    for (size_t i = 0; i < g_windows.size(); ++i)
+        if (g_windows[i].first == g) {
+            WindowBufs &b = *g_windows[i].second;
+            for (void *p : {(void *)b.src, (void *)b.dst, (void *)b.vals, (void *)b.vals_alt, (void *)b.bstart,
+                            (void *)b.bsplit, (void *)b.tile_cnt})
+                if (p) cudaFree(p);
+            if (b.cap_stream) cudaStreamDestroy(b.cap_stream);
+            g_windows.erase(g_windows.begin() + i);
+            return;
+        }
+}
+
+// Enqueues the device work of one window (no allocation, no host sync).
+static void enqueue_window(gv_graph *g, WindowBufs &wb, uint32_t nb, const uint32_t *dsrc, const uint32_t *ddst,
+                           uint64_t total, uint32_t flags, cudaStream_t s) {
+    const bool sym = !g->cfg.directed;
+    const uint64_t E = sym ? 2 * total : total;
+    BatchScratch &bs = g->bs;
+    const unsigned long long sent = (g->bitsn >= 32) ? ~0ull : ((1ull << (2 * g->bitsn)) - 1ull);
+    GV_LAUNCH(k_window_expand, grid_for(total, 256, 148 * 16), 256, 0, s, dsrc, ddst, total,
+              (const unsigned long long *)wb.bstart, (const unsigned long long *)wb.bsplit, nb, sym ? 1 : 0, g->d.n,
+              g->bitsn, bs.keys, wb.vals, g->d.affected, g->d.ctl);
+    const int which = radix_sort_u64(bs.keys, bs.keys_alt, wb.vals, wb.vals_alt, E, 2 * (int)g->bitsn, bs.rs_counts,
+                                     bs.scan_tmp, s);
+    const unsigned long long *K = which ? bs.keys_alt : bs.keys;
+    const uint32_t *V = which ? wb.vals_alt : wb.vals;
+    unsigned long long *out = which ? bs.keys : bs.keys_alt;
+    const unsigned ntiles = (unsigned)((E + NET_TILE - 1) / NET_TILE);
+    uint32_t *count = wb.tile_cnt + ntiles;
+    for (uint32_t want = 1;; want = 0) {  // net inserts, then net deletes
+        GV_LAUNCH(k_net_count, ntiles, NET_THREADS, 0, s, K, V, E, sent, want, wb.tile_cnt);
+        scan_exclusive_u32(wb.tile_cnt, wb.tile_cnt, ntiles, count, bs.scan_tmp, s);
+        GV_LAUNCH(k_net_write, ntiles, NET_THREADS, 0, s, K, V, E, sent, want, (const uint32_t *)wb.tile_cnt, out);
+        GV_LAUNCH(k_fill_sent, grid_for(E, 256, 148 * 16), 256, 0, s, out, (const uint32_t *)count, E, sent);
+        apply_sorted(g, out, nullptr, E, sym, nullptr, want == 0, want == 0, s);
+        if (want == 0) break;
+    }
+    if (flags & GV_BATCH_COMPACT) run_compact(g, s);
+}
+
+}  // namespace gv
+
+using namespace gv;
+
+extern "C" gv_status gv_batch_run(gv_graph *g, const gv_batch_desc *descs, uint32_t nbatches, const uint32_t *src,
+                                  const uint32_t *dst, int mem, uint32_t flags, void *stream) {
+    if (!g || (nbatches && !descs)) { set_error("null argument"); return GV_ERR_INVALID; }
+    if (g->cfg.weighted) { set_error("gv_batch_run handles unweighted stores"); return GV_ERR_UNSUPPORTED; }
+    if (nbatches == 0) return GV_OK;
+    uint64_t total = 0;
+    for (uint32_t i = 0; i < nbatches; ++i) {
+        if (descs[i].offset != total) { set_error("batches must be laid out consecutively"); return GV_ERR_INVALID; }
+        total += (uint64_t)descs[i].n_insert + descs[i].n_delete;
+    }
+    if (total == 0) return GV_OK;
+    if (!src || !dst) { set_error("null src/dst"); return GV_ERR_INVALID; }
+    if (total > 0x7FFFFFFFull) { set_error("window too large"); return GV_ERR_CAPACITY; }
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (prev != g->cfg.device) cudaSetDevice(g->cfg.device);
+    cudaStream_t s = (cudaStream_t)stream;
+    WindowBufs &wb = window_bufs(g);
+    const bool sym = !g->cfg.directed;
+    const uint64_t E = sym ? 2 * total : total;
+    gv_status st = ensure_batch_scratch(g, E, 1);
+    const uint64_t ntiles = (E + NET_TILE - 1) / NET_TILE;
+    if (st == GV_OK) st = grow(&wb.vals, wb.cap_vals, E, 4, "window vals");
+    if (st == GV_OK) st = grow(&wb.vals_alt, wb.cap_vals_alt, E, 4, "window vals");
+    if (st == GV_OK) st = grow(&wb.bstart, wb.cap_bstart, nbatches, 8, "window starts");
+    if (st == GV_OK) st = grow(&wb.bsplit, wb.cap_bsplit, nbatches, 8, "window splits");
+    if (st == GV_OK) st = grow(&wb.tile_cnt, wb.cap_tiles, ntiles + 2, 4, "window tiles");
+    const uint32_t *dsrc = src, *ddst = dst;
+    if (st == GV_OK && mem == GV_MEM_HOST) {
+        const uint32_t n = g->d.n;
+        for (uint64_t i = 0; i < total; ++i)
+            if (src[i] >= n || dst[i] >= n) { set_error("vertex id out of range"); st = GV_ERR_INVALID; break; }
+        if (st == GV_OK) st = grow(&wb.src, wb.cap_src, total, 4, "window src");
+        if (st == GV_OK) st = grow(&wb.dst, wb.cap_dst, total, 4, "window dst");
+        if (st == GV_OK) {
+            cudaMemcpyAsync(wb.src, src, total * 4, cudaMemcpyHostToDevice, s);
+            cudaMemcpyAsync(wb.dst, dst, total * 4, cudaMemcpyHostToDevice, s);
+            dsrc = wb.src;
+            ddst = wb.dst;
+        }
+    }
+    if (st == GV_OK) {
+        std::vector<unsigned long long> hs(nbatches), hp(nbatches);
+        for (uint32_t i = 0; i < nbatches; ++i) {
+            hs[i] = descs[i].offset;
+            hp[i] = descs[i].offset + descs[i].n_insert;
+        }
+        cudaMemcpyAsync(wb.bstart, hs.data(), nbatches * 8, cudaMemcpyHostToDevice, s);
+        cudaMemcpyAsync(wb.bsplit, hp.data(), nbatches * 8, cudaMemcpyHostToDevice, s);
+        // the host vectors die here: wait for the copies before returning
+        cudaError_t e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) st = cuda_status(e, "window descriptors");
+    }
+    if (st == GV_OK) {
+        if (flags & GV_BATCH_GRAPH) {
+            if (!wb.cap_stream) cudaStreamCreateWithFlags(&wb.cap_stream, cudaStreamNonBlocking);
+            cudaGraph_t graph = nullptr;
+            cudaGraphExec_t exec = nullptr;
+            cudaError_t e = cudaStreamBeginCapture(wb.cap_stream, cudaStreamCaptureModeRelaxed);
+            if (e == cudaSuccess) {
+                enqueue_window(g, wb, nbatches, dsrc, ddst, total, flags, wb.cap_stream);
+                e = cudaStreamEndCapture(wb.cap_stream, &graph);
+            }
+            if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+            if (e == cudaSuccess) e = cudaGraphLaunch(exec, s);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // the exec is destroyed below
+            if (exec) cudaGraphExecDestroy(exec);
+            if (graph) cudaGraphDestroy(graph);
+            st = cuda_status(e, "window graph");
+        } else {
+            enqueue_window(g, wb, nbatches, dsrc, ddst, total, flags, s);
+            st = cuda_status(cudaGetLastError(), "window launch");
+        }
+    }
+    if (prev >= 0 && prev != g->cfg.device) cudaSetDevice(prev);
+    return st;
+}
+
+// Autotuner: builds the sample graph once per candidate (edge-block size x
+// threads per vertex), times one window of batches and one PageRank with
+// CUDA events, and keeps the fastest total.
+extern "C" gv_status gv_autotune(const gv_config *base, const uint32_t *src0, const uint32_t *dst0, uint64_t k0,
+                                 const gv_batch_desc *descs, uint32_t nbatches, const uint32_t *bsrc,
+                                 const uint32_t *bdst, int mem, gv_tune_result *results, uint32_t *nresults,
+                                 gv_config *best) {
+    if (!base || !best || (k0 && (!src0 || !dst0))) { set_error("null argument"); return GV_ERR_INVALID; }
+    static const uint32_t blocks[] = {32, 64, 128};
+    static const uint32_t tpvs[] = {4, 8, 16, 32};
+    *best = *base;
+    float best_ms = 1e30f;
+    uint32_t nr = 0;
+    cudaEvent_t e0, e1, e2;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventCreate(&e2);
+    gv_status st = GV_OK;
+    std::vector<float> x(base->num_vertices);
+    for (uint32_t B : blocks)
+        for (uint32_t T : tpvs) {
+            gv_config c = *base;
+            c.block_size = B;
+            c.threads_per_vertex = T;
+            gv_graph *g = nullptr;
+            st = gv_create(&c, &g);
+            if (st != GV_OK) break;
+            st = gv_insert_edges(g, src0, dst0, nullptr, k0, mem, nullptr);
+            if (st == GV_OK) st = gv_synchronize(g, nullptr);
+            float upd = 0.f, pr = 0.f;
+            if (st == GV_OK) {
+                cudaEventRecord(e0, 0);
+                st = gv_batch_run(g, descs, nbatches, bsrc, bdst, mem, GV_BATCH_COMPACT, nullptr);
+                cudaEventRecord(e1, 0);
+                int32_t sw = 0;
+                if (st == GV_OK) st = gv_pagerank(g, 0.85f, 1e-6f, 100, x.data(), &sw, GV_MEM_HOST, nullptr);
+                cudaEventRecord(e2, 0);
+                cudaEventSynchronize(e2);
+                cudaEventElapsedTime(&upd, e0, e1);
+                cudaEventElapsedTime(&pr, e1, e2);
+            }
+            gv_destroy(g);
+            if (st != GV_OK) break;
+            if (results && nresults && nr < *nresults) results[nr] = {B, T, upd, pr};
+            ++nr;
+            if (upd + pr < best_ms) {
+                best_ms = upd + pr;
+                *best = c;
+            }
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaEventDestroy(e2);
+    if (nresults) *nresults = nr;
+    return st;
+}

@@ -65,6 +65,13 @@ gv_status read_ctl(gv_graph *g, Ctl *out, cudaStream_t s);
 // Update pipeline stages (launch only).
 gv_status run_update(gv_graph *g, const uint32_t *dsrc, const uint32_t *ddst, const float *dw,
                      uint64_t k, bool symmetric, bool is_delete, cudaStream_t s);
+// Segment + membership + apply from keys already sorted (src << bitsn | dst);
+// V = original entry index per key (weighted inserts), else nullptr.
+gv_status apply_sorted(gv_graph *g, const unsigned long long *K, const uint32_t *V, uint64_t E, bool symmetric,
+                       const float *dw, bool is_delete, bool finish, cudaStream_t s);
+void launch_commit_keep_abort(gv_graph *g, cudaStream_t s);
+void launch_finish(gv_graph *g, cudaStream_t s);
+void release_window(gv_graph *g);
 gv_status run_compact(gv_graph *g, cudaStream_t s);
 gv_status run_export(gv_graph *g, unsigned long long *offsets, uint32_t *dst, float *w,
                      cudaStream_t s);

@@ -328,6 +328,14 @@ __global__ void k_finish(Ctl *ctl) {
     ctl->batch_abort = 0;
 }
 
+// Commits one stage of a multi-stage window but keeps the abort flag, so a
+// window rejected in an earlier stage skips the later ones too.
+__global__ void k_commit_keep_abort(Ctl *ctl) {
+    if (!ctl->batch_abort) ctl->free_top -= ctl->alloc_cursor;
+    ctl->alloc_cursor = 0;
+    ctl->nbig = 0;
+}
+
 // ------------------------------------------------------------------- apply
 // Pool index of new block t of a segment (popped from the top of the stack).
 __device__ __forceinline__ uint32_t new_block(const DevGraph &g, unsigned long long top, uint32_t base,
@@ -774,6 +782,19 @@ gv_status run_update(gv_graph *g, const uint32_t *dsrc, const uint32_t *ddst, co
     }
     const unsigned long long *K = which ? bs.keys_alt : bs.keys;
     const uint32_t *V = which ? bs.vals_alt : bs.vals;
+    return apply_sorted(g, K, vals ? V : nullptr, E, symmetric, dw, is_delete, true, s);
+}
+
+void launch_commit_keep_abort(gv_graph *g, cudaStream_t s) {
+    GV_LAUNCH(k_commit_keep_abort, 1, 1, 0, s, g->d.ctl);
+}
+
+void launch_finish(gv_graph *g, cudaStream_t s) { GV_LAUNCH(k_finish, 1, 1, 0, s, g->d.ctl); }
+
+gv_status apply_sorted(gv_graph *g, const unsigned long long *K, const uint32_t *V, uint64_t E, bool symmetric,
+                       const float *dw, bool is_delete, bool finish, cudaStream_t s) {
+    BatchScratch &bs = g->bs;
+    const bool vals = (V != nullptr) && (dw != nullptr) && !is_delete;
     const unsigned long long sent = (g->bitsn >= 32) ? ~0ull : ((1ull << (2 * g->bitsn)) - 1ull);
     const unsigned ntiles = (unsigned)((E + SEG_TILE - 1) / SEG_TILE);
     {
@@ -821,7 +842,8 @@ gv_status run_update(gv_graph *g, const uint32_t *dsrc, const uint32_t *ddst, co
                   vals ? bs.bw : nullptr, bs.found, bs.seg_found, bs.seg_newblocks, bs.seg_blkbase,
                   bs.big_list);
     }
-    GV_LAUNCH(k_finish, 1, 1, 0, s, d.ctl);
+    if (finish) GV_LAUNCH(k_finish, 1, 1, 0, s, d.ctl);
+    else GV_LAUNCH(k_commit_keep_abort, 1, 1, 0, s, d.ctl);
     return cuda_status(cudaGetLastError(), "update launch");
 }
 

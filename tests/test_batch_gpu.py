@@ -1,0 +1,116 @@
+"""GPU tests of the batched forms: a window of update batches applied by
+gv_batch_run must leave exactly the graph that applying the batches one by
+one leaves (the oracle applies them one by one); batched PPR queries must
+match the oracle per query; the autotuner must return a valid config."""
+import numpy as np
+import pytest
+
+import oracle
+from tests.helpers import assert_same_adjacency, assert_sound, make_graph, rmat_graph, sample_existing
+
+gv_b200 = pytest.importorskip("gv_b200")
+pytestmark = pytest.mark.gpu
+
+PR_L1 = 1e-6
+
+
+def _window(n, off, dst, rng, nb=12):
+    """Batches that overlap on purpose: pairs inserted, deleted, re-inserted
+    across batches, duplicates, self-loops."""
+    batches = []
+    pool_s, pool_d = gv_b200.gen_uniform(n, 4000, seed=int(rng.integers(1 << 30)))
+    for b in range(nb):
+        k = int(rng.integers(50, 800))
+        ins = rng.integers(0, len(pool_s), k)
+        ins_s, ins_d = pool_s[ins], pool_d[ins]
+        es, ed = sample_existing(off, dst, int(rng.integers(20, 400)), rng)
+        # delete some of the shared pool too, so later batches re-insert them
+        dl = rng.integers(0, len(pool_s), int(rng.integers(10, 300)))
+        del_s = np.concatenate([es, pool_s[dl]])
+        del_d = np.concatenate([ed, pool_d[dl]])
+        loops = rng.integers(0, n, 5).astype(np.uint32)
+        ins_s = np.concatenate([ins_s, loops, ins_s[:10]])
+        ins_d = np.concatenate([ins_d, loops, ins_d[:10]])
+        batches.append((ins_s.astype(np.uint32), ins_d.astype(np.uint32), del_s.astype(np.uint32),
+                        del_d.astype(np.uint32)))
+    return batches
+
+
+@pytest.mark.parametrize("graph_mode,device_inputs", [(False, False), (True, False), (False, True)])
+def test_window_equals_sequential(graph_mode, device_inputs):
+    import torch
+    scale = 11
+    n = 1 << scale
+    s, d = rmat_graph(scale, 16, seed=3)
+    o = oracle.OracleGraph(n)
+    o.insert(s, d)
+    off, dst, _ = o.export()
+    batches = _window(n, off, dst, np.random.default_rng(11))
+    g = make_graph(n)
+    g.batch_insert(s, d)
+    if device_inputs:
+        descs, srcs, dsts, p = [], [], [], 0
+        for a, b, c, e in batches:
+            descs.append((p, len(a), len(c)))
+            srcs += [a, c]
+            dsts += [b, e]
+            p += len(a) + len(c)
+        src = torch.from_numpy(np.concatenate(srcs).view(np.int32)).cuda()
+        dstt = torch.from_numpy(np.concatenate(dsts).view(np.int32)).cuda()
+        g.batch_run((descs, src, dstt), compact=True, graph=graph_mode)
+    else:
+        g.batch_run(batches, compact=True, graph=graph_mode)
+    g.synchronize()
+    for ins_s, ins_d, del_s, del_d in batches:
+        o.insert(ins_s, ins_d)
+        o.delete(del_s, del_d)
+    assert_same_adjacency(g, o)
+    assert_sound(g)
+
+
+def test_window_rejects_bad_ids_whole():
+    import torch
+    n = 512
+    s, d = rmat_graph(9, 8, seed=5)
+    g = make_graph(n)
+    g.batch_insert(s, d)
+    g.synchronize()
+    before = g.export_csr()
+    src = torch.tensor([1, 2, 3, 4000], dtype=torch.int32, device="cuda")
+    dst = torch.tensor([5, 6, 7, 8], dtype=torch.int32, device="cuda")
+    g.batch_run(([(0, 2, 2)], src, dst), compact=True)
+    with pytest.raises(gv_b200.GvError):
+        g.synchronize()
+    after = g.export_csr()
+    assert np.array_equal(before[0], after[0]) and np.array_equal(np.sort(before[1]), np.sort(after[1]))
+    assert_sound(g)
+
+
+def test_ppr_batch_matches_oracle_per_query():
+    scale = 12
+    n = 1 << scale
+    s, d = rmat_graph(scale, 16, seed=8)
+    g = make_graph(n)
+    g.batch_insert(s, d)
+    o = oracle.OracleGraph(n)
+    o.insert(s, d)
+    sources = np.random.default_rng(2).choice(n, 24, replace=False).astype(np.uint32)
+    x, sweeps = g.ppr_batch(sources, 0.85, 1e-6, 100)
+    assert x.shape == (n, len(sources))
+    for j, src in enumerate(sources):
+        xo, _ = o.ppr(int(src), 0.85, 1e-6, 100, fixed_sweeps=sweeps)
+        assert np.abs(x[:, j] - xo).sum() < PR_L1, j
+
+
+def test_autotune_returns_a_candidate():
+    scale = 10
+    n = 1 << scale
+    s, d = rmat_graph(scale, 8, seed=4)
+    o = oracle.OracleGraph(n)
+    o.insert(s, d)
+    off, dst, _ = o.export()
+    batches = _window(n, off, dst, np.random.default_rng(5), nb=4)
+    best, results = gv_b200.autotune(n, s, d, batches, hbm_budget_bytes=256 << 20)
+    assert len(results) == 12
+    assert best["block_size"] in (32, 64, 128) and best["threads_per_vertex"] in (4, 8, 16, 32)
+    assert all(r["update_ms"] > 0 and r["pagerank_ms"] > 0 for r in results)
