@@ -53,6 +53,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-clocks", action="store_true")
+    ap.add_argument("--no-batching", action="store_true", help="skip the scale-24 batched-vs-plain section")
+    ap.add_argument("--batch-scale", type=int, default=24)
+    ap.add_argument("--c3-batches", type=int, default=64)
     return ap.parse_args()
 
 
@@ -134,6 +137,39 @@ def bc_sources(n, k, seed):
     return np.random.default_rng(seed + 7).choice(n, size=k, replace=False).astype(np.uint32)
 
 
+def zipf_ids(rng, n, k, a=1.1):
+    """k vertex ids, Zipf(a)-skewed over a seeded permutation of [0, n)."""
+    out = np.empty(0, np.int64)
+    while len(out) < k:
+        z = rng.zipf(a, size=2 * (k - len(out)))
+        out = np.concatenate([out, z[z <= n] - 1])
+    out = out[:k]
+    mult = 0x9E3779B1 | 1  # odd multiplier: a bijection on [0, 2^scale)
+    return ((out * mult + 12345) & (n - 1)).astype(np.uint32)
+
+
+def make_c3_batches(n, off, dst, nb, seed, lo=1_000, hi=4_000_000):
+    """nb batches: sizes log-uniform in [lo, hi], insert fraction U[0.2, 0.8],
+    sources Zipf(1.1); inserts pair a source with a uniform vertex, deletes
+    pick an existing neighbour of the source."""
+    rng = np.random.default_rng(seed)
+    deg = np.diff(off).astype(np.int64)
+    batches = []
+    for _ in range(nb):
+        size = int(np.exp(rng.uniform(np.log(lo), np.log(hi))))
+        ni = int(size * rng.uniform(0.2, 0.8))
+        nd = size - ni
+        ins_s = zipf_ids(rng, n, ni)
+        ins_d = rng.integers(0, n, ni, dtype=np.int64).astype(np.uint32)
+        cand = zipf_ids(rng, n, 2 * nd + 16)
+        cand = cand[deg[cand] > 0][:nd]
+        pick = (rng.random(len(cand)) * deg[cand]).astype(np.int64)
+        del_s = cand
+        del_d = dst[off[cand].astype(np.int64) + pick]
+        batches.append((ins_s, ins_d, del_s.astype(np.uint32), del_d.astype(np.uint32)))
+    return batches
+
+
 # ----------------------------------------------------------------- CPU legs
 def cpu_sample(args, pairs, batches, n, threads, steps):
     """Times the oracle (the reference's semantics restated on the CPU) on
@@ -203,6 +239,105 @@ def workload_config(args, n, m0):
             "block_size": args.block, "threads_per_vertex": args.tpv,
             "l2": "working set larger than L2 (adjacency ~0.5 GB vs 126 MB); each step uses fresh batch buffers",
             "parallelism": "replicas"}
+
+
+# ------------------------------------------------------------ batching leg
+def insert_chunked(g, s_dev, d_dev, chunk=1 << 26):
+    for i in range(0, len(s_dev), chunk):
+        g.batch_insert(s_dev[i:i + chunk], d_dev[i:i + chunk])
+    g.synchronize()
+
+
+def run_batching(args, dev):
+    """64 uneven Zipf batches on R-MAT scale 24, plain
+    (one synchronous call per batch + compaction, as the reference) against
+    the batched window; 32 PPR queries one by one against one batched call."""
+    import torch
+    import gv_b200
+    scale = args.batch_scale
+    n = 1 << scale
+    seed = args.seed + 100
+    # autotune on a scale-20 sample of the same workload shape
+    ts, td = gv_b200.gen_rmat(20, 16 << 20, seed)
+    to = gv_b200.GraphVine(1 << 20, hbm_budget_bytes=4 << 30)
+    to.batch_insert(ts, td)
+    toff, tdst, _ = to.export_csr()
+    to.close()
+    tune_batches = make_c3_batches(1 << 20, toff, tdst, 16, seed, hi=200_000)
+    best, tune = gv_b200.autotune(1 << 20, ts, td, tune_batches, hbm_budget_bytes=4 << 30)
+    cfg = dict(block_size=best["block_size"], threads_per_vertex=best["threads_per_vertex"],
+               hbm_budget_bytes=24 << 30, max_batch_pairs=1 << 22, device=dev.index or 0)
+    s_dev, d_dev = gv_b200.gen_rmat(scale, args.edge_factor << scale, seed, device=dev)
+    gp = gv_b200.GraphVine(n, **cfg)
+    insert_chunked(gp, s_dev, d_dev)
+    off, dst, _ = gp.export_csr()
+    m0 = int(off[-1])
+    batches = make_c3_batches(n, off, dst, args.c3_batches, seed)
+    del off, dst
+    gb = gv_b200.GraphVine(n, **cfg)
+    insert_chunked(gb, s_dev, d_dev)
+    del s_dev, d_dev
+    torch.cuda.empty_cache()
+    tot = sum(len(b[0]) + len(b[2]) for b in batches)
+    dev_b = [tuple(torch.from_numpy(a.view(np.int32)).to(dev) for a in b) for b in batches]
+    descs, srcs, dsts, p = [], [], [], 0
+    for a, b_, c, e in batches:
+        descs.append((p, len(a), len(c)))
+        srcs += [a, c]
+        dsts += [b_, e]
+        p += len(a) + len(c)
+    wsrc = torch.from_numpy(np.concatenate(srcs).view(np.int32)).to(dev)
+    wdst = torch.from_numpy(np.concatenate(dsts).view(np.int32)).to(dev)
+    torch.cuda.synchronize()
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    e[0].record()
+    for ins_s, ins_d, del_s, del_d in dev_b:
+        gp.batch_insert(ins_s, ins_d)
+        gp.synchronize()
+        gp.batch_delete(del_s, del_d)
+        gp.synchronize()
+        gp.compaction()
+        gp.synchronize()
+    e[1].record()
+    torch.cuda.synchronize()
+    e[2].record()
+    gb.batch_run((descs, wsrc, wdst), compact=True, graph=True)
+    gb.synchronize()
+    e[3].record()
+    torch.cuda.synchronize()
+    plain_ms, batched_ms = e[0].elapsed_time(e[1]), e[2].elapsed_time(e[3])
+    m_p, m_b = gp.num_edges(), gb.num_edges()
+    # PageRank queries: 32 sources one by one vs one batched call
+    srcs_q = np.random.default_rng(seed).choice(n, 32, replace=False).astype(np.uint32)
+    xq = torch.empty(n, dtype=torch.float32, device=dev)
+    xb = torch.empty((n, 32), dtype=torch.float32, device=dev)
+    torch.cuda.synchronize()
+    e[0].record()
+    sw_plain = 0
+    for sq in srcs_q:
+        _, sw = gp.ppr(int(sq), out=xq)
+        sw_plain += sw
+    e[1].record()
+    torch.cuda.synchronize()
+    e[2].record()
+    _, sw_b = gb.ppr_batch(srcs_q, out=xb)
+    e[3].record()
+    torch.cuda.synchronize()
+    pr_plain_ms, pr_batched_ms = e[0].elapsed_time(e[1]), e[2].elapsed_time(e[3])
+    gteps_plain = m_p * sw_plain / (pr_plain_ms / 1e3) / 1e9
+    gteps_batched = m_b * sw_b * 32 / (pr_batched_ms / 1e3) / 1e9
+    gp.close()
+    gb.close()
+    return {"workload": (f"R-MAT scale {scale} ef {args.edge_factor}, {len(batches)} batches log-uniform in "
+                         f"[1K, 4M] updates, Zipf(1.1) sources, insert fraction U[0.2, 0.8]; 32 PPR queries"),
+            "m_initial_entries": m0, "updates": tot, "edges_after_plain": m_p, "edges_after_batched": m_b,
+            "plain_updates_per_s": tot / (plain_ms / 1e3), "batched_updates_per_s": tot / (batched_ms / 1e3),
+            "updates_speedup": plain_ms / batched_ms,
+            "plain": "one synchronous insert, delete and compaction call per batch",
+            "batched": "gv_batch_run: one coalesced window, compaction once, CUDA graph",
+            "pagerank_gteps_plain": gteps_plain, "pagerank_gteps_batched": gteps_batched,
+            "pagerank_speedup": pr_plain_ms / pr_batched_ms,
+            "autotune_best": best, "autotune": tune}
 
 
 # ------------------------------------------------------------------ GPU leg
@@ -370,6 +505,8 @@ def run_gv(args, rank, world, local_rank):
     if e2e:
         line["e2e"] = {"value": updates / (e2e_ms / 1e3), "unit": "edge updates/s",
                        "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"]}
+    if world == 1 and not args.no_batching:
+        line["batching"] = run_batching(args, torch.device("cuda", local_rank))
     if world == 1 and not args.no_cpu_baseline:
         import gv_b200 as gvb
         pairs = gvb.gen_rmat(args.scale, args.edge_factor << args.scale, seed)

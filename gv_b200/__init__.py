@@ -329,11 +329,13 @@ class GraphVine:
                                               _stream(stream)), "gv_pagerank_dynamic")
         return xr, sw.value
 
-    def ppr(self, source: int, alpha: float = 0.85, epsilon: float = 1e-6, max_iter: int = 100, stream=None):
-        x = np.empty(self.n, np.float32)
+    def ppr(self, source: int, alpha: float = 0.85, epsilon: float = 1e-6, max_iter: int = 100, out=None,
+            stream=None):
+        x = np.empty(self.n, np.float32) if out is None else out
+        px, mem, _ = _ptr(x, np.float32)
         sw = C.c_int32()
-        _check(_lib.lib().gv_ppr(self._h, source, alpha, epsilon, max_iter, x.ctypes.data, C.byref(sw),
-                                 GV_MEM_HOST, _stream(stream)), "gv_ppr")
+        _check(_lib.lib().gv_ppr(self._h, source, alpha, epsilon, max_iter, px, C.byref(sw), mem, _stream(stream)),
+               "gv_ppr")
         return x, sw.value
 
     def static_tc(self, per_vertex: bool = True, stream=None):
