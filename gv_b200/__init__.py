@@ -195,6 +195,17 @@ class GraphVine:
     def handle(self) -> int:
         return self._h.value
 
+    def view(self) -> "GraphVine":
+        """A read-only view: shares this graph's store and owns its analytics
+        scratch, so queries can run on other threads and streams while nothing
+        updates the graph.  Close views before the graph."""
+        h = C.c_void_p()
+        _check(_lib.lib().gv_view_create(self._h, C.byref(h)), "gv_view_create")
+        v = GraphVine.__new__(GraphVine)
+        v._h, v.n, v.weighted, v.directed, v.device = h, self.n, self.weighted, self.directed, self.device
+        v._parent = self
+        return v
+
     # -- updates (GraphVine::bulkBuild / batchInsert / batchDelete / compaction)
     def bulk_build(self, offsets, dst, weights=None, stream=None) -> None:
         po, mem, k1 = _ptr(offsets, np.uint64)
@@ -390,3 +401,73 @@ class GraphVine:
                                           grad.ctypes.data, m, lam.ctypes.data, C.byref(sw), GV_MEM_HOST,
                                           _stream(stream)), "gv_wpr_backward")
         return grad[:m], lam, sw.value
+
+    # -- serving -----------------------------------------------------------
+    def serve(self, trace, *, slots: int = 4, ppr_batch: int = 32, max_coalesce: int = 64, pace: bool = True,
+              hbm_budget_bytes: int = 32 << 30, alpha: float = 0.85, epsilon: float = 1e-6, max_iter: int = 100,
+              outputs: bool = False):
+        """Run a request trace through gv_serve_trace.
+
+        trace items (arrival_s last, non-decreasing):
+          ("update", ins_src, ins_dst, del_src, del_dst, arrival_s)
+          ("ppr", source, arrival_s)
+          ("tc", vertices, arrival_s)      incident-triangle counts of the vertices
+          ("bc", sources, arrival_s)       betweenness from the given sources
+        Returns (results, outs): results a structured array with start_s, done_s,
+        latency_ms, epoch, status, sweeps, group per request; outs a list with
+        each query's result (None for updates) when outputs=True."""
+        kinds = {"update": _lib.GV_REQ_UPDATE, "ppr": _lib.GV_REQ_PPR, "tc": _lib.GV_REQ_TC, "bc": _lib.GV_REQ_BC}
+        nreq = len(trace)
+        reqs = (_lib.gv_request * max(nreq, 1))()
+        srcs, dsts, qv = [], [], []
+        upd_off = q_off = 0
+        for i, item in enumerate(trace):
+            r = reqs[i]
+            r.kind = kinds[item[0]]
+            r.arrival_s = float(item[-1])
+            if item[0] == "update":
+                ins_s, ins_d, del_s, del_d = (np.asarray(a, np.uint32) for a in item[1:5])
+                r.count0, r.count1, r.offset = len(ins_s), len(del_s), upd_off
+                srcs += [ins_s, del_s]
+                dsts += [ins_d, del_d]
+                upd_off += len(ins_s) + len(del_s)
+            elif item[0] == "ppr":
+                r.source = int(item[1])
+            else:
+                v = np.asarray(item[1], np.uint32)
+                r.count0, r.offset = len(v), q_off
+                qv.append(v)
+                q_off += len(v)
+        src = np.concatenate(srcs) if srcs else np.zeros(1, np.uint32)
+        dst = np.concatenate(dsts) if dsts else np.zeros(1, np.uint32)
+        qvert = np.concatenate(qv) if qv else np.zeros(1, np.uint32)
+        cfg = _lib.gv_serve_config()
+        L = _lib.lib()
+        _check(L.gv_serve_config_init(C.byref(cfg)), "gv_serve_config_init")
+        cfg.slots, cfg.ppr_batch, cfg.max_coalesce, cfg.pace = slots, ppr_batch, max_coalesce, int(pace)
+        cfg.hbm_budget_bytes, cfg.alpha, cfg.epsilon, cfg.max_iter = hbm_budget_bytes, alpha, epsilon, max_iter
+        res = (_lib.gv_request_result * max(nreq, 1))()
+        outs_list = [None] * nreq
+        po = None
+        if outputs:
+            ptr_ppr = (C.c_void_p * max(nreq, 1))()
+            ptr_tc = (C.c_void_p * max(nreq, 1))()
+            ptr_bc = (C.c_void_p * max(nreq, 1))()
+            for i, item in enumerate(trace):
+                if item[0] == "ppr":
+                    outs_list[i] = np.zeros(self.n, np.float32)
+                    ptr_ppr[i] = outs_list[i].ctypes.data
+                elif item[0] == "tc":
+                    outs_list[i] = np.zeros(len(item[1]), np.uint64)
+                    ptr_tc[i] = outs_list[i].ctypes.data
+                elif item[0] == "bc":
+                    outs_list[i] = np.zeros(self.n, np.float32)
+                    ptr_bc[i] = outs_list[i].ctypes.data
+            po = _lib.gv_serve_outputs(C.cast(ptr_ppr, C.c_void_p), C.cast(ptr_tc, C.c_void_p),
+                                       C.cast(ptr_bc, C.c_void_p))
+        _check(L.gv_serve_trace(self._h, C.byref(cfg), reqs, nreq, src.ctypes.data, dst.ctypes.data,
+                                qvert.ctypes.data, res, C.byref(po) if po is not None else None), "gv_serve_trace")
+        dt = np.dtype([("start_s", np.float64), ("done_s", np.float64), ("latency_ms", np.float64),
+                       ("epoch", np.uint32), ("status", np.uint32), ("sweeps", np.uint32), ("group", np.uint32)])
+        out = np.frombuffer(bytes(res), dtype=dt, count=nreq).copy() if nreq else np.zeros(0, dt)
+        return out, outs_list

@@ -1,4 +1,4 @@
-"""ctypes binding of libgv.so (the C ABI in include/gv.h and include/gv_gen.h).
+"""ctypes binding of libgv.so (the C ABI in include/*.h).
 
 The library is loaded from this package directory only; there is no CPU
 fallback, so a missing library is an ImportError.
@@ -41,6 +41,28 @@ class gv_tune_result(C.Structure):
 
 GV_BATCH_COMPACT, GV_BATCH_GRAPH = 1, 2
 
+GV_REQ_UPDATE, GV_REQ_PPR, GV_REQ_TC, GV_REQ_BC = range(4)
+
+
+class gv_request(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("count0", C.c_uint32), ("count1", C.c_uint32), ("source", C.c_uint32),
+                ("offset", C.c_uint64), ("arrival_s", C.c_double)]
+
+
+class gv_request_result(C.Structure):
+    _fields_ = [("start_s", C.c_double), ("done_s", C.c_double), ("latency_ms", C.c_double),
+                ("epoch", C.c_uint32), ("status", C.c_uint32), ("sweeps", C.c_uint32), ("group", C.c_uint32)]
+
+
+class gv_serve_config(C.Structure):
+    _fields_ = [("slots", C.c_uint32), ("ppr_batch", C.c_uint32), ("max_coalesce", C.c_uint32),
+                ("pace", C.c_uint32), ("hbm_budget_bytes", C.c_uint64), ("alpha", C.c_float),
+                ("epsilon", C.c_float), ("max_iter", C.c_int32)]
+
+
+class gv_serve_outputs(C.Structure):
+    _fields_ = [("ppr", C.c_void_p), ("tc", C.c_void_p), ("bc", C.c_void_p)]
+
 P = C.c_void_p
 u32, u64, i32, f32 = C.c_uint32, C.c_uint64, C.c_int32, C.c_float
 pu32, pu64, pi32, pf32, pu8 = C.POINTER(C.c_uint32), C.POINTER(C.c_uint64), C.POINTER(C.c_int32), C.POINTER(C.c_float), C.POINTER(C.c_uint8)
@@ -49,6 +71,7 @@ pu32, pu64, pi32, pf32, pu8 = C.POINTER(C.c_uint32), C.POINTER(C.c_uint64), C.PO
 SIGNATURES = {
     "gv_config_init": (C.c_int, [C.POINTER(gv_config), u32]),
     "gv_create": (C.c_int, [C.POINTER(gv_config), C.POINTER(P)]),
+    "gv_view_create": (C.c_int, [P, C.POINTER(P)]),
     "gv_destroy": (C.c_int, [P]),
     "gv_bulk_build_csr": (C.c_int, [P, P, P, P, C.c_int, P]),
     "gv_insert_edges": (C.c_int, [P, P, P, P, u64, C.c_int, P]),
@@ -85,6 +108,9 @@ SIGNATURES = {
     "gv_ppr_batch": (C.c_int, [P, P, u32, f32, f32, i32, P, pi32, C.c_int, P]),
     "gv_autotune": (C.c_int, [C.POINTER(gv_config), P, P, u64, C.POINTER(gv_batch_desc), u32, P, P, C.c_int,
                               C.POINTER(gv_tune_result), pu32, C.POINTER(gv_config)]),
+    "gv_serve_config_init": (C.c_int, [C.POINTER(gv_serve_config)]),
+    "gv_serve_trace": (C.c_int, [P, C.POINTER(gv_serve_config), C.POINTER(gv_request), u32, P, P, P,
+                                 C.POINTER(gv_request_result), C.POINTER(gv_serve_outputs)]),
     "gv_gen_rmat": (C.c_int, [u32, u64, u64, u64, P, P, C.c_int, P]),
     "gv_gen_uniform": (C.c_int, [u32, u64, u64, P, P, C.c_int, P]),
 }

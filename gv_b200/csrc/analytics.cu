@@ -33,6 +33,7 @@ constexpr int BIG_TAB_A = 1024;
 // Pull sweeps route vertices by used slots: lane groups up to LIGHT_FILL,
 // one CTA per vertex up to HUB_FILL, the whole grid above.
 constexpr uint32_t LIGHT_FILL = 256;
+constexpr uint32_t TINY_FILL = 32;  // thread-per-vertex tier of the pull sweeps
 constexpr uint32_t HUB_FILL = 16384;
 constexpr int HV_THREADS = 512;
 // BFS levels, BC dependencies and the TC snapshot expand vertices with more
@@ -81,6 +82,49 @@ __device__ __forceinline__ float pull_finish(const PullArgs &a, uint32_t v, floa
     return xv;
 }
 
+// Vertices with at most TINY_FILL entries: one thread per vertex issues all
+// of its (at most 8) 16-byte loads and gathers at once, so the dependent
+// chain vertex -> block -> neighbours is paid once per thread instead of
+// once per vertex by a whole lane group.
+template <bool W>
+__global__ void __launch_bounds__(AN_THREADS) k_pull_tiny(DevGraph g, PullArgs a, uint32_t part_base) {
+    __shared__ double red[AN_THREADS / 32];
+    if (a.state[0]) return;
+    double res = 0.0;
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < g.n; v += gridDim.x * blockDim.x) {
+        const uint4 rec = g.vtx[v];
+        const uint32_t fill = rec.y;
+        if (fill > TINY_FILL) continue;  // k_pull / k_pull_items
+        float sum = 0.f;
+        if (fill) {
+            const size_t base = (size_t)rec.x << g.logB;  // fill <= 32 <= B: one block
+#pragma unroll
+            for (uint32_t e = 0; e < TINY_FILL; e += 4) {
+                if (e < fill) {
+                    const uint4 q = *reinterpret_cast<const uint4 *>(g.pool + base + e);
+                    float4 wq = make_float4(1.f, 1.f, 1.f, 1.f);
+                    if (W) wq = *reinterpret_cast<const float4 *>(g.wpool + base + e);
+                    const uint32_t ev[4] = {q.x, q.y, q.z, q.w};
+                    const float wv[4] = {wq.x, wq.y, wq.z, wq.w};
+#pragma unroll
+                    for (int j = 0; j < 4; ++j)
+                        if (e + j < fill && ev[j] != GV_TOMB)
+                            sum += W ? wv[j] * __ldg(a.gather + ev[j]) : __ldg(a.gather + ev[j]);
+                }
+            }
+        }
+        pull_finish(a, v, sum, rec.z, res);
+    }
+    res = warp_sum(res);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = res;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int i = 0; i < AN_THREADS / 32; ++i) t += red[i];
+        a.partial[part_base + blockIdx.x] = t;
+    }
+}
+
 template <int TPV, bool W>
 __global__ void __launch_bounds__(AN_THREADS) k_pull(DevGraph g, PullArgs a) {
     __shared__ double red[AN_THREADS / 32];
@@ -94,7 +138,7 @@ __global__ void __launch_bounds__(AN_THREADS) k_pull(DevGraph g, PullArgs a) {
     for (uint32_t v = blockIdx.x * GPC + threadIdx.x / TPV; v < g.n; v += ngroups) {
         const uint4 rec = g.vtx[v];
         const uint32_t fill = rec.y, nb = blocks_for(fill, g.logB);
-        if (fill > LIGHT_FILL) continue;  // chunked items (k_pull_items)
+        if (fill > LIGHT_FILL || fill <= TINY_FILL) continue;  // k_pull_items / k_pull_tiny
         float sum = 0.f;
         if (nb == 1) {
             const size_t base = (size_t)rec.x << g.logB;
@@ -305,7 +349,8 @@ IterBufs carve_iter(void *base, uint32_t n, uint32_t parts) {
 constexpr unsigned PULL_GRID = 148 * 8;
 constexpr unsigned HUB_GRID = 148 * 2;
 constexpr unsigned FIN_GRID = 148;
-constexpr unsigned SWEEP_PARTS = PULL_GRID + FIN_GRID;
+constexpr unsigned TINY_GRID = 148 * 8;
+constexpr unsigned SWEEP_PARTS = PULL_GRID + FIN_GRID + TINY_GRID;
 
 // Builds the chunked item list of the current graph (aux scratch slots 1, 2);
 // *ipart gets one 4-byte slot per item.
@@ -375,6 +420,8 @@ gv_status run_sweeps(gv_graph *g, cudaStream_t s, IterBufs &b, PullArgs proto, b
                 if (weighted) GV_LAUNCH((k_pull<T, true>), PULL_GRID, AN_THREADS, 0, s, d, a);
                 else GV_LAUNCH((k_pull<T, false>), PULL_GRID, AN_THREADS, 0, s, d, a);
             });
+            if (weighted) GV_LAUNCH(k_pull_tiny<true>, TINY_GRID, AN_THREADS, 0, s, d, a, PULL_GRID + FIN_GRID);
+            else GV_LAUNCH(k_pull_tiny<false>, TINY_GRID, AN_THREADS, 0, s, d, a, PULL_GRID + FIN_GRID);
             if (it.nitems) {
                 if (weighted) GV_LAUNCH(k_pull_items<true>, PULL_GRID, AN_THREADS, 0, s, d, a, it, ipart);
                 else GV_LAUNCH(k_pull_items<false>, PULL_GRID, AN_THREADS, 0, s, d, a, it, ipart);
@@ -1134,7 +1181,8 @@ gv_status tc_run(gv_graph *g, cudaStream_t s, bool incident, unsigned long long 
         GV_LAUNCH(k_tc_sort_big, 148, 1024, smem, s, (const unsigned long long *)b.off, b.snap,
                   (const uint32_t *)b.big, (const unsigned long long *)b.cnts, P);
     }
-    unsigned long long *work = &d.ctl->scratch1;
+    // per-graph word (views own theirs), so concurrent counts on views do not share it
+    unsigned long long *work = (unsigned long long *)g->bs.tile_cnt + 1;
     cudaMemsetAsync(work, 0, 8, s);
     const char *hash_env = std::getenv("GV_TC_HASH");
     if (!(hash_env && hash_env[0] == '1')) {

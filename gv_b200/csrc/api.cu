@@ -380,9 +380,41 @@ fail:
     return st;
 }
 
+gv_status gv_view_create(gv_graph *g, gv_graph **out) {
+    if (!g || !out) { set_error("null argument"); return GV_ERR_INVALID; }
+    if (g->parent) g = g->parent;
+    DeviceGuard dg(g->cfg.device);
+    gv_graph *v = new gv_graph();
+    v->cfg = g->cfg;
+    v->bitsn = g->bitsn;
+    v->d = g->d;
+    v->parent = g;
+    v->weighted_alloc = g->weighted_alloc;
+    // analytics need a scan scratch and a few words of their own
+    const uint64_t elems = (uint64_t)g->d.n + 2;
+    gv_status st = dmalloc((char **)&v->bs.scan_tmp, scan_scratch_bytes(elems), "view scan");
+    if (st == GV_OK) st = dmalloc(&v->bs.tile_cnt, 64, "view words");
+    if (st != GV_OK) {
+        dfree(v->bs.scan_tmp);
+        delete v;
+        return st;
+    }
+    *out = v;
+    return GV_OK;
+}
+
 gv_status gv_destroy(gv_graph *g) {
     if (!g) return GV_OK;
     DeviceGuard dg(g->cfg.device);
+    if (g->parent) {  // a view: free only its own scratch
+        dfree(g->bs.scan_tmp);
+        dfree(g->bs.tile_cnt);
+        if (g->an_buf) cudaFree(g->an_buf);
+        for (int i = 0; i < 4; ++i)
+            if (g->aux[i]) cudaFree(g->aux[i]);
+        delete g;
+        return GV_OK;
+    }
     release_window(g);
     DevGraph &d = g->d;
     dfree(d.vtx); dfree(d.left); dfree(d.right); dfree(d.pred); dfree(d.bcount); dfree(d.owner);
@@ -421,6 +453,7 @@ static gv_status stage_pairs(gv_graph *g, const uint32_t *src, const uint32_t *d
 static gv_status update_common(gv_graph *g, const uint32_t *src, const uint32_t *dst, const float *w,
                                uint64_t k, int mem, void *stream, bool is_delete, bool force_directed) {
     if (!g || (k && (!src || !dst))) { set_error("null argument"); return GV_ERR_INVALID; }
+    if (g->parent) { set_error("a view is read-only"); return GV_ERR_STATE; }
     if (mem != GV_MEM_HOST && mem != GV_MEM_DEVICE) { set_error("bad mem flag"); return GV_ERR_INVALID; }
     if (!is_delete && g->cfg.weighted && k && !w) { set_error("weighted store needs weights"); return GV_ERR_INVALID; }
     if (!g->cfg.weighted) w = nullptr;
@@ -451,6 +484,7 @@ gv_status gv_delete_edges(gv_graph *g, const uint32_t *src, const uint32_t *dst,
 gv_status gv_bulk_build_csr(gv_graph *g, const uint64_t *offsets, const uint32_t *dst,
                             const float *weights, int mem, void *stream) {
     if (!g || !offsets) { set_error("null argument"); return GV_ERR_INVALID; }
+    if (g->parent) { set_error("a view is read-only"); return GV_ERR_STATE; }
     DeviceGuard dg(g->cfg.device);
     cudaStream_t s = (cudaStream_t)stream;
     Ctl c;
@@ -484,6 +518,7 @@ gv_status gv_bulk_build_csr(gv_graph *g, const uint64_t *offsets, const uint32_t
 
 gv_status gv_compact(gv_graph *g, void *stream) {
     if (!g) return GV_ERR_INVALID;
+    if (g->parent) { set_error("a view is read-only"); return GV_ERR_STATE; }
     DeviceGuard dg(g->cfg.device);
     return run_compact(g, (cudaStream_t)stream);
 }

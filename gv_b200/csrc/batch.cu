@@ -206,6 +206,7 @@ using namespace gv;
 extern "C" gv_status gv_batch_run(gv_graph *g, const gv_batch_desc *descs, uint32_t nbatches, const uint32_t *src,
                                   const uint32_t *dst, int mem, uint32_t flags, void *stream) {
     if (!g || (nbatches && !descs)) { set_error("null argument"); return GV_ERR_INVALID; }
+    if (g->parent) { set_error("a view is read-only"); return GV_ERR_STATE; }
     if (g->cfg.weighted) { set_error("gv_batch_run handles unweighted stores"); return GV_ERR_UNSUPPORTED; }
     if (nbatches == 0) return GV_OK;
     uint64_t total = 0;

@@ -49,6 +49,8 @@ struct gv_graph {
     // independent auxiliary device buffers, grown on demand
     void *aux[4] = {nullptr, nullptr, nullptr, nullptr};
     size_t aux_bytes[4] = {0, 0, 0, 0};
+    // a view shares the parent's store and owns only analytics scratch
+    gv_graph *parent = nullptr;
 };
 
 namespace gv {

@@ -71,8 +71,17 @@ gv_status gv_config_init(gv_config *cfg, uint32_t num_vertices);
 /* Replaces GraphVine::GraphVine(CSR*) allocation half
  * (src/dynamicStructure/graphvine.cu:5-35, :38-130). */
 gv_status gv_create(const gv_config *cfg, gv_graph **out);
-/* The reference never frees (include/dynamicStructure/graphvine.cuh:32). */
+/* The reference never frees (include/dynamicStructure/graphvine.cuh:32).
+ * Destroying a view frees only the view. */
 gv_status gv_destroy(gv_graph *g);
+
+/* A read-only view of g: it shares g's device-resident store and owns its
+ * own analytics scratch, so queries on different views (each on its own
+ * stream and host thread) can run concurrently.  Updates through a view
+ * return GV_ERR_STATE; the caller orders updates on g after queries on
+ * views.  Destroy views before g.  No reference counterpart: the reference
+ * keeps one global store per process (src/dynamicStructure/graphvine.cu:3). */
+gv_status gv_view_create(gv_graph *g, gv_graph **view);
 
 /* Bulk build from a CSR of directed entries: offsets[n+1] (uint64), dst[m].
  * Self-loops and duplicates are dropped, every other entry is stored as

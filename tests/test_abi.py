@@ -66,3 +66,15 @@ def test_no_gpu_fails_loudly():
     with pytest.raises(gv_b200.GvError) as e:
         gv_b200.GraphVine(64)
     assert "no CUDA device" in str(e.value) or "GV_ERR_CUDA" in str(e.value)
+
+
+def test_serve_config_defaults_and_null_graph():
+    from gv_b200 import _lib
+    L = _lib.lib()
+    cfg = _lib.gv_serve_config()
+    assert L.gv_serve_config_init(C.byref(cfg)) == 0
+    assert cfg.slots >= 1 and 1 <= cfg.ppr_batch <= 32 and cfg.pace == 1
+    res = (_lib.gv_request_result * 1)()
+    reqs = (_lib.gv_request * 1)()
+    assert L.gv_serve_trace(None, C.byref(cfg), reqs, 1, None, None, None, res, None) == _lib.GV_ERR_INVALID
+    assert L.gv_view_create(None, None) == _lib.GV_ERR_INVALID
