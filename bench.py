@@ -249,7 +249,7 @@ def insert_chunked(g, s_dev, d_dev, chunk=1 << 26):
 
 
 def run_batching(args, dev):
-    """64 uneven Zipf batches on R-MAT scale 24, plain
+    """Batching workload: 64 uneven Zipf batches on R-MAT scale 24, plain
     (one synchronous call per batch + compaction, as the reference) against
     the batched window; 32 PPR queries one by one against one batched call."""
     import torch

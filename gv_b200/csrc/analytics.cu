@@ -1936,30 +1936,40 @@ gv_status gv_tc_subset(gv_graph *g, const uint32_t *subset, uint64_t ns, uint64_
     if (mem == GV_MEM_HOST)
         for (uint64_t i = 0; i < ns; ++i)
             if (subset[i] >= g->d.n) { set_error("subset vertex out of range"); return GV_ERR_INVALID; }
-    unsigned long long *tc = nullptr;
-    gv_status st = tc_run(g, s, true, &tc);
-    if (st != GV_OK) return st;
     uint32_t *didx = nullptr;
     unsigned long long *dout = nullptr;
     if (mem == GV_MEM_DEVICE) {
         didx = const_cast<uint32_t *>(subset);
         dout = (unsigned long long *)out;
     } else {
-        if (cudaMalloc(&didx, ns * 4) != cudaSuccess || cudaMalloc(&dout, ns * 8) != cudaSuccess) {
-            cudaGetLastError();
-            if (didx) cudaFree(didx);
-            return GV_ERR_NOMEM;
-        }
-        cudaMemcpyAsync(didx, subset, ns * 4, cudaMemcpyHostToDevice, s);
+        const size_t at = (ns * 4 + 255) & ~size_t(255);
+        char *b = (char *)aux_scratch(g, 0, at + ns * 8);
+        if (!b) return GV_ERR_NOMEM;
+        didx = (uint32_t *)b;
+        dout = (unsigned long long *)(b + at);
+        cudaError_t e = cudaMemcpyAsync(didx, subset, ns * 4, cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess) return cuda_status(e, "tc subset input");
     }
-    GV_LAUNCH(k_gather_u64, grid_for(ns, 256), 256, 0, s, (const unsigned long long *)tc, (const uint32_t *)didx, ns, dout);
+    // local counts (neighbour hash sets, tc_local.cu) unless the subset's
+    // neighbourhoods cover more than a few passes over the store;
+    // GV_TC_SUBSET=local / global picks one path (for comparing them)
+    const char *mode = std::getenv("GV_TC_SUBSET");
+    const bool force_global = mode && std::strcmp(mode, "global") == 0;
+    const bool force_local = mode && std::strcmp(mode, "local") == 0;
+    bool done = false;
+    gv_status st = GV_OK;
+    if (!force_global) st = tc_local_subset(g, didx, ns, dout, s, &done, force_local);
+    if (st != GV_OK) return st;
+    g->last_tc_local = done ? 1 : 0;
+    if (!done) {
+        unsigned long long *tc = nullptr;
+        st = tc_run(g, s, true, &tc);
+        if (st != GV_OK) return st;
+        GV_LAUNCH(k_gather_u64, grid_for(ns, 256), 256, 0, s, (const unsigned long long *)tc, (const uint32_t *)didx, ns, dout);
+    }
     cudaError_t e = cudaSuccess;
     if (mem != GV_MEM_DEVICE) e = cudaMemcpyAsync(out, dout, ns * 8, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (mem != GV_MEM_DEVICE) {
-        cudaFree(didx);
-        cudaFree(dout);
-    }
     return cuda_status(e, "tc subset");
 }
 

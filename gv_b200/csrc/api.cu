@@ -410,7 +410,7 @@ gv_status gv_destroy(gv_graph *g) {
         dfree(g->bs.scan_tmp);
         dfree(g->bs.tile_cnt);
         if (g->an_buf) cudaFree(g->an_buf);
-        for (int i = 0; i < 4; ++i)
+        for (int i = 0; i < gv_graph::AUX_SLOTS; ++i)
             if (g->aux[i]) cudaFree(g->aux[i]);
         delete g;
         return GV_OK;
@@ -423,7 +423,7 @@ gv_status gv_destroy(gv_graph *g) {
     free_batch_entries(g->bs);
     free_batch_inputs(g->bs);
     if (g->an_buf) cudaFree(g->an_buf);
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < gv_graph::AUX_SLOTS; ++i)
         if (g->aux[i]) cudaFree(g->aux[i]);
     if (g->host_pinned) cudaFreeHost(g->host_pinned);
     delete g;
@@ -659,10 +659,14 @@ gv_status gv_last_stat(gv_graph *g, const char *key, double *value) {
             *value = (double)g->last_tc_oriented;
             return GV_OK;
         }
-        Ctl c;
-        gv_status st = read_ctl(g, &c, 0);
-        if (st == GV_OK) *value = (double)c.scratch1;
-        return st;
+        unsigned long long w = 0;  // work counter of the last count (per-graph scratch word)
+        cudaError_t e = cudaMemcpy(&w, (unsigned long long *)g->bs.tile_cnt + 1, 8, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) *value = (double)w;
+        return cuda_status(e, "tc_work");
+    }
+    if (std::strcmp(key, "tc_subset_local") == 0) {
+        *value = (double)g->last_tc_local;
+        return GV_OK;
     }
     if (std::strcmp(key, "sweeps") == 0) {
         *value = (double)g->last_sweeps;

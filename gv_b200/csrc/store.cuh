@@ -45,10 +45,12 @@ struct gv_graph {
     size_t host_pinned_bytes = 0;
     // facts about the last analytics calls (gv_last_stat)
     uint64_t last_tc_oriented = 0;
+    int32_t last_tc_local = 0;  // 1: the last subset count took the local path
     int32_t last_sweeps = 0;
     // independent auxiliary device buffers, grown on demand
-    void *aux[4] = {nullptr, nullptr, nullptr, nullptr};
-    size_t aux_bytes[4] = {0, 0, 0, 0};
+    static constexpr int AUX_SLOTS = 6;
+    void *aux[AUX_SLOTS] = {};
+    size_t aux_bytes[AUX_SLOTS] = {};
     // a view shares the parent's store and owns only analytics scratch
     gv_graph *parent = nullptr;
 };
@@ -59,7 +61,7 @@ void set_error(const std::string &msg);
 gv_status cuda_status(cudaError_t e, const char *what);
 gv_status ensure_batch_scratch(gv_graph *g, uint64_t entries, uint64_t pairs);
 void *analytics_scratch(gv_graph *g, size_t bytes);
-// Auxiliary buffer `slot` (0..3) of at least `bytes`, kept across calls.
+// Auxiliary buffer `slot` (0..AUX_SLOTS-1) of at least `bytes`, kept across calls.
 void *aux_scratch(gv_graph *g, int slot, size_t bytes);
 // Device-to-host copy of the control block (synchronises the stream).
 gv_status read_ctl(gv_graph *g, Ctl *out, cudaStream_t s);
@@ -79,6 +81,12 @@ gv_status run_export(gv_graph *g, unsigned long long *offsets, uint32_t *dst, fl
                      cudaStream_t s);
 gv_status run_check(gv_graph *g, uint64_t *violations, uint32_t *code, uint32_t *vertex);
 void launch_degrees(gv_graph *g, uint32_t *deg, cudaStream_t s);
+// Incident-triangle counts of the subset d_sub[ns] (device) into d_out[ns]
+// from neighbour hash sets, without a whole-graph pass.  *done = false (and
+// nothing written) when the subset's neighbourhoods are too large for that
+// to pay, unless force.
+gv_status tc_local_subset(gv_graph *g, const uint32_t *d_sub, uint64_t ns, unsigned long long *d_out,
+                          cudaStream_t s, bool *done, bool force);
 
 template <int T>
 struct Tpv {

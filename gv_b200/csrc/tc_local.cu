@@ -1,0 +1,410 @@
+// Incident-triangle counts for a vertex subset without a whole-graph pass.
+//
+// For u in the subset, t(u) = 1/2 * sum_{v in N(u)} |N(u) & N(v)| on the
+// symmetric store (no self-loops, no duplicates).  Each subset vertex u is
+// a group: N(u) goes into an open-addressing hash set (shared memory when it
+// has at most TL_SMEM_LIVE live entries, else a table in global memory that
+// stays in L2), and every neighbour list N(v), v in N(u), is streamed block
+// by block with 16-byte loads and probed against it.  The work is cut into
+// pieces (32 blocks of one N(v)) and units (64 consecutive pieces of one
+// group, one CTA pass), so a hub neighbour is spread over many warps and
+// CTAs.  Cost: sum over the subset of sum_{v in N(u)} deg(v) entry reads,
+// against the whole-graph oriented count the reference's tc_kernel_VC
+// (src/algorithm/tc/tc_kernel.cu:3-74) would run; the caller takes the
+// whole-graph path when that sum exceeds TL_WHOLE_RATIO passes over the store.
+#include <algorithm>
+#include <vector>
+#include "store.cuh"
+#include "prims.cuh"
+#include "launch.hpp"
+
+namespace gv {
+namespace {
+
+constexpr int TL_THREADS = 256;
+constexpr uint32_t TL_PIECE_BLOCKS = 32;                     // blocks of N(v) per piece (one per lane)
+constexpr uint32_t TL_UNIT_PIECES = 64;                      // pieces per unit
+constexpr uint32_t TL_SMEM_LOG = 14;                         // shared hash: 16384 slots, 64 KB
+constexpr uint32_t TL_SMEM_LIVE = (1u << TL_SMEM_LOG) / 2;   // load factor <= 1/2
+constexpr int TL_COUNT_CTAS_PER_SM = 3;                      // 64 KB of shared memory each
+constexpr double TL_WHOLE_RATIO = 128.0;                     // streamed / stored entries where the paths cross
+
+struct TlGroups {
+    const uint32_t *hv;                   // hashed vertex per group
+    const unsigned long long *pair_off;   // G + 1: scanned vertices of group g are pair_v[pair_off[g], pair_off[g+1])
+    const uint32_t *pair_v;
+    const unsigned long long *piece_off;  // P + 1
+    const uint32_t *unit_off;             // G + 1
+    const unsigned long long *gh_off;     // slot offset of the group's global table (~0: shared memory)
+    const uint32_t *tab_log;              // log2 of the table's slots
+    uint32_t *gh;                         // global tables
+    uint32_t G;
+};
+
+__device__ __forceinline__ uint32_t tl_hash(uint32_t w, uint32_t logc) { return (w * 0x9E3779B1u) >> (32 - logc); }
+
+__device__ __forceinline__ void tl_insert(uint32_t *tab, uint32_t logc, uint32_t w, uint32_t *err) {
+    const uint32_t mask = (1u << logc) - 1u;
+    uint32_t h = tl_hash(w, logc);
+    for (uint32_t i = 0; i <= mask; ++i) {
+        const uint32_t old = atomicCAS(tab + h, GV_NIL, w);
+        if (old == GV_NIL || old == w) return;
+        h = (h + 1u) & mask;
+    }
+    atomicOr(err, 2u);  // table full: live counts and entries disagree
+}
+
+__device__ __forceinline__ uint32_t tl_probe(const uint32_t *tab, uint32_t logc, uint32_t w) {
+    const uint32_t mask = (1u << logc) - 1u;
+    uint32_t h = tl_hash(w, logc);
+    for (uint32_t i = 0; i <= mask; ++i) {
+        const uint32_t x = tab[h];
+        if (x == w) return 1u;
+        if (x == GV_NIL) return 0u;
+        h = (h + 1u) & mask;
+    }
+    return 0u;
+}
+
+// Pool index of block kb0 + lane of a vertex, GV_NIL past its last block.
+__device__ __forceinline__ uint32_t tl_lane_block(const DevGraph &g, uint32_t root, uint32_t kb0, uint32_t nb) {
+    const uint32_t k = kb0 + (threadIdx.x & 31u);
+    if (k >= nb) return GV_NIL;
+    return k == 0 ? root : cbt_block(g.left, g.right, root, k);
+}
+
+// Calls f(w) for every live entry of blocks [kb0, kb0 + nblk) of a vertex
+// with `fill` used slots.  Block kb0 + r is held in `blk` by lane
+// lane_off + r (tl_lane_block of the run starting lane_off blocks earlier).
+// The warp reads each block with 16-byte loads (B/4 lanes per block).  Every
+// lane of the warp must call it with the same kb0 / lane_off / nblk.
+template <typename F>
+__device__ __forceinline__ void tl_scan_blocks(const DevGraph &g, uint32_t blk, uint32_t kb0, uint32_t lane_off,
+                                               uint32_t nblk, uint32_t fill, F &&f) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t lpb = min(32u, g.B >> 2), bpw = 32u / lpb, sub = lane / lpb, sl = lane % lpb;
+    for (uint32_t s0 = 0; s0 < nblk; s0 += bpw) {
+        const uint32_t kr = s0 + sub;
+        const uint32_t b = __shfl_sync(GV_FULL_MASK, blk, (lane_off + kr) & 31u);
+        if (kr < nblk) {
+            const uint32_t e = ((kb0 + kr) << g.logB) + sl * 4u;
+            if (e < fill) {
+                const uint4 q = *reinterpret_cast<const uint4 *>(g.pool + ((size_t)b << g.logB) + sl * 4u);
+                const uint32_t ev[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    if (e + j < fill && ev[j] != GV_TOMB) f(ev[j]);
+            }
+        }
+    }
+}
+
+__global__ void k_tl_deg(DevGraph g, const uint32_t *__restrict__ hv, uint32_t G, uint2 *__restrict__ du) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < G; i += gridDim.x * blockDim.x) {
+        const uint32_t u = hv[i];
+        if (u >= g.n) {
+            du[i] = make_uint2(GV_NIL, 0u);  // rejected on the host
+            continue;
+        }
+        const uint4 rec = g.vtx[u];
+        du[i] = make_uint2(rec.z, rec.y);  // live, fill
+    }
+}
+
+// Scan lists of the subset groups: pair_v = the live entries of N(u), and per
+// entry the pieces its own list takes.  One CTA per group, warps over blocks.
+__global__ void __launch_bounds__(TL_THREADS) k_tl_pairs(DevGraph g, TlGroups t, uint32_t *__restrict__ cursor,
+                                                         uint32_t *__restrict__ pair_v, uint32_t *__restrict__ pieces,
+                                                         unsigned long long *__restrict__ words) {
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nwarps = TL_THREADS / 32;
+    uint32_t *err = reinterpret_cast<uint32_t *>(words + 1);
+    unsigned long long blocks = 0;
+    for (uint32_t gi = blockIdx.x; gi < t.G; gi += gridDim.x) {
+        const uint32_t u = t.hv[gi];
+        const uint4 rec = g.vtx[u];
+        const uint32_t fill = rec.y, nb = blocks_for(fill, g.logB);
+        const unsigned long long p0 = t.pair_off[gi], cap = t.pair_off[gi + 1] - p0;
+        for (uint32_t kb = warp * TL_PIECE_BLOCKS; kb < nb; kb += nwarps * TL_PIECE_BLOCKS) {
+            const uint32_t blk = tl_lane_block(g, rec.x, kb, nb);
+            const uint32_t nblk = min(TL_PIECE_BLOCKS, nb - kb);
+            const uint32_t lpb = min(32u, g.B >> 2), bpw = 32u / lpb;
+            // one step = bpw blocks; every lane holds up to 4 entries
+            for (uint32_t s0 = 0; s0 < nblk; s0 += bpw) {
+                uint32_t mine[4];
+                uint32_t c = 0;
+                tl_scan_blocks(g, blk, kb + s0, s0, min(bpw, nblk - s0), fill, [&](uint32_t w) { mine[c++] = w; });
+                uint32_t incl = c;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t y = __shfl_up_sync(GV_FULL_MASK, incl, o);
+                    if (lane >= (uint32_t)o) incl += y;
+                }
+                const uint32_t tot = __shfl_sync(GV_FULL_MASK, incl, 31);
+                uint32_t base = 0;
+                if (lane == 0 && tot) base = atomicAdd(cursor + gi, tot);
+                base = __shfl_sync(GV_FULL_MASK, base, 0);
+                const uint32_t at = base + incl - c;
+                for (uint32_t j = 0; j < c; ++j) {
+                    if ((unsigned long long)(at + j) >= cap) {
+                        atomicOr(err, 1u);
+                        break;
+                    }
+                    const uint32_t w = mine[j];
+                    const uint32_t nbw = blocks_for(g.vtx[w].y, g.logB);
+                    pair_v[p0 + at + j] = w;
+                    pieces[p0 + at + j] = (nbw + TL_PIECE_BLOCKS - 1) / TL_PIECE_BLOCKS;
+                    blocks += nbw;
+                }
+            }
+        }
+    }
+    blocks = warp_sum(blocks);
+    if (lane == 0 && blocks) atomicAdd(words, blocks);
+}
+
+__global__ void k_tl_units(TlGroups t, uint32_t *__restrict__ units) {
+    for (uint32_t gi = blockIdx.x * blockDim.x + threadIdx.x; gi < t.G; gi += gridDim.x * blockDim.x) {
+        const unsigned long long np = t.piece_off[t.pair_off[gi + 1]] - t.piece_off[t.pair_off[gi]];
+        units[gi] = (uint32_t)((np + TL_UNIT_PIECES - 1) / TL_UNIT_PIECES);
+    }
+}
+
+// Inserts the live entries of N(hv) into a table: warps over 32-block runs.
+__device__ void tl_build(const DevGraph &g, uint32_t u, uint32_t *tab, uint32_t logc, uint32_t *err) {
+    const uint32_t warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const uint4 rec = g.vtx[u];
+    const uint32_t fill = rec.y, nb = blocks_for(fill, g.logB);
+    for (uint32_t kb = warp * TL_PIECE_BLOCKS; kb < nb; kb += nwarps * TL_PIECE_BLOCKS) {
+        const uint32_t blk = tl_lane_block(g, rec.x, kb, nb);
+        tl_scan_blocks(g, blk, kb, 0, min(TL_PIECE_BLOCKS, nb - kb), fill, [&](uint32_t w) { tl_insert(tab, logc, w, err); });
+    }
+}
+
+__global__ void __launch_bounds__(TL_THREADS) k_tl_gbuild(DevGraph g, TlGroups t, const uint32_t *__restrict__ big,
+                                                          uint32_t nbig, uint32_t *err) {
+    for (uint32_t b = blockIdx.x; b < nbig; b += gridDim.x) {
+        const uint32_t gi = big[b];
+        tl_build(g, t.hv[gi], t.gh + t.gh_off[gi], t.tab_log[gi], err);
+    }
+}
+
+template <bool SHARED>
+__device__ __forceinline__ uint32_t tl_count_pieces(const DevGraph &g, const TlGroups &t, const uint32_t *tab,
+                                                    uint32_t logc, unsigned long long lo, unsigned long long hi,
+                                                    unsigned long long pstart, const uint32_t *qpair) {
+    const uint32_t warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    uint32_t c = 0;
+    for (unsigned long long q = lo + warp; q < hi; q += nwarps) {
+        const unsigned long long p = pstart + qpair[q - lo];
+        const uint32_t v = t.pair_v[p];
+        const uint4 rec = g.vtx[v];
+        const uint32_t fill = rec.y, nb = blocks_for(fill, g.logB);
+        const uint32_t kb0 = (uint32_t)(q - t.piece_off[p]) * TL_PIECE_BLOCKS;
+        if (kb0 >= nb) continue;  // warp-uniform
+        const uint32_t blk = tl_lane_block(g, rec.x, kb0, nb);
+        tl_scan_blocks(g, blk, kb0, 0, min(TL_PIECE_BLOCKS, nb - kb0), fill, [&](uint32_t w) { c += tl_probe(tab, logc, w); });
+    }
+    return c;
+}
+
+__global__ void __launch_bounds__(TL_THREADS) k_tl_count(DevGraph g, TlGroups t, uint32_t U,
+                                                         unsigned long long *__restrict__ cnt, uint32_t *err) {
+    extern __shared__ uint32_t stab[];
+    __shared__ uint32_t s_gi;
+    __shared__ unsigned long long s_pstart;
+    __shared__ uint32_t qpair[TL_UNIT_PIECES];
+    __shared__ uint32_t red[TL_THREADS / 32];
+    for (uint32_t unit = blockIdx.x; unit < U; unit += gridDim.x) {
+        if (threadIdx.x == 0) {
+            uint32_t lo = 0, hi = t.G;  // last group with unit_off <= unit
+            while (hi - lo > 1) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (t.unit_off[mid] <= unit) lo = mid;
+                else hi = mid;
+            }
+            s_gi = lo;
+        }
+        __syncthreads();
+        const uint32_t gi = s_gi;
+        const unsigned long long p0 = t.pair_off[gi], p1 = t.pair_off[gi + 1];
+        const unsigned long long lo = t.piece_off[p0] + (unsigned long long)(unit - t.unit_off[gi]) * TL_UNIT_PIECES;
+        const unsigned long long hi = min(lo + TL_UNIT_PIECES, t.piece_off[p1]);
+        if (threadIdx.x == 0) {
+            unsigned long long a = p0, b = p1;  // last pair with piece_off <= lo
+            while (b - a > 1) {
+                const unsigned long long mid = (a + b) >> 1;
+                if (t.piece_off[mid] <= lo) a = mid;
+                else b = mid;
+            }
+            s_pstart = a;
+        }
+        const uint32_t logc = t.tab_log[gi];
+        const bool shared = t.gh_off[gi] == ~0ull;
+        if (shared) {
+            for (uint32_t k = threadIdx.x; k < (1u << logc); k += blockDim.x) stab[k] = GV_NIL;
+        }
+        __syncthreads();
+        const unsigned long long pstart = s_pstart;
+        for (unsigned long long p = pstart + threadIdx.x; p < p1 && t.piece_off[p] < hi; p += blockDim.x) {
+            const unsigned long long a = max(t.piece_off[p], lo), b = min(t.piece_off[p + 1], hi);
+            for (unsigned long long q = a; q < b; ++q) qpair[q - lo] = (uint32_t)(p - pstart);
+        }
+        if (shared) tl_build(g, t.hv[gi], stab, logc, err);
+        __syncthreads();
+        uint32_t c = shared ? tl_count_pieces<true>(g, t, stab, logc, lo, hi, pstart, qpair)
+                            : tl_count_pieces<false>(g, t, t.gh + t.gh_off[gi], logc, lo, hi, pstart, qpair);
+        c = warp_sum(c);
+        if ((threadIdx.x & 31u) == 0) red[threadIdx.x >> 5] = c;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned long long tot = 0;
+            for (int w = 0; w < TL_THREADS / 32; ++w) tot += red[w];
+            if (tot) atomicAdd(cnt + gi, tot);
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void k_tl_out(const unsigned long long *__restrict__ cnt, uint32_t G, unsigned long long *__restrict__ out) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < G; i += gridDim.x * blockDim.x) out[i] = cnt[i] >> 1;
+}
+
+inline size_t al256(size_t x) { return (x + 255) & ~size_t(255); }
+
+uint32_t ceil_log2(uint64_t x) {
+    uint32_t l = 0;
+    while ((1ull << l) < x) ++l;
+    return l;
+}
+
+}  // namespace
+
+gv_status tc_local_subset(gv_graph *g, const uint32_t *d_sub, uint64_t ns, unsigned long long *d_out,
+                          cudaStream_t s, bool *done, bool force) {
+    *done = false;
+    const DevGraph &d = g->d;
+    if (ns == 0 || ns > 0xFFFFFFF0ull) return GV_OK;
+    const uint32_t G = (uint32_t)ns;
+    uint64_t live = 0;
+    {
+        Ctl c;
+        gv_status st = read_ctl(g, &c, s);
+        if (st != GV_OK) return st;
+        live = c.live_edges;
+    }
+    // group-sized arrays (aux slot 4)
+    const size_t o_du = 0, o_poff = o_du + al256(8ull * G), o_ghoff = o_poff + al256(8ull * (G + 1));
+    const size_t o_tlog = o_ghoff + al256(8ull * G), o_cur = o_tlog + al256(4ull * G);
+    const size_t o_uoff = o_cur + al256(4ull * G), o_cnt = o_uoff + al256(4ull * (G + 1));
+    const size_t o_words = o_cnt + al256(8ull * G), bytes4 = o_words + 256;
+    char *b4 = (char *)aux_scratch(g, 4, bytes4);
+    if (!b4) return GV_ERR_NOMEM;
+    uint2 *du = (uint2 *)(b4 + o_du);
+    GV_LAUNCH(k_tl_deg, grid_for(G, 256), 256, 0, s, d, d_sub, G, du);
+    std::vector<uint2> hdu(G);
+    cudaError_t e = cudaMemcpyAsync(hdu.data(), du, 8ull * G, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_status(e, "tc subset degrees");
+    std::vector<unsigned long long> poff(G + 1), ghoff(G);
+    std::vector<uint32_t> tlog(G), big;
+    unsigned long long gslots = 0;
+    poff[0] = 0;
+    for (uint32_t i = 0; i < G; ++i)
+        if (hdu[i].x == GV_NIL) {
+            set_error("subset vertex out of range");
+            return GV_ERR_INVALID;
+        }
+    for (uint32_t i = 0; i < G; ++i) {
+        const uint32_t lv = hdu[i].x;
+        poff[i + 1] = poff[i] + lv;
+        tlog[i] = std::max<uint32_t>(5, ceil_log2(2ull * lv));
+        if (lv > TL_SMEM_LIVE) {
+            ghoff[i] = gslots;
+            gslots += 1ull << tlog[i];
+            big.push_back(i);
+        } else {
+            ghoff[i] = ~0ull;
+        }
+    }
+    const uint64_t P = poff[G];
+    // the scan lists alone reach half of the store: the whole-graph count is cheaper
+    if (!force && P > live / 2) return GV_OK;
+    // list-sized arrays (aux slot 5)
+    const uint64_t scan_n = std::max<uint64_t>(P + 1, (uint64_t)G + 1);
+    const size_t o_pv = 0, o_pc = o_pv + al256(4ull * (P + 1)), o_qoff = o_pc + al256(4ull * (P + 1));
+    const size_t o_tmp = o_qoff + al256(8ull * (P + 1)), o_gh = o_tmp + al256(scan_scratch_bytes(scan_n));
+    const size_t o_big = o_gh + al256(4ull * gslots), bytes5 = o_big + al256(4ull * big.size() + 4);
+    char *b5 = (char *)aux_scratch(g, 5, bytes5);
+    if (!b5) return GV_ERR_NOMEM;
+    TlGroups t;
+    t.hv = d_sub;
+    t.pair_off = (const unsigned long long *)(b4 + o_poff);
+    t.pair_v = (const uint32_t *)(b5 + o_pv);
+    t.piece_off = (const unsigned long long *)(b5 + o_qoff);
+    t.unit_off = (const uint32_t *)(b4 + o_uoff);
+    t.gh_off = (const unsigned long long *)(b4 + o_ghoff);
+    t.tab_log = (const uint32_t *)(b4 + o_tlog);
+    t.gh = (uint32_t *)(b5 + o_gh);
+    t.G = G;
+    unsigned long long *words = (unsigned long long *)(b4 + o_words);
+    uint32_t *err = (uint32_t *)(words + 1);
+    uint32_t *units = (uint32_t *)(b4 + o_uoff);
+    unsigned long long *cnt = (unsigned long long *)(b4 + o_cnt);
+    e = cudaMemcpyAsync(b4 + o_poff, poff.data(), 8ull * (G + 1), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(b4 + o_ghoff, ghoff.data(), 8ull * G, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(b4 + o_tlog, tlog.data(), 4ull * G, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && !big.empty())
+        e = cudaMemcpyAsync(b5 + o_big, big.data(), 4ull * big.size(), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b4 + o_cur, 0, 4ull * G, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(cnt, 0, 8ull * G, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(words, 0, 16, s);
+    if (e != cudaSuccess) return cuda_status(e, "tc subset setup");
+    uint32_t *pv = (uint32_t *)(b5 + o_pv), *pc = (uint32_t *)(b5 + o_pc);
+    GV_LAUNCH(k_tl_pairs, std::min<uint32_t>(G, 148 * 8), TL_THREADS, 0, s, d, t, (uint32_t *)(b4 + o_cur), pv, pc, words);
+    scan_exclusive_u32_to_u64(pc, (unsigned long long *)(b5 + o_qoff), P, (unsigned long long *)(b5 + o_qoff) + P,
+                              b5 + o_tmp, s);
+    GV_LAUNCH(k_tl_units, grid_for(G, 256), 256, 0, s, t, units);
+    scan_exclusive_u32(units, units, G, units + G, b5 + o_tmp, s);
+    struct {
+        unsigned long long blocks, err;
+    } hw{};
+    uint32_t U = 0;
+    e = cudaMemcpyAsync(&hw, words, 16, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&U, units + G, 4, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_status(e, "tc subset plan");
+    if ((uint32_t)hw.err) {
+        set_error("tc subset: live counts and stored entries disagree");
+        return GV_ERR_STATE;
+    }
+    // Hub lists are read again and again from L2, so a streamed entry costs
+    // far less than one stored entry does in the whole-graph count (R-MAT
+    // scale 22, B200: 1.2e10 streamed entries in 99 ms against 208 ms for the
+    // whole-graph count of 1.3e8 entries).  Past TL_WHOLE_RATIO streamed
+    // entries per stored entry the whole-graph count wins.
+    if (!force && (double)hw.blocks * d.B > TL_WHOLE_RATIO * (double)live + (double)d.B * 1024.0) return GV_OK;
+    if (gslots) {
+        e = cudaMemsetAsync(t.gh, 0xFF, 4ull * gslots, s);
+        if (e != cudaSuccess) return cuda_status(e, "tc subset tables");
+        GV_LAUNCH(k_tl_gbuild, std::min<uint32_t>((uint32_t)big.size(), 148 * 4), TL_THREADS, 0, s, d, t,
+                  (const uint32_t *)(b5 + o_big), (uint32_t)big.size(), err);
+    }
+    if (U) {
+        const size_t smem = (1u << TL_SMEM_LOG) * 4u;
+        cudaFuncSetAttribute(k_tl_count, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        GV_LAUNCH(k_tl_count, std::min<uint32_t>(U, 148 * TL_COUNT_CTAS_PER_SM), TL_THREADS, smem, s, d, t, U, cnt, err);
+    }
+    GV_LAUNCH(k_tl_out, grid_for(G, 256), 256, 0, s, (const unsigned long long *)cnt, G, d_out);
+    uint32_t herr = 0;
+    e = cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_status(e, "tc subset count");
+    if (herr) {
+        set_error("tc subset: a neighbour table overflowed (live counts and stored entries disagree)");
+        return GV_ERR_STATE;
+    }
+    *done = true;
+    return GV_OK;
+}
+
+}  // namespace gv

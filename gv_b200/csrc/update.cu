@@ -488,7 +488,8 @@ __global__ void __launch_bounds__(BIG_THREADS) k_apply_big(DevGraph g, const uin
 // tail blocks that end up empty go back to the free stack and are unlinked
 // from their parents.  Replaces compactionVertexCentric
 // (src/dynamicStructure/kernels/delete_kernels.cu:50-261), which fills holes
-// from the tail and can drop live entries.
+// from the tail and can drop live entries when a hole and the tail entry
+// meet in the same block.
 template <int TPV>
 __global__ void __launch_bounds__(UPD_THREADS) k_compact(DevGraph g, uint32_t *__restrict__ big_list) {
     constexpr int GPC = UPD_THREADS / TPV;

@@ -137,7 +137,12 @@ gv_status gv_clear_affected(gv_graph *g, void *stream);
 /* Structural invariant check on the device: CBT child/predecessor links,
  * per-block counts, owners, live counts, and that used + free blocks cover
  * the pool exactly once.  Synchronous.  *violations = 0 on a sound store;
- * *first_code names the first failed check. */
+ * *first_code names the first failed check: 1 root/fill mismatch, 2 live >
+ * fill, 3 block index out of the pool, 4 wrong owner, 5 wrong block count,
+ * 6 wrong predecessor, 7/8 left/right child link disagrees with the CBT
+ * shape, 9 last-block record wrong, 10 live count wrong, 11 block not used
+ * or free exactly once, 12 free-stack entry out of the pool, 13 free-stack
+ * size inconsistent. */
 gv_status gv_check(gv_graph *g, uint64_t *violations, uint32_t *first_code,
                    uint32_t *first_vertex);
 

@@ -206,3 +206,37 @@ def test_wpr_forward_and_gradient():
         err = np.abs(gg - gref).max() / scale
         print(f"mode {mode}: max |grad - fp64| / max|grad| = {err:.3e}")
         assert err < 1e-4
+
+
+@pytest.mark.parametrize("mode", ["local", "global", ""])
+def test_triangle_subset_paths_agree(mode, monkeypatch):
+    """Both subset paths (neighbour hash sets, whole-graph oriented count) are
+    bit-exact; the graph has a hub above the shared-memory table (global
+    table path), tombstones from deletes without compaction, and the subset
+    repeats vertices."""
+    scale = 14
+    n = 1 << scale
+    s, d = rmat_graph(scale, 8, seed=31)
+    rng = np.random.default_rng(3)
+    hub = 77
+    nb = rng.choice(n, 9000, replace=False).astype(np.uint32)
+    nb = nb[nb != hub]
+    s = np.concatenate([s, np.full(len(nb), hub, np.uint32)])
+    d = np.concatenate([d, nb])
+    g = make_graph(n)
+    g.batch_insert(s, d)
+    o = oracle.OracleGraph(n)
+    o.insert(s, d)
+    off, dst, _ = o.export()
+    ds, dd = sample_existing(off, dst, 3000, rng)
+    g.batch_delete(ds, dd)
+    o.delete(ds, dd)
+    sub = np.concatenate([[hub], rng.choice(n, 400), nb[:60], [hub]]).astype(np.uint32)
+    if mode:
+        monkeypatch.setenv("GV_TC_SUBSET", mode)
+    got = g.tc_subset(sub)
+    assert np.array_equal(got, o.tc_incident(sub))
+    if mode == "local":
+        assert g.last_stat("tc_subset_local") == 1
+    elif mode == "global":
+        assert g.last_stat("tc_subset_local") == 0
