@@ -1,6 +1,6 @@
 // Analytics that traverse the edge-block CBT store directly: PageRank,
-// personalised PageRank, exact triangle counting, betweenness centrality and
-// weighted PageRank with its adjoint.
+// personalised PageRank, exact triangle counting and weighted PageRank with
+// its adjoint (betweenness centrality: bc.cu; subset triangles: tc_local.cu).
 //
 // Reference kernels replaced:
 //   PageRank   src/algorithm/pagerank/pr_kernel.cu:3-103, pagerank.cu:3-132
@@ -10,10 +10,6 @@
 //   TC         src/algorithm/tc/tc_kernel.cu:3-147 (triple linear scans,
 //              float counts) -> degree-oriented sorted snapshot + merge-path
 //              intersection, uint64 counts;
-//   BC         src/algorithm/bc/bc_kernel.cu:3-119, bc.cu:3-88 (one source
-//              per host loop, int sigma, unordered dependency pass) ->
-//              batched multi-source level-synchronous BFS with uint64 sigma
-//              and a level-ordered fp64 dependency sweep.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -35,11 +31,6 @@ constexpr int BIG_TAB_A = 1024;
 constexpr uint32_t LIGHT_FILL = 256;
 constexpr uint32_t TINY_FILL = 32;  // thread-per-vertex tier of the pull sweeps
 constexpr uint32_t HUB_FILL = 16384;
-constexpr int HV_THREADS = 512;
-// BFS levels, BC dependencies and the TC snapshot expand vertices with more
-// used slots than this with every CTA (of their source slot) instead of one
-// lane group.
-constexpr uint32_t BFS_LIGHT_FILL = 2048;
 
 // Lanes per block and blocks per warp step for the grid-cooperative paths.
 struct WarpBlocks {
@@ -1224,336 +1215,6 @@ gv_status tc_run(gv_graph *g, cudaStream_t s, bool incident, unsigned long long 
     return cuda_status(cudaGetLastError(), "tc launch");
 }
 
-// ------------------------------------------------------------------- BC
-// Batched multi-source BFS: source slot b of the batch owns rows b*n.. of
-// dist/sigma/delta and a BFS order queue; all slots advance one level per
-// launch (grid.y = slot).
-struct BcBufs {
-    int32_t *dist;
-    unsigned long long *sigma;
-    double *delta;
-    uint32_t *queue;              // BFS order per slot (levels contiguous)
-    unsigned long long *lstart;   // [slot][MAXL+1] level boundaries
-    unsigned long long *qtail;    // per slot
-    int *active;                  // any slot still expanding
-    double *bc;                   // fp64 accumulator (n)
-    uint32_t *hv;                 // [slot][n] frontier vertices routed to the hub kernels
-    unsigned long long *hv_cnt;   // per slot
-};
-
-constexpr int BC_MAXL = 4096;
-
-__device__ __forceinline__ void bfs_visit(uint32_t w, int32_t nl, unsigned long long sv, int32_t *dist,
-                                          unsigned long long *sigma, uint32_t *queue, unsigned long long *qtail) {
-    int32_t dw = dist[w];
-    if (dw < 0) {
-        dw = atomicCAS(&dist[w], -1, nl);
-        if (dw < 0) {
-            dw = nl;
-            queue[atomicAdd(qtail, 1ull)] = w;
-        }
-    }
-    if (dw == nl) atomicAdd(&sigma[w], sv);
-}
-
-template <int TPV>
-__global__ void __launch_bounds__(AN_THREADS) k_bfs_level(DevGraph g, BcBufs b, uint32_t level) {
-    constexpr int GPC = AN_THREADS / TPV;
-    __shared__ uint32_t tabs[GPC][BIG_BLOCKS];
-    const uint32_t slot = blockIdx.y, n = g.n;
-    const unsigned long long *ls = b.lstart + (size_t)slot * (BC_MAXL + 1);
-    const unsigned long long f0 = ls[level], f1 = ls[level + 1];
-    if (f0 >= f1) return;
-    int32_t *dist = b.dist + (size_t)slot * n;
-    unsigned long long *sigma = b.sigma + (size_t)slot * n;
-    uint32_t *queue = b.queue + (size_t)slot * n;
-    Group<TPV> G;
-    uint32_t *tab = tabs[threadIdx.x / TPV];
-    const int32_t nl = (int32_t)level + 1;
-    const unsigned long long ngroups = (unsigned long long)gridDim.x * GPC;
-    for (unsigned long long fi = f0 + (unsigned long long)blockIdx.x * GPC + threadIdx.x / TPV; fi < f1; fi += ngroups) {
-        const uint32_t v = queue[fi];
-        const unsigned long long sv = sigma[v];
-        const uint4 rec = g.vtx[v];
-        const uint32_t fill = rec.y, nb = blocks_for(fill, g.logB);
-        if (fill > BFS_LIGHT_FILL) {
-            if (G.gl == 0) b.hv[(size_t)slot * n + atomicAdd(&b.hv_cnt[slot], 1ull)] = v;
-            continue;
-        }
-        fill_block_table(g, rec.x, 0, nb, tab, G.gl, TPV);
-        G.sync();
-        for (uint32_t e = G.gl; e < fill; e += TPV) {
-            const uint32_t w = g.pool[((size_t)tab[e >> g.logB] << g.logB) + (e & (g.B - 1))];
-            if (w != GV_TOMB) bfs_visit(w, nl, sv, dist, sigma, queue, &b.qtail[slot]);
-        }
-        G.sync();
-    }
-}
-
-// Heavy frontier vertices of one level: all CTAs of the slot split their blocks.
-__global__ void __launch_bounds__(HV_THREADS) k_bfs_hub(DevGraph g, BcBufs b, uint32_t level) {
-    const uint32_t slot = blockIdx.y, n = g.n;
-    const uint32_t cnt = (uint32_t)b.hv_cnt[slot];
-    if (cnt == 0) return;
-    int32_t *dist = b.dist + (size_t)slot * n;
-    unsigned long long *sigma = b.sigma + (size_t)slot * n;
-    uint32_t *queue = b.queue + (size_t)slot * n;
-    const uint32_t *hv = b.hv + (size_t)slot * n;
-    const int32_t nl = (int32_t)level + 1;
-    WarpBlocks W(g.B);
-    const uint32_t gw = blockIdx.x * (HV_THREADS / 32) + (threadIdx.x >> 5), nw = gridDim.x * (HV_THREADS / 32);
-    for (uint32_t h = 0; h < cnt; ++h) {
-        const uint32_t v = hv[h];
-        const unsigned long long sv = sigma[v];
-        const uint4 rec = g.vtx[v];
-        const uint32_t fill = rec.y, nb = blocks_for(fill, g.logB);
-        for (uint32_t k0 = gw * W.bpw; k0 < nb; k0 += nw * W.bpw) {
-            const uint32_t k = k0 + W.sub;
-            if (k >= nb) continue;
-            const uint32_t blk = (k == 0) ? rec.x : cbt_block(g.left, g.right, rec.x, k);
-            const uint32_t slots = min(g.B, fill - (k << g.logB));
-            const size_t base = (size_t)blk << g.logB;
-            for (uint32_t e = W.sl * 4; e < slots; e += W.lpb * 4) {
-                const uint4 q = *reinterpret_cast<const uint4 *>(g.pool + base + e);
-                const uint32_t ev[4] = {q.x, q.y, q.z, q.w};
-#pragma unroll
-                for (int j = 0; j < 4; ++j)
-                    if (e + j < slots && ev[j] != GV_TOMB) bfs_visit(ev[j], nl, sv, dist, sigma, queue, &b.qtail[slot]);
-            }
-        }
-    }
-}
-
-// Closes a level for every slot: records where the next level ends.
-__global__ void k_bfs_close(BcBufs b, uint32_t nslots, uint32_t level) {
-    const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
-    if (slot >= nslots) return;
-    unsigned long long *ls = b.lstart + (size_t)slot * (BC_MAXL + 1);
-    const unsigned long long t = b.qtail[slot];
-    ls[level + 2] = t;
-    b.hv_cnt[slot] = 0;
-    if (t > ls[level + 1]) atomicOr(b.active, 1);
-}
-
-__global__ void k_bfs_init(BcBufs b, uint32_t n, const uint32_t *__restrict__ sources, uint32_t nslots) {
-    const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
-    if (slot >= nslots) return;
-    const uint32_t s = sources[slot];
-    b.dist[(size_t)slot * n + s] = 0;
-    b.sigma[(size_t)slot * n + s] = 1ull;
-    b.queue[(size_t)slot * n] = s;
-    b.qtail[slot] = 1;
-    unsigned long long *ls = b.lstart + (size_t)slot * (BC_MAXL + 1);
-    ls[0] = 0;
-    ls[1] = 1;
-}
-
-template <int TPV>
-__global__ void __launch_bounds__(AN_THREADS) k_bc_dep(DevGraph g, BcBufs b, uint32_t level) {
-    constexpr int GPC = AN_THREADS / TPV;
-    __shared__ uint32_t tabs[GPC][BIG_BLOCKS];
-    const uint32_t slot = blockIdx.y, n = g.n;
-    const unsigned long long *ls = b.lstart + (size_t)slot * (BC_MAXL + 1);
-    const unsigned long long f0 = ls[level], f1 = ls[level + 1];
-    if (f0 >= f1) return;
-    const int32_t *dist = b.dist + (size_t)slot * n;
-    const unsigned long long *sigma = b.sigma + (size_t)slot * n;
-    double *delta = b.delta + (size_t)slot * n;
-    const uint32_t *queue = b.queue + (size_t)slot * n;
-    Group<TPV> G;
-    uint32_t *tab = tabs[threadIdx.x / TPV];
-    const int32_t nl = (int32_t)level + 1;
-    const unsigned long long ngroups = (unsigned long long)gridDim.x * GPC;
-    for (unsigned long long fi = f0 + (unsigned long long)blockIdx.x * GPC + threadIdx.x / TPV; fi < f1; fi += ngroups) {
-        const uint32_t v = queue[fi];
-        const double sv = (double)sigma[v];
-        const uint4 rec = g.vtx[v];
-        const uint32_t fill = rec.y, nb = blocks_for(fill, g.logB);
-        if (fill > BFS_LIGHT_FILL) {
-            if (G.gl == 0) b.hv[(size_t)slot * n + atomicAdd(&b.hv_cnt[slot], 1ull)] = v;
-            continue;
-        }
-        double acc = 0.0;
-        fill_block_table(g, rec.x, 0, nb, tab, G.gl, TPV);
-        G.sync();
-        for (uint32_t e = G.gl; e < fill; e += TPV) {
-            const uint32_t w = g.pool[((size_t)tab[e >> g.logB] << g.logB) + (e & (g.B - 1))];
-            if (w != GV_TOMB && dist[w] == nl) acc += (sv / (double)sigma[w]) * (1.0 + delta[w]);
-        }
-        G.sync();
-        acc = G.sum(acc);
-        if (G.gl == 0) delta[v] = acc;
-    }
-}
-
-// Heavy vertices of one dependency level: every CTA of the slot adds a warp
-// partial per block share into delta[v] (fp64 atomics; delta of heavy
-// vertices starts at zero).
-__global__ void __launch_bounds__(HV_THREADS) k_bc_dep_hub(DevGraph g, BcBufs b, uint32_t level) {
-    const uint32_t slot = blockIdx.y, n = g.n;
-    const uint32_t cnt = (uint32_t)b.hv_cnt[slot];
-    if (cnt == 0) return;
-    const int32_t *dist = b.dist + (size_t)slot * n;
-    const unsigned long long *sigma = b.sigma + (size_t)slot * n;
-    double *delta = b.delta + (size_t)slot * n;
-    const uint32_t *hv = b.hv + (size_t)slot * n;
-    const int32_t nl = (int32_t)level + 1;
-    WarpBlocks W(g.B);
-    const uint32_t lane = threadIdx.x & 31;
-    const uint32_t gw = blockIdx.x * (HV_THREADS / 32) + (threadIdx.x >> 5), nw = gridDim.x * (HV_THREADS / 32);
-    for (uint32_t h = 0; h < cnt; ++h) {
-        const uint32_t v = hv[h];
-        const double sv = (double)sigma[v];
-        const uint4 rec = g.vtx[v];
-        const uint32_t fill = rec.y, nb = blocks_for(fill, g.logB);
-        double acc = 0.0;
-        bool any = false;
-        for (uint32_t k0 = gw * W.bpw; k0 < nb; k0 += nw * W.bpw) {
-            any = true;
-            const uint32_t k = k0 + W.sub;
-            if (k >= nb) continue;
-            const uint32_t blk = (k == 0) ? rec.x : cbt_block(g.left, g.right, rec.x, k);
-            const uint32_t slots = min(g.B, fill - (k << g.logB));
-            const size_t base = (size_t)blk << g.logB;
-            for (uint32_t e = W.sl * 4; e < slots; e += W.lpb * 4) {
-                const uint4 q = *reinterpret_cast<const uint4 *>(g.pool + base + e);
-                const uint32_t ev[4] = {q.x, q.y, q.z, q.w};
-#pragma unroll
-                for (int j = 0; j < 4; ++j)
-                    if (e + j < slots && ev[j] != GV_TOMB && dist[ev[j]] == nl)
-                        acc += (sv / (double)sigma[ev[j]]) * (1.0 + delta[ev[j]]);
-            }
-        }
-        if (!any) continue;  // warp-uniform
-        acc = warp_sum(acc);
-        if (lane == 0 && acc != 0.0) atomicAdd(&delta[v], acc);
-    }
-}
-
-// bc[v] += sum over slots of delta (fixed slot order), skipping each slot's source.
-__global__ void k_bc_reduce(BcBufs b, uint32_t n, uint32_t nslots, const uint32_t *__restrict__ sources) {
-    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
-        double t = 0.0;
-        for (uint32_t s = 0; s < nslots; ++s)
-            if (sources[s] != v && b.dist[(size_t)s * n + v] > 0) t += b.delta[(size_t)s * n + v];
-        b.bc[v] += t;
-    }
-}
-
-__global__ void k_f64_to_f32(const double *__restrict__ x, float *__restrict__ y, uint32_t n) {
-    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) y[v] = (float)x[v];
-}
-
-// Runs forward BFS for a batch of sources; returns the deepest level count.
-gv_status bfs_batch(gv_graph *g, cudaStream_t s, BcBufs &b, const uint32_t *dsrc, uint32_t nslots, uint32_t *depth_out,
-                    int *h_active) {
-    DevGraph d = g->d;
-    const uint32_t n = d.n;
-    cudaMemsetAsync(b.dist, 0xFF, (size_t)nslots * n * 4, s);
-    cudaMemsetAsync(b.sigma, 0, (size_t)nslots * n * 8, s);
-    cudaMemsetAsync(b.hv_cnt, 0, (size_t)nslots * 8, s);
-    GV_LAUNCH(k_bfs_init, (nslots + 63) / 64, 64, 0, s, b, n, dsrc, nslots);
-    uint32_t level = 0;
-    const unsigned gx = grid_for((uint64_t)n, AN_THREADS, 148 * 8 / std::max(1u, nslots) + 1);
-    const unsigned hx = std::max(1u, 148u * 2 / std::max(1u, nslots));
-    while (true) {
-        const int chunk = 4;
-        cudaMemsetAsync(b.active, 0, 4, s);
-        for (int i = 0; i < chunk; ++i) {
-            if (level + 2 > BC_MAXL) { set_error("BFS deeper than the level table"); return GV_ERR_UNSUPPORTED; }
-            {
-                ProfScope ps(PROF_BFS_LEVEL, s);
-                dispatch_tpv(g->cfg.threads_per_vertex, [&](auto t) {
-                    constexpr int T = decltype(t)::value;
-                    GV_LAUNCH((k_bfs_level<T>), dim3(gx, nslots), AN_THREADS, 0, s, d, b, level);
-                });
-                GV_LAUNCH(k_bfs_hub, dim3(hx, nslots), HV_THREADS, 0, s, d, b, level);
-            }
-            GV_LAUNCH(k_bfs_close, (nslots + 63) / 64, 64, 0, s, b, nslots, level);
-            ++level;
-        }
-        cudaError_t e = cudaMemcpyAsync(h_active, b.active, 4, cudaMemcpyDeviceToHost, s);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-        if (e != cudaSuccess) return cuda_status(e, "bfs");
-        if (!*h_active) break;
-    }
-    *depth_out = level;
-    return GV_OK;
-}
-
-gv_status bc_impl(gv_graph *g, const uint32_t *sources, uint64_t ns, float *bc_out, int mem, cudaStream_t s) {
-    DevGraph d = g->d;
-    const uint32_t n = d.n;
-    std::vector<uint32_t> src_all;
-    const uint32_t *hs = sources;
-    if (!sources || ns == 0) {
-        src_all.resize(n);
-        for (uint32_t i = 0; i < n; ++i) src_all[i] = i;
-        hs = src_all.data();
-        ns = n;
-    } else if (mem == GV_MEM_DEVICE) {
-        src_all.resize(ns);
-        cudaMemcpy(src_all.data(), sources, ns * 4, cudaMemcpyDeviceToHost);
-        hs = src_all.data();
-    }
-    for (uint64_t i = 0; i < ns; ++i)
-        if (hs[i] >= n) { set_error("BC source out of range"); return GV_ERR_INVALID; }
-    // slots per batch: bounded by memory (~24 B per vertex per slot)
-    uint64_t slots = 64;
-    const uint64_t per_slot = (uint64_t)n * (4 + 8 + 8 + 4 + 4) + (BC_MAXL + 1) * 8 + 16 + 8;
-    size_t fr = 0, tot = 0;
-    cudaMemGetInfo(&fr, &tot);
-    while (slots > 1 && slots * per_slot > fr / 4) slots >>= 1;
-    if (slots > ns) slots = ns;
-    const size_t bytes = slots * per_slot + (size_t)n * 8 + slots * 4 + 256;
-    void *buf = analytics_scratch(g, bytes);
-    if (!buf) return GV_ERR_NOMEM;
-    char *p = (char *)buf;
-    BcBufs b;
-    b.bc = (double *)p; p += (size_t)n * 8;
-    b.delta = (double *)p; p += slots * n * 8;
-    b.sigma = (unsigned long long *)p; p += slots * n * 8;
-    b.lstart = (unsigned long long *)p; p += slots * (BC_MAXL + 1) * 8;
-    b.qtail = (unsigned long long *)p; p += slots * 8;
-    b.hv_cnt = (unsigned long long *)p; p += slots * 8;
-    b.dist = (int32_t *)p; p += slots * n * 4;
-    b.queue = (uint32_t *)p; p += slots * n * 4;
-    b.hv = (uint32_t *)p; p += slots * n * 4;
-    b.active = (int *)p; p += 16;
-    uint32_t *dsrc = (uint32_t *)p;
-    cudaMemsetAsync(b.bc, 0, (size_t)n * 8, s);
-    std::vector<unsigned long long> hls;
-    int *h_active = nullptr;
-    cudaMallocHost(&h_active, 16);
-    gv_status st = GV_OK;
-    for (uint64_t s0 = 0; s0 < ns; s0 += slots) {
-        const uint32_t nsl = (uint32_t)std::min<uint64_t>(slots, ns - s0);
-        cudaMemcpyAsync(dsrc, hs + s0, nsl * 4, cudaMemcpyHostToDevice, s);
-        uint32_t depth = 0;
-        st = bfs_batch(g, s, b, dsrc, nsl, &depth, h_active);
-        if (st != GV_OK) break;
-        cudaMemsetAsync(b.delta, 0, (size_t)nsl * n * 8, s);
-        cudaMemsetAsync(b.hv_cnt, 0, (size_t)nsl * 8, s);
-        const unsigned gx = grid_for((uint64_t)n, AN_THREADS, 148 * 8 / std::max(1u, nsl) + 1);
-        const unsigned hx = std::max(1u, 148u * 2 / std::max(1u, nsl));
-        for (int32_t lv = (int32_t)depth; lv >= 0; --lv) {
-            ProfScope ps(PROF_BC_DEP, s);
-            dispatch_tpv(g->cfg.threads_per_vertex, [&](auto t) {
-                constexpr int T = decltype(t)::value;
-                GV_LAUNCH((k_bc_dep<T>), dim3(gx, nsl), AN_THREADS, 0, s, d, b, (uint32_t)lv);
-            });
-            GV_LAUNCH(k_bc_dep_hub, dim3(hx, nsl), HV_THREADS, 0, s, d, b, (uint32_t)lv);
-            cudaMemsetAsync(b.hv_cnt, 0, (size_t)nsl * 8, s);
-        }
-        GV_LAUNCH(k_bc_reduce, grid_for(n, 256), 256, 0, s, b, n, nsl, (const uint32_t *)dsrc);
-    }
-    cudaFreeHost(h_active);
-    if (st != GV_OK) return st;
-    float *tmp = (float *)b.dist;  // reuse: n floats fit in the dist rows
-    GV_LAUNCH(k_f64_to_f32, grid_for(n, 256), 256, 0, s, (const double *)b.bc, tmp, n);
-    return copy_out_f32(tmp, bc_out, n, mem, s);
-}
-
 // ------------------------------------------------------- weighted PageRank
 __global__ void k_row_sums(DevGraph g, float *__restrict__ rinv) {
     for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < g.n; u += gridDim.x * blockDim.x) {
@@ -1971,45 +1632,6 @@ gv_status gv_tc_subset(gv_graph *g, const uint32_t *subset, uint64_t ns, uint64_
     if (mem != GV_MEM_DEVICE) e = cudaMemcpyAsync(out, dout, ns * 8, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     return cuda_status(e, "tc subset");
-}
-
-gv_status gv_bc(gv_graph *g, const uint32_t *sources, uint64_t ns, float *bc_out, int mem, void *stream) {
-    if (!g || !bc_out) return GV_ERR_INVALID;
-    return bc_impl(g, sources, ns, bc_out, mem, (cudaStream_t)stream);
-}
-
-gv_status gv_bfs_sigma(gv_graph *g, uint32_t source, int32_t *dist, uint64_t *sigma, int mem, void *stream) {
-    if (!g || !dist || !sigma || source >= g->d.n) return GV_ERR_INVALID;
-    cudaStream_t s = (cudaStream_t)stream;
-    const uint32_t n = g->d.n;
-    const size_t bytes = (size_t)n * (4 + 8 + 8 + 4 + 4) + (BC_MAXL + 1) * 8 + 256;
-    void *buf = analytics_scratch(g, bytes);
-    if (!buf) return GV_ERR_NOMEM;
-    char *p = (char *)buf;
-    BcBufs b;
-    b.bc = nullptr;
-    b.delta = nullptr;
-    b.sigma = (unsigned long long *)p; p += (size_t)n * 8;
-    b.lstart = (unsigned long long *)p; p += (BC_MAXL + 1) * 8;
-    b.qtail = (unsigned long long *)p; p += 8;
-    b.hv_cnt = (unsigned long long *)p; p += 8;
-    b.dist = (int32_t *)p; p += (size_t)n * 4;
-    b.queue = (uint32_t *)p; p += (size_t)n * 4;
-    b.hv = (uint32_t *)p; p += (size_t)n * 4;
-    b.active = (int *)p; p += 16;
-    uint32_t *dsrc = (uint32_t *)p;
-    cudaMemcpyAsync(dsrc, &source, 4, cudaMemcpyHostToDevice, s);
-    int *h_active = nullptr;
-    cudaMallocHost(&h_active, 16);
-    uint32_t depth = 0;
-    gv_status st = bfs_batch(g, s, b, dsrc, 1, &depth, h_active);
-    cudaFreeHost(h_active);
-    if (st != GV_OK) return st;
-    const cudaMemcpyKind k = mem == GV_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
-    cudaError_t e = cudaMemcpyAsync(dist, b.dist, (size_t)n * 4, k, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(sigma, b.sigma, (size_t)n * 8, k, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    return cuda_status(e, "bfs sigma");
 }
 
 gv_status gv_wpr_forward(gv_graph *g, float alpha, float tol, int32_t max_iter, float *x_out, int32_t *sweeps, int mem,

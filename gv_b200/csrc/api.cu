@@ -410,6 +410,7 @@ gv_status gv_destroy(gv_graph *g) {
         dfree(g->bs.scan_tmp);
         dfree(g->bs.tile_cnt);
         if (g->an_buf) cudaFree(g->an_buf);
+        if (g->host_pinned) cudaFreeHost(g->host_pinned);
         for (int i = 0; i < gv_graph::AUX_SLOTS; ++i)
             if (g->aux[i]) cudaFree(g->aux[i]);
         delete g;

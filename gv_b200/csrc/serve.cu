@@ -57,7 +57,7 @@ struct Server {
         switch (kind) {
             case GV_REQ_PPR: return 16ull * n * k + 16ull * n;
             case GV_REQ_TC: return 64ull * n + 8ull * g->d.P * g->d.B / 2;
-            default: return 32ull * 28ull * n + 16ull * n;  // BC, 32 sources
+            default: return 256ull * n + 4ull * 32 * n + 40ull * n;  // BC: sigma rows, 32 level masks, lists
         }
     }
 
