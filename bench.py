@@ -56,6 +56,12 @@ def parse():
     ap.add_argument("--no-batching", action="store_true", help="skip the scale-24 batched-vs-plain section")
     ap.add_argument("--batch-scale", type=int, default=24)
     ap.add_argument("--c3-batches", type=int, default=64)
+    ap.add_argument("--no-serving", action="store_true", help="skip the scale-25 serving section")
+    ap.add_argument("--serve-scale", type=int, default=25)
+    ap.add_argument("--serve-requests", type=int, default=120)
+    ap.add_argument("--serve-slots", type=int, default=4)
+    ap.add_argument("--serve-load", type=float, default=0.7, help="Poisson rate as a fraction of served capacity")
+    ap.add_argument("--serve-hbm", type=int, default=96, help="GB of HBM the serving loop may give queries")
     return ap.parse_args()
 
 
@@ -340,6 +346,158 @@ def run_batching(args, dev):
             "autotune_best": best, "autotune": tune}
 
 
+def make_serve_trace(n, s_dev, d_dev, nreq, seed):
+    """Serving requests: 60% update batches (log-uniform 1K-1M updates, half
+    inserts of uniform-random pairs, half deletes sampled from the graph's
+    generated pairs), 40% queries split evenly between PPR from a random
+    source, incident triangles of 10K random vertices and BC from 32 sampled
+    sources.  Arrival times are set by the caller."""
+    import torch
+    import gv_b200
+    rng = np.random.default_rng(seed)
+    items = []
+    m = len(s_dev)
+    for _ in range(nreq):
+        r = rng.random()
+        if r < 0.6:
+            k = int(np.exp(rng.uniform(np.log(1e3), np.log(1e6))))
+            ni = k // 2
+            ins_s, ins_d = gv_b200.gen_uniform(n, ni, seed=int(rng.integers(1 << 62)))
+            idx = torch.from_numpy(rng.integers(0, m, k - ni)).to(s_dev.device)
+            del_s = s_dev[idx].cpu().numpy().view(np.uint32)
+            del_d = d_dev[idx].cpu().numpy().view(np.uint32)
+            items.append(("update", ins_s, ins_d, del_s, del_d))
+        elif r < 0.6 + 0.4 / 3:
+            items.append(("ppr", int(rng.integers(n))))
+        elif r < 0.6 + 0.8 / 3:
+            v = np.unique(rng.integers(0, n, 10_200))[:10_000]
+            items.append(("tc", rng.permutation(v).astype(np.uint32)))
+        else:
+            items.append(("bc", np.unique(rng.integers(0, n, 40))[:32].astype(np.uint32)))
+    return items
+
+
+def _pct(a, q):
+    return float(np.percentile(np.asarray(a), q)) if len(a) else None
+
+
+def run_serving(args, dev):
+    """Serving workload: a resident R-MAT scale-25 graph and a seeded request
+    trace.  plain = every request through its own synchronous call in trace
+    order; served = gv_serve_trace with everything arrived (throughput); paced
+    = gv_serve_trace with Poisson arrivals at a fraction of the served
+    capacity (p50 / p99 latency)."""
+    import torch
+    import gv_b200
+    scale = args.serve_scale
+    n = 1 << scale
+    seed = args.seed + 200
+    cfg = dict(block_size=args.block, threads_per_vertex=args.tpv, hbm_budget_bytes=48 << 30,
+               max_batch_pairs=1 << 22, device=dev.index or 0)
+    s_dev, d_dev = gv_b200.gen_rmat(scale, args.edge_factor << scale, seed, device=dev)
+    items = make_serve_trace(n, s_dev, d_dev, args.serve_requests, seed)
+    kinds = [it[0] for it in items]
+    upd_pairs = sum(len(it[1]) + len(it[3]) for it in items if it[0] == "update")
+
+    def build():
+        g = gv_b200.GraphVine(n, **cfg)
+        insert_chunked(g, s_dev, d_dev)
+        g.compaction()
+        g.synchronize()
+        return g
+
+    # plain: one synchronous call per request, results left on the device
+    g = build()
+    m0 = g.num_edges()
+    xq = torch.empty(n, dtype=torch.float32, device=dev)
+    bq = torch.empty(n, dtype=torch.float32, device=dev)
+    lib = gv_b200._lib.lib()
+    t_kind = {"update": 0.0, "ppr": 0.0, "tc": 0.0, "bc": 0.0}
+    ppr_edges = 0
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for it in items:
+        ta = time.perf_counter()
+        if it[0] == "update":
+            g.batch_insert(it[1], it[2])
+            g.batch_delete(it[3], it[4])
+            g.compaction()
+            g.synchronize()
+        elif it[0] == "ppr":
+            _, sw = g.ppr(it[1], ALPHA, EPS, MAX_ITER, out=xq)
+            ppr_edges += m0 * sw
+        elif it[0] == "tc":
+            g.tc_subset(it[1])
+        else:
+            src = torch.from_numpy(np.ascontiguousarray(it[1], np.uint32).view(np.int32)).to(dev)
+            gv_b200._check(lib.gv_bc(g._h, src.data_ptr(), len(src), bq.data_ptr(), gv_b200.GV_MEM_DEVICE, 0),
+                           "gv_bc")
+            torch.cuda.synchronize()
+        t_kind[it[0]] += time.perf_counter() - ta
+    plain_s = time.perf_counter() - t0
+    g.close()
+
+    # served, everything arrived at t = 0
+    def trace(arrivals):
+        return [it + (float(a),) for it, a in zip(items, arrivals)]
+
+    g = build()
+    t0 = time.perf_counter()
+    res, _ = g.serve(trace(np.zeros(len(items))), slots=args.serve_slots, ppr_batch=32, pace=False,
+                     alpha=ALPHA, epsilon=EPS, max_iter=MAX_ITER, hbm_budget_bytes=args.serve_hbm << 30)
+    served_s = time.perf_counter() - t0
+    g.close()
+    assert np.all(res["status"] == 0)
+
+    def group_time(res, kind):
+        spans = {}
+        for i, k in enumerate(kinds):
+            if k == kind:
+                spans[int(res["group"][i])] = float(res["done_s"][i] - res["start_s"][i])
+        return sum(spans.values())
+
+    ppr_edges_served = sum(m0 * int(res["sweeps"][i]) for i, k in enumerate(kinds) if k == "ppr")
+    served = {"makespan_s": served_s, "requests_per_s": len(items) / served_s,
+              "updates_per_s": upd_pairs / served_s,
+              "update_engine_updates_per_s": upd_pairs / max(group_time(res, "update"), 1e-9),
+              "ppr_gteps": ppr_edges_served / max(group_time(res, "ppr"), 1e-9) / 1e9,
+              "groups": int(len(np.unique(res["group"])))}
+    plain = {"makespan_s": plain_s, "requests_per_s": len(items) / plain_s, "updates_per_s": upd_pairs / plain_s,
+             "update_engine_updates_per_s": upd_pairs / max(t_kind["update"], 1e-9),
+             "ppr_gteps": ppr_edges / max(t_kind["ppr"], 1e-9) / 1e9,
+             "seconds_by_kind": t_kind}
+
+    # paced: Poisson arrivals at a fraction of the served capacity
+    rate = args.serve_load * len(items) / served_s
+    arr = np.cumsum(np.random.default_rng(seed + 1).exponential(1.0 / rate, len(items)))
+    arr -= arr[0]
+    g = build()
+    res, _ = g.serve(trace(arr), slots=args.serve_slots, ppr_batch=32, pace=True, alpha=ALPHA, epsilon=EPS,
+                     max_iter=MAX_ITER, hbm_budget_bytes=args.serve_hbm << 30)
+    g.close()
+    del s_dev, d_dev
+    torch.cuda.empty_cache()
+    lat = res["latency_ms"]
+    span = float(res["done_s"].max() - arr[0])
+    per_kind = {}
+    for k in ("update", "ppr", "tc", "bc"):
+        sel = [lat[i] for i in range(len(items)) if kinds[i] == k]
+        per_kind[k] = {"count": len(sel), "p50_ms": _pct(sel, 50), "p99_ms": _pct(sel, 99)}
+    return {"workload": (f"R-MAT scale {scale} ef {args.edge_factor} resident; {len(items)} requests: 60% update "
+                         f"batches (log-uniform 1K-1M updates, 50/50), 40% queries (PPR / TC over 10K vertices / "
+                         f"BC from 32 sources)"),
+            "m_initial_entries": m0, "update_pairs": upd_pairs,
+            "mix": {k: kinds.count(k) for k in ("update", "ppr", "tc", "bc")},
+            "plain": plain, "served": served,
+            "served_vs_plain": {"requests": plain_s / served_s,
+                                "updates_per_s": served["updates_per_s"] / plain["updates_per_s"],
+                                "ppr_gteps": served["ppr_gteps"] / plain["ppr_gteps"] if plain["ppr_gteps"] else None},
+            "paced": {"poisson_rate_per_s": rate, "load": args.serve_load, "slots": args.serve_slots,
+                      "hbm_budget_gb": args.serve_hbm, "p50_ms": _pct(lat, 50), "p99_ms": _pct(lat, 99),
+                      "throughput_requests_per_s": len(items) / span, "updates_per_s": upd_pairs / span,
+                      "by_kind": per_kind}}
+
+
 # ------------------------------------------------------------------ GPU leg
 def run_gv(args, rank, world, local_rank):
     import torch
@@ -507,6 +665,8 @@ def run_gv(args, rank, world, local_rank):
                        "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"]}
     if world == 1 and not args.no_batching:
         line["batching"] = run_batching(args, torch.device("cuda", local_rank))
+    if world == 1 and not args.no_serving:
+        line["serving"] = run_serving(args, torch.device("cuda", local_rank))
     if world == 1 and not args.no_cpu_baseline:
         import gv_b200 as gvb
         pairs = gvb.gen_rmat(args.scale, args.edge_factor << args.scale, seed)

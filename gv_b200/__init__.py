@@ -405,7 +405,7 @@ class GraphVine:
     # -- serving -----------------------------------------------------------
     def serve(self, trace, *, slots: int = 4, ppr_batch: int = 32, max_coalesce: int = 64, pace: bool = True,
               hbm_budget_bytes: int = 32 << 30, alpha: float = 0.85, epsilon: float = 1e-6, max_iter: int = 100,
-              outputs: bool = False):
+              outputs: bool = False, fresh: bool = True):
         """Run a request trace through gv_serve_trace.
 
         trace items (arrival_s last, non-decreasing):
@@ -413,9 +413,12 @@ class GraphVine:
           ("ppr", source, arrival_s)
           ("tc", vertices, arrival_s)      incident-triangle counts of the vertices
           ("bc", sources, arrival_s)       betweenness from the given sources
+        fresh=True lets a query see updates that arrived after it (never fewer
+        than those before it); fresh=False gives it exactly those before it.
         Returns (results, outs): results a structured array with start_s, done_s,
-        latency_ms, epoch, status, sweeps, group per request; outs a list with
-        each query's result (None for updates) when outputs=True."""
+        latency_ms, epoch, status, sweeps, group per request (epoch = update
+        requests, in trace order, applied before the query ran); outs a list
+        with each query's result (None for updates) when outputs=True."""
         kinds = {"update": _lib.GV_REQ_UPDATE, "ppr": _lib.GV_REQ_PPR, "tc": _lib.GV_REQ_TC, "bc": _lib.GV_REQ_BC}
         nreq = len(trace)
         reqs = (_lib.gv_request * max(nreq, 1))()
@@ -446,6 +449,7 @@ class GraphVine:
         _check(L.gv_serve_config_init(C.byref(cfg)), "gv_serve_config_init")
         cfg.slots, cfg.ppr_batch, cfg.max_coalesce, cfg.pace = slots, ppr_batch, max_coalesce, int(pace)
         cfg.hbm_budget_bytes, cfg.alpha, cfg.epsilon, cfg.max_iter = hbm_budget_bytes, alpha, epsilon, max_iter
+        cfg.fresh = int(fresh)
         res = (_lib.gv_request_result * max(nreq, 1))()
         outs_list = [None] * nreq
         po = None

@@ -57,7 +57,7 @@ class gv_request_result(C.Structure):
 class gv_serve_config(C.Structure):
     _fields_ = [("slots", C.c_uint32), ("ppr_batch", C.c_uint32), ("max_coalesce", C.c_uint32),
                 ("pace", C.c_uint32), ("hbm_budget_bytes", C.c_uint64), ("alpha", C.c_float),
-                ("epsilon", C.c_float), ("max_iter", C.c_int32)]
+                ("epsilon", C.c_float), ("max_iter", C.c_int32), ("fresh", C.c_uint32)]
 
 
 class gv_serve_outputs(C.Structure):

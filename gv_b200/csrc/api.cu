@@ -157,12 +157,20 @@ void *analytics_scratch(gv_graph *g, size_t bytes) {
         if (g->an_buf) cudaFree(g->an_buf);
         g->an_buf = nullptr;
         g->an_bytes = 0;
-        if (cudaMalloc(&g->an_buf, bytes) != cudaSuccess) {
+        // a quarter more than asked, so calls of slightly different sizes
+        // (and the device-wide stall of cudaFree) do not repeat
+        size_t want = bytes + bytes / 4;
+        if (cudaMalloc(&g->an_buf, want) != cudaSuccess) {
             cudaGetLastError();
-            t_err = "analytics scratch allocation of " + std::to_string(bytes) + " B failed";
-            return nullptr;
+            want = bytes;
+            if (cudaMalloc(&g->an_buf, want) != cudaSuccess) {
+                cudaGetLastError();
+                g->an_buf = nullptr;
+                t_err = "analytics scratch allocation of " + std::to_string(bytes) + " B failed";
+                return nullptr;
+            }
         }
-        g->an_bytes = bytes;
+        g->an_bytes = want;
     }
     return g->an_buf;
 }

@@ -59,6 +59,9 @@ struct MsBufs {
     uint32_t n;
 };
 
+__device__ __forceinline__ double as_f64(unsigned long long x) { return __longlong_as_double((long long)x); }
+__device__ __forceinline__ unsigned long long as_u64(double x) { return (unsigned long long)__double_as_longlong(x); }
+
 __device__ __forceinline__ uint32_t ms_block(const DevGraph &g, uint32_t root, uint32_t k) {
     return k == 0 ? root : cbt_block(g.left, g.right, root, k);
 }
@@ -208,13 +211,51 @@ __global__ void k_ms_close(MsBufs b, uint32_t *__restrict__ next_mask, uint32_t 
     if (threadIdx.x == 0 && any) atomicOr(flag, 1u);
 }
 
-__device__ __forceinline__ double as_f64(unsigned long long x) { return __longlong_as_double((long long)x); }
-__device__ __forceinline__ unsigned long long as_u64(double x) { return (unsigned long long)__double_as_longlong(x); }
 
-struct BwdPre {
-    const uint32_t *deeper;
-    __device__ __forceinline__ uint32_t operator()(uint32_t w) const { return deeper[w]; }
-};
+// Backward sum over one block's entries for the lanes in A: entries 32 at a
+// time, lane j loads entry j and masks[L+1] of it; then every lane adds
+// coef(w_j) for the entries one level deeper for its source.  The gathers are
+// predicated and unrolled so a warp keeps several in flight.
+__device__ __forceinline__ double ms_bwd_block(const DevGraph &g, const MsBufs &b, const uint32_t *__restrict__ deeper,
+                                               uint32_t blk, uint32_t slots, uint32_t A) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t *bp = g.pool + ((size_t)blk << g.logB);
+    const unsigned long long *row = b.row;
+    double acc = 0.0;
+    for (uint32_t e0 = 0; e0 < slots; e0 += 32) {
+        const uint32_t e = e0 + lane;
+        uint32_t w = 0, mw = 0;
+        if (e < slots) {
+            w = bp[e];
+            if (w != GV_TOMB) mw = deeper[w] & A;
+            else w = 0;
+        }
+        if (!__any_sync(GV_FULL_MASK, mw != 0)) continue;
+#pragma unroll 8
+        for (uint32_t j = 0; j < 32; ++j) {
+            const uint32_t wj = __shfl_sync(GV_FULL_MASK, w, j);
+            const uint32_t cj = __shfl_sync(GV_FULL_MASK, mw, j);
+            const bool take = (cj >> lane) & 1u;
+            const unsigned long long x = take ? __ldg(row + (size_t)wj * 32 + lane) : 0ull;
+            acc += as_f64(x);
+        }
+    }
+    return acc;
+}
+
+// Backward walk of a light vertex (lanes hold its block indices).
+__device__ __forceinline__ double ms_bwd_light(const DevGraph &g, const MsBufs &b, const uint32_t *__restrict__ deeper,
+                                               uint4 rec, uint32_t A) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t fill = rec.y, nb = blocks_for(fill, g.logB);
+    const uint32_t blk = lane < nb ? ms_block(g, rec.x, lane) : GV_NIL;
+    double acc = 0.0;
+    for (uint32_t k = 0; k < nb; ++k) {
+        const uint32_t bk = __shfl_sync(GV_FULL_MASK, blk, k);
+        acc += ms_bwd_block(g, b, deeper, bk, min(g.B, fill - (k << g.logB)), A);
+    }
+    return acc;
+}
 
 // Finishes (v, lanes in A) from acc: delta = sigma * acc, coef replaces
 // sigma, returns the lane's delta (0 outside A).
@@ -235,11 +276,7 @@ __global__ void __launch_bounds__(MS_THREADS) k_ms_bwd_light(DevGraph g, MsBufs 
         const uint32_t v = b.light[i];
         const uint32_t A = mask[v];
         const unsigned long long sig = ((A >> lane) & 1u) ? b.row[(size_t)v * 32 + lane] : 0ull;
-        double acc = 0.0;
-        ms_walk_light(g, g.vtx[v], BwdPre{deeper}, [&](uint32_t w, uint32_t mw) {
-            const uint32_t c = A & mw;
-            if ((c >> lane) & 1u) acc += as_f64(b.row[(size_t)w * 32 + lane]);
-        });
+        const double acc = ms_bwd_light(g, b, deeper, g.vtx[v], A);
         double d = ms_finish(b, v, A, sig, acc);
         d = warp_sum(d);
         if (lane == 0) b.bc[v] += d;
@@ -257,10 +294,16 @@ __global__ void __launch_bounds__(MS_THREADS) k_ms_bwd_heavy(DevGraph g, MsBufs 
         const uint32_t A = mask[v];
         const unsigned long long sig = ((A >> lane) & 1u) ? b.row[(size_t)v * 32 + lane] : 0ull;
         double acc = 0.0;
-        ms_walk_heavy(g, g.vtx[v], tab, BwdPre{deeper}, [&](uint32_t w, uint32_t mw) {
-            const uint32_t c = A & mw;
-            if ((c >> lane) & 1u) acc += as_f64(b.row[(size_t)w * 32 + lane]);
-        });
+        const uint4 rec = g.vtx[v];
+        const uint32_t fill = rec.y, nb = blocks_for(fill, g.logB);
+        for (uint32_t k0 = 0; k0 < nb; k0 += MS_TAB) {
+            const uint32_t cnt = min(MS_TAB, nb - k0);
+            __syncthreads();
+            for (uint32_t t = threadIdx.x; t < cnt; t += blockDim.x) tab[t] = ms_block(g, rec.x, k0 + t);
+            __syncthreads();
+            for (uint32_t t = warp; t < cnt; t += MS_WARPS)
+                acc += ms_bwd_block(g, b, deeper, tab[t], min(g.B, fill - ((k0 + t) << g.logB)), A);
+        }
         red[warp][lane] = acc;
         __syncthreads();
         if (warp == 0) {

@@ -55,29 +55,63 @@ struct Server {
     uint64_t estimate(uint32_t kind, uint32_t k) const {
         const uint64_t n = g->d.n;
         switch (kind) {
-            case GV_REQ_PPR: return 16ull * n * k + 16ull * n;
+            case GV_REQ_PPR: return 20ull * n * k + 16ull * n;  // 4 iterate blocks + the result block
             case GV_REQ_TC: return 64ull * n + 8ull * g->d.P * g->d.B / 2;
             default: return 256ull * n + 4ull * 32 * n + 40ull * n;  // BC: sigma rows, 32 level masks, lists
         }
     }
 
-    void run_job(gv_graph *view, cudaStream_t s, Job &jb) {
+    // Device buffer of a worker, grown on demand (results stay on the device
+    // unless the caller asked for them).
+    struct DevBuf {
+        void *p = nullptr;
+        size_t bytes = 0;
+        void *get(size_t want) {
+            if (want <= bytes) return p;
+            if (p) cudaFree(p);
+            p = nullptr;
+            bytes = 0;
+            if (cudaMalloc(&p, want) != cudaSuccess) {
+                cudaGetLastError();
+                return nullptr;
+            }
+            bytes = want;
+            return p;
+        }
+        ~DevBuf() {
+            if (p) cudaFree(p);
+        }
+    };
+
+    void run_job(gv_graph *view, cudaStream_t s, DevBuf &buf, Job &jb) {
         const uint32_t n = g->d.n;
         const double start = now();
         gv_status st = GV_OK;
+        cudaError_t e = cudaSuccess;
         std::vector<uint32_t> sweeps(jb.reqs.size(), 0);
         if (jb.kind == GV_REQ_PPR) {
             std::vector<uint32_t> srcs;
             for (uint32_t r : jb.reqs) srcs.push_back(reqs[r].source);
             const uint32_t k = (uint32_t)srcs.size();
-            std::vector<float> x((size_t)n * k);
+            // sources to the device ahead of the vector block (gv_ppr_batch reads
+            // them with the same memory kind as the output)
+            float *x = (float *)buf.get((size_t)n * k * 4 + 256);  // k <= 32 sources fit in the tail
             int32_t sw = 0;
-            st = gv_ppr_batch(view, srcs.data(), k, cfg.alpha, cfg.epsilon, cfg.max_iter, x.data(), &sw, GV_MEM_HOST, s);
+            if (!x) st = GV_ERR_NOMEM;
+            uint32_t *dsrc = x ? (uint32_t *)((char *)x + (size_t)n * k * 4) : nullptr;
+            if (st == GV_OK) e = cudaMemcpyAsync(dsrc, srcs.data(), k * 4, cudaMemcpyHostToDevice, s);
+            if (st == GV_OK && e != cudaSuccess) st = cuda_status(e, "serve ppr sources");
+            // one query: the single-vector sweeps; more: one lane per query
+            if (st == GV_OK && k == 1)
+                st = gv_ppr(view, srcs[0], cfg.alpha, cfg.epsilon, cfg.max_iter, x, &sw, GV_MEM_DEVICE, s);
+            else if (st == GV_OK)
+                st = gv_ppr_batch(view, dsrc, k, cfg.alpha, cfg.epsilon, cfg.max_iter, x, &sw, GV_MEM_DEVICE, s);
             for (uint32_t j = 0; j < k && st == GV_OK; ++j) {
                 sweeps[j] = (uint32_t)sw;
                 float *out = (outs && outs->ppr) ? outs->ppr[jb.reqs[j]] : nullptr;
-                if (out)
-                    for (uint32_t v = 0; v < n; ++v) out[v] = x[(size_t)v * k + j];
+                // column j of the n x k block
+                if (out) e = cudaMemcpy2DAsync(out, 4, x + j, (size_t)k * 4, 4, n, cudaMemcpyDeviceToHost, s);
+                if (e != cudaSuccess) st = cuda_status(e, "serve ppr out");
             }
         } else if (jb.kind == GV_REQ_TC) {
             std::vector<uint32_t> verts;
@@ -92,10 +126,26 @@ struct Server {
             }
         } else {  // BC: one request per job
             const gv_request &q = reqs[jb.reqs[0]];
-            std::vector<float> b(n);
-            st = gv_bc(view, qvert + q.offset, q.count0, b.data(), GV_MEM_HOST, s);
+            // sources to the device behind the score vector (gv_bc reads them
+            // with the same memory kind as its output)
+            const size_t at = ((size_t)n * 4 + 255) & ~size_t(255);
+            float *b = (float *)buf.get(at + (size_t)q.count0 * 4 + 4);
+            if (!b) st = GV_ERR_NOMEM;
+            uint32_t *dsrc = b ? (uint32_t *)((char *)b + at) : nullptr;
+            if (st == GV_OK && q.count0) {
+                e = cudaMemcpyAsync(dsrc, qvert + q.offset, (size_t)q.count0 * 4, cudaMemcpyHostToDevice, s);
+                if (e != cudaSuccess) st = cuda_status(e, "serve bc sources");
+            }
+            if (st == GV_OK) st = gv_bc(view, q.count0 ? dsrc : nullptr, q.count0, b, GV_MEM_DEVICE, s);
             float *out = (outs && outs->bc) ? outs->bc[jb.reqs[0]] : nullptr;
-            if (out && st == GV_OK) std::memcpy(out, b.data(), (size_t)n * sizeof(float));
+            if (out && st == GV_OK) {
+                e = cudaMemcpyAsync(out, b, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost, s);
+                if (e != cudaSuccess) st = cuda_status(e, "serve bc out");
+            }
+        }
+        if (st == GV_OK) {
+            e = cudaStreamSynchronize(s);
+            if (e != cudaSuccess) st = cuda_status(e, "serve job");
         }
         const double done = now();
         for (size_t j = 0; j < jb.reqs.size(); ++j) {
@@ -118,6 +168,7 @@ struct Server {
         cudaStream_t s = nullptr;
         cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
         gv_status vs = gv_view_create(g, &view);
+        DevBuf buf;
         for (;;) {
             Job jb;
             {
@@ -126,7 +177,7 @@ struct Server {
                 if (busy[w] != 1 && stop) break;
                 jb = job[w];
             }
-            if (vs == GV_OK) run_job(view, s, jb);
+            if (vs == GV_OK) run_job(view, s, buf, jb);
             else {
                 std::lock_guard<std::mutex> lk(mu);
                 if (first_error == GV_OK) first_error = vs;
@@ -159,6 +210,7 @@ extern "C" gv_status gv_serve_config_init(gv_serve_config *cfg) {
     cfg->alpha = 0.85f;
     cfg->epsilon = 1e-6f;
     cfg->max_iter = 100;
+    cfg->fresh = 1;
     return GV_OK;
 }
 
@@ -176,6 +228,7 @@ extern "C" gv_status gv_serve_trace(gv_graph *g, const gv_serve_config *cfg, con
         if (reqs[i].kind > GV_REQ_BC) { set_error("bad request kind"); return GV_ERR_INVALID; }
         if ((reqs[i].kind == GV_REQ_TC || reqs[i].kind == GV_REQ_BC) && !qvert) { set_error("qvert needed"); return GV_ERR_INVALID; }
         if (reqs[i].kind == GV_REQ_UPDATE && (!src || !dst)) { set_error("src/dst needed"); return GV_ERR_INVALID; }
+        if (reqs[i].kind == GV_REQ_PPR && reqs[i].source >= g->d.n) { set_error("PPR source out of range"); return GV_ERR_INVALID; }
     }
     std::memset(results, 0, sizeof(gv_request_result) * nreq);
     Server S;
@@ -198,56 +251,59 @@ extern "C" gv_status gv_serve_trace(gv_graph *g, const gv_serve_config *cfg, con
     uint32_t next = 0, epoch = 0, group = 0;
     auto arrived = [&](uint32_t i) { return !cfg->pace || reqs[i].arrival_s <= S.now(); };
     gv_status st = GV_OK;
-    while (next < nreq && st == GV_OK) {
-        if (!arrived(next)) {
-            const double wait = reqs[next].arrival_s - S.now();
-            if (wait > 0) std::this_thread::sleep_for(std::chrono::duration<double>(std::min(wait, 0.0005)));
-            continue;
+
+    // Applies pending updates idx (trace order, contiguous pair ranges) in
+    // windows of at most max_coalesce requests, after every query in flight
+    // has finished.
+    auto apply_updates = [&](const std::vector<uint32_t> &idx) {
+        {
+            std::unique_lock<std::mutex> lk(S.mu);
+            S.cv.wait(lk, [&] { return S.inflight == 0; });
         }
-        if (reqs[next].kind == GV_REQ_UPDATE) {
-            uint32_t j = next;
-            while (j < nreq && reqs[j].kind == GV_REQ_UPDATE && arrived(j) && j - next < cfg->max_coalesce) ++j;
-            {  // the window waits for every query of the current epoch
-                std::unique_lock<std::mutex> lk(S.mu);
-                S.cv.wait(lk, [&] { return S.inflight == 0; });
-            }
+        for (size_t w0 = 0; w0 < idx.size() && st == GV_OK; w0 += cfg->max_coalesce) {
+            const size_t w1 = std::min(idx.size(), w0 + cfg->max_coalesce);
             const double start = S.now();
             std::vector<gv_batch_desc> descs;
-            const uint64_t base = reqs[next].offset;
+            const uint64_t base = reqs[idx[w0]].offset;
             uint64_t p = 0;
-            for (uint32_t i = next; i < j; ++i) {
-                if (reqs[i].offset != base + p) { set_error("update pairs must follow trace order"); st = GV_ERR_INVALID; break; }
-                descs.push_back({p, reqs[i].count0, reqs[i].count1});
-                p += (uint64_t)reqs[i].count0 + reqs[i].count1;
+            for (size_t q = w0; q < w1; ++q) {
+                const gv_request &r = reqs[idx[q]];
+                if (r.offset != base + p) {
+                    set_error("update pairs must be laid out in trace order");
+                    st = GV_ERR_INVALID;
+                    return;
+                }
+                descs.push_back({p, r.count0, r.count1});
+                p += (uint64_t)r.count0 + r.count1;
             }
-            gv_status us_st = GV_OK;
-            if (st == GV_OK) {
-                us_st = gv_batch_run(g, descs.data(), (uint32_t)descs.size(), src + base, dst + base, GV_MEM_HOST,
-                                     GV_BATCH_COMPACT, us);
-                if (us_st == GV_OK) us_st = gv_synchronize(g, us);
-            }
+            gv_status us_st = gv_batch_run(g, descs.data(), (uint32_t)descs.size(), src + base, dst + base,
+                                           GV_MEM_HOST, GV_BATCH_COMPACT, us);
+            if (us_st == GV_OK) us_st = gv_synchronize(g, us);
             const double done = S.now();
             ++group;
-            for (uint32_t i = next; i < j; ++i) {
-                results[i].start_s = start;
-                results[i].done_s = done;
-                results[i].latency_ms = (done - reqs[i].arrival_s) * 1e3;
-                results[i].epoch = epoch;
-                results[i].status = (uint32_t)us_st;
-                results[i].group = group;
+            for (size_t q = w0; q < w1; ++q) {
+                gv_request_result &rr = results[idx[q]];
+                rr.start_s = start;
+                rr.done_s = done;
+                rr.latency_ms = (done - reqs[idx[q]].arrival_s) * 1e3;
+                rr.epoch = epoch;
+                rr.status = (uint32_t)us_st;
+                rr.group = group;
             }
-            epoch += j - next;
-            next = j;
-            continue;
+            if (us_st != GV_OK && S.first_error == GV_OK) S.first_error = us_st;
+            epoch += (uint32_t)(w1 - w0);
         }
-        // arrived queries of this epoch, in order, until an update or a future arrival
-        uint32_t j = next;
-        while (j < nreq && reqs[j].kind != GV_REQ_UPDATE && arrived(j)) ++j;
+    };
+
+    // Groups queries idx (PPR into batches of at most ppr_batch, triangle
+    // subsets into one count, one BC each) and hands the groups to free
+    // workers as slots and HBM budget allow.
+    auto dispatch_queries = [&](const std::vector<uint32_t> &idx) {
         std::vector<Job> jobs;
         Job ppr, tc;
         ppr.kind = GV_REQ_PPR;
         tc.kind = GV_REQ_TC;
-        for (uint32_t i = next; i < j; ++i) {
+        for (uint32_t i : idx) {
             if (reqs[i].kind == GV_REQ_PPR) {
                 ppr.reqs.push_back(i);
                 if (ppr.reqs.size() == cfg->ppr_batch) {
@@ -288,7 +344,41 @@ extern "C" gv_status gv_serve_trace(gv_graph *g, const gv_serve_config *cfg, con
             lk.unlock();
             S.cv.notify_all();
         }
-        next = j;
+    };
+
+    std::vector<uint32_t> pend_u, pend_q;  // arrived, not yet issued (trace order)
+    while ((next < nreq || !pend_u.empty() || !pend_q.empty()) && st == GV_OK) {
+        for (; next < nreq && arrived(next); ++next) {
+            if (reqs[next].kind == GV_REQ_UPDATE) pend_u.push_back(next);
+            else pend_q.push_back(next);
+        }
+        if (pend_u.empty() && pend_q.empty()) {
+            const double wait = reqs[next].arrival_s - S.now();
+            if (wait > 0) std::this_thread::sleep_for(std::chrono::duration<double>(std::min(wait, 0.0005)));
+            continue;
+        }
+        // queries that arrived before the first pending update run on the current epoch
+        const uint32_t first_u = pend_u.empty() ? nreq : pend_u.front();
+        std::vector<uint32_t> now_q, later_q;
+        for (uint32_t i : pend_q) (i < first_u ? now_q : later_q).push_back(i);
+        if (!now_q.empty()) dispatch_queries(now_q);
+        pend_q.swap(later_q);
+        if (pend_u.empty()) continue;
+        if (cfg->fresh) {
+            // every arrived update, then every arrived query: a query sees at
+            // least the updates that arrived before it
+            apply_updates(pend_u);
+            pend_u.clear();
+            if (!pend_q.empty()) dispatch_queries(pend_q);
+            pend_q.clear();
+        } else {
+            // the updates up to the next pending query, as one run
+            const uint32_t first_q = pend_q.empty() ? nreq : pend_q.front();
+            std::vector<uint32_t> run, rest;
+            for (uint32_t i : pend_u) (i < first_q ? run : rest).push_back(i);
+            apply_updates(run);
+            pend_u.swap(rest);
+        }
     }
     {
         std::unique_lock<std::mutex> lk(S.mu);

@@ -8,8 +8,12 @@
  * estimate fits the HBM budget.  Queries that arrive while others run are
  * admitted as slots free up (continuous batching): arrived PPR queries are
  * merged into batched launches, arrived triangle-subset queries share one
- * triangle count.  Epochs: a query sees exactly the updates that arrived
- * before it.  No reference counterpart (the reference has no serving path).
+ * triangle count.  Epochs: with fresh = 0 a query sees exactly the updates
+ * that arrived before it; with fresh = 1 (the default) it sees at least
+ * those, so queries that arrive behind an update wait for it and run
+ * together after it.  results[i].epoch names the updates each query saw (the
+ * first epoch update requests in trace order).  No reference counterpart (the
+ * reference has no serving path).
  */
 #ifndef GV_SERVE_H
 #define GV_SERVE_H
@@ -49,6 +53,9 @@ typedef struct gv_serve_config {
     float alpha;
     float epsilon;
     int32_t max_iter;
+    uint32_t fresh;            /* 1: a query sees at least the updates that arrived before it
+                                  (the loop applies every arrived update, then runs every
+                                  arrived query together); 0: exactly those updates       */
 } gv_serve_config;
 
 /* Optional host buffers for results, indexed by request (entries may be

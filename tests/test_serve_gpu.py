@@ -1,7 +1,8 @@
 """GPU tests of the request loop (gv_serve_trace): every query in a mixed
 trace of updates and queries must return what the same query returns alone
-on a graph holding exactly the updates that arrived before it, whether the
-loop runs queries one at a time or several at once on views."""
+on a graph holding the updates its epoch names (exactly those that arrived
+before it, or at least those in the fresh mode), whether the loop runs
+queries one at a time or several at once on views."""
 import numpy as np
 import pytest
 
@@ -40,49 +41,63 @@ def _trace(n, s, d, rng, nreq=60, gap=0.0):
     return trace
 
 
-def _replay_and_check(n, s, d, trace, res, outs):
-    """Applies the updates in order on a fresh graph (and the oracle) and runs
-    each query alone after the updates its epoch says it saw."""
+def _replay_and_check(n, s, d, trace, res, outs, fresh):
+    """Applies the updates in trace order on a fresh graph (and the oracle)
+    and runs each query alone after the updates its epoch says it saw: the
+    first `epoch` update requests of the trace."""
     g = make_graph(n)
     g.batch_insert(s, d)
     o = oracle.OracleGraph(n)
     o.insert(s, d)
-    applied = 0
+    updates = [item for item in trace if item[0] == "update"]
+    before = 0
+    by_epoch = {}
     for i, item in enumerate(trace):
         assert res["status"][i] == 0, (i, res["status"][i])
         if item[0] == "update":
+            before += 1
+            continue
+        # a query sees every update that arrived before it (exactly those unless fresh)
+        if fresh:
+            assert res["epoch"][i] >= before, (i, res["epoch"][i], before)
+        else:
+            assert res["epoch"][i] == before, (i, res["epoch"][i], before)
+        by_epoch.setdefault(int(res["epoch"][i]), []).append(i)
+    for e in range(len(updates) + 1):
+        if e:
+            item = updates[e - 1]
             g.batch_insert(item[1], item[2])
             g.batch_delete(item[3], item[4])
             g.compaction()
             o.insert(item[1], item[2])
             o.delete(item[3], item[4])
-            applied += 1
-            continue
-        # a query sees exactly the updates that arrived before it
-        assert res["epoch"][i] == applied, (i, res["epoch"][i], applied)
-        if item[0] == "ppr":
-            xo, _ = o.ppr(item[1], ALPHA, EPS, 100, fixed_sweeps=int(res["sweeps"][i]))
-            assert np.abs(outs[i] - xo).sum() < PR_L1, i
-        elif item[0] == "tc":
-            assert np.array_equal(outs[i], g.tc_subset(item[1])), i
-        else:
-            ref = g.bc(item[1])
-            assert np.allclose(outs[i], ref, rtol=BC_REL, atol=BC_REL), i
+        for i in by_epoch.get(e, []):
+            item = trace[i]
+            if item[0] == "ppr":
+                xo, _ = o.ppr(item[1], ALPHA, EPS, 100, fixed_sweeps=int(res["sweeps"][i]))
+                assert np.abs(outs[i] - xo).sum() < PR_L1, i
+            elif item[0] == "tc":
+                assert np.array_equal(outs[i], g.tc_subset(item[1])), i
+            else:
+                ref = g.bc(item[1])
+                assert np.allclose(outs[i], ref, rtol=BC_REL, atol=BC_REL), i
     g.close()
 
 
-@pytest.mark.parametrize("slots,gap", [(1, 0.0), (4, 0.0), (4, 0.002)])
-def test_mixed_trace_matches_each_query_alone(slots, gap):
+@pytest.mark.parametrize("slots,gap,fresh", [(1, 0.0, False), (4, 0.0, False), (4, 0.002, False),
+                                             (4, 0.0, True), (4, 0.002, True)])
+def test_mixed_trace_matches_each_query_alone(slots, gap, fresh):
     scale = 12
     n = 1 << scale
     s, d = rmat_graph(scale, 8, seed=21)
     trace = _trace(n, s, d, np.random.default_rng(5 + slots), gap=gap)
     g = make_graph(n)
     g.batch_insert(s, d)
-    res, outs = g.serve(trace, slots=slots, ppr_batch=8, pace=gap > 0, alpha=ALPHA, epsilon=EPS, outputs=True)
+    res, outs = g.serve(trace, slots=slots, ppr_batch=8, pace=gap > 0, alpha=ALPHA, epsilon=EPS, outputs=True,
+                        fresh=fresh)
     g.synchronize()
     assert np.all(res["done_s"] >= res["start_s"])
-    _replay_and_check(n, s, d, trace, res, outs)
+    _replay_and_check(n, s, d, trace, res, outs, fresh)
     # the served graph ends equal to the replayed one
     g2 = make_graph(n)
     g2.batch_insert(s, d)
@@ -95,6 +110,26 @@ def test_mixed_trace_matches_each_query_alone(slots, gap):
     assert np.array_equal(a[0], b[0])
     g.close()
     g2.close()
+
+
+def test_fresh_mode_runs_arrived_queries_together():
+    """Everything arrived at once: all updates go first and every query after
+    the first update then runs on the last epoch, PPR queries in one launch."""
+    scale = 11
+    n = 1 << scale
+    s, d = rmat_graph(scale, 8, seed=6)
+    trace = _trace(n, s, d, np.random.default_rng(17), nreq=40)
+    nupd = sum(1 for t in trace if t[0] == "update")
+    g = make_graph(n)
+    g.batch_insert(s, d)
+    res, _ = g.serve(trace, slots=4, ppr_batch=32, pace=False, fresh=True)
+    q = [i for i, t in enumerate(trace) if t[0] != "update"]
+    first_u = min(i for i, t in enumerate(trace) if t[0] == "update")
+    for i in q:
+        assert res["epoch"][i] == (0 if i < first_u else nupd), i
+    ppr_groups = {int(res["group"][i]) for i in q if trace[i][0] == "ppr" and i > first_u}
+    assert len(ppr_groups) == 1
+    g.close()
 
 
 def test_budget_of_one_byte_runs_groups_one_at_a_time():
