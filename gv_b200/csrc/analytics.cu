@@ -9,10 +9,12 @@
 //              device, no host round trip per sweep;
 //   TC         src/algorithm/tc/tc_kernel.cu:3-147 (triple linear scans,
 //              float counts) -> degree-oriented sorted snapshot + merge-path
-//              intersection, uint64 counts;
+//              intersection (packed hash probe behind GV_TC_PACKED=1),
+//              uint64 counts;
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 #include "../../include/gv_batch.h"
 #include "store.cuh"
@@ -25,6 +27,9 @@ namespace gv {
 namespace {
 
 constexpr int AN_THREADS = 256;
+// What a triangle count credits: the smallest id of each triangle (per-vertex
+// counts as the reference keeps them), all three vertices, or only the total.
+constexpr int TC_OWNER = 0, TC_INCIDENT = 1, TC_TOTAL = 2;
 constexpr int BIG_TAB_A = 1024;
 // Pull sweeps route vertices by used slots: lane groups up to LIGHT_FILL,
 // one CTA per vertex up to HUB_FILL, the whole grid above.
@@ -709,9 +714,10 @@ __device__ __forceinline__ uint32_t corank(const uint32_t *A, uint32_t la, const
 }
 
 // Group per oriented edge (u -> v): merge-path intersection of N+(u), N+(v).
-// INCIDENT: credit all three vertices; else credit the smallest id (the
-// reference's owner, tc_kernel.cu:25-30).
-template <int TPV, bool INCIDENT>
+// MODE TC_INCIDENT: credit all three vertices; TC_OWNER: credit the smallest
+// id (the reference's owner, tc_kernel.cu:25-30); TC_TOTAL: only the sum is
+// wanted, every triangle is credited to u (no per-vertex meaning).
+template <int TPV, int MODE>
 __global__ void __launch_bounds__(AN_THREADS) k_tc_count(const unsigned long long *__restrict__ off,
                                                          const uint32_t *__restrict__ snap,
                                                          const uint32_t *__restrict__ esrc, uint64_t m_plus,
@@ -754,7 +760,9 @@ __global__ void __launch_bounds__(AN_THREADS) k_tc_count(const unsigned long lon
         uint32_t cu = 0, cv = 0;
         const uint32_t uv_min = min(u, v);
         auto credit = [&](uint32_t w) {
-            if (INCIDENT) {
+            if (MODE == TC_TOTAL) {
+                ++cu;
+            } else if (MODE == TC_INCIDENT) {
                 ++cu; ++cv;
                 add(w, 1ull);
             } else if (w < uv_min) {
@@ -783,16 +791,44 @@ __global__ void __launch_bounds__(AN_THREADS) k_tc_count(const unsigned long lon
             const uint32_t per = (tot + TPV - 1) / TPV;
             const uint32_t d0 = min(tot, G.gl * per), d1 = min(tot, d0 + per);
             uint32_t i = corank(A, la, Bv, lb, d0), j = d0 - i;
-            // branch-free merge step: lanes stay converged, only matches diverge
-            uint32_t a = (i < la) ? __ldg(A + i) : 0xFFFFFFFFu;
-            uint32_t bb = (j < lb) ? __ldg(Bv + j) : 0xFFFFFFFFu;
-            for (uint32_t d = d0; d < d1; ++d) {
-                const uint32_t ta = (a <= bb) ? 1u : 0u;  // ties consume A first
-                if (a == bb && a != 0xFFFFFFFFu) credit(a);
-                i += ta;
-                j += 1u - ta;
-                a = (i < la) ? __ldg(A + i) : 0xFFFFFFFFu;
-                bb = (j < lb) ? __ldg(Bv + j) : 0xFFFFFFFFu;
+            auto ld = [](const uint32_t *X, uint32_t x, uint32_t len) {
+                return x < len ? __ldg(X + x) : 0xFFFFFFFFu;
+            };
+            if (MODE == TC_TOTAL) {
+                // the next four entries of each list sit in registers and the
+                // load that refills a window is needed four steps later, so
+                // steps do not wait on each other's loads (1.5x faster on
+                // R-MAT scale 22; with per-vertex credits the branchy step
+                // loses to the branch-free one below)
+                uint32_t a0 = ld(A, i, la), a1 = ld(A, i + 1, la), a2 = ld(A, i + 2, la), a3 = ld(A, i + 3, la);
+                uint32_t b0 = ld(Bv, j, lb), b1 = ld(Bv, j + 1, lb), b2 = ld(Bv, j + 2, lb), b3 = ld(Bv, j + 3, lb);
+                for (uint32_t d = d0; d < d1; ++d) {
+                    cu += (a0 == b0 && a0 != 0xFFFFFFFFu) ? 1u : 0u;
+                    if (a0 <= b0) {  // ties consume A first
+                        a0 = a1;
+                        a1 = a2;
+                        a2 = a3;
+                        a3 = ld(A, i + 4, la);
+                        ++i;
+                    } else {
+                        b0 = b1;
+                        b1 = b2;
+                        b2 = b3;
+                        b3 = ld(Bv, j + 4, lb);
+                        ++j;
+                    }
+                }
+            } else {
+                // branch-free merge step: lanes stay converged, only matches diverge
+                uint32_t a = ld(A, i, la), bb = ld(Bv, j, lb);
+                for (uint32_t d = d0; d < d1; ++d) {
+                    const uint32_t ta = (a <= bb) ? 1u : 0u;  // ties consume A first
+                    if (a == bb && a != 0xFFFFFFFFu) credit(a);
+                    i += ta;
+                    j += 1u - ta;
+                    a = ld(A, i, la);
+                    bb = ld(Bv, j, lb);
+                }
             }
             touched = tot;
         }
@@ -881,158 +917,291 @@ __device__ __forceinline__ bool set_has(const uint32_t *tab, uint32_t mask, uint
     return false;
 }
 
-template <bool INCIDENT>
-__device__ __forceinline__ void tc_credit(TcCredit &cr, uint32_t u, uint32_t v, uint32_t w, uint32_t &cu,
-                                          uint32_t &cv) {
-    if (INCIDENT) {
+// ------------------------------------ packed hash-probe intersection
+// (GV_TC_PACKED=1; on R-MAT scale 22 it reads 26% fewer list entries than the
+// merge path but takes 1.8x longer: each probe is a random shared-memory
+// access with a few slots of linear probing, where a merge step reads the
+// next cached entry)
+// u-centric: N+(u) goes into a hash set in shared memory; the lists N+(v),
+// v in N+(u), are streamed as one concatenated run, 32 entries per warp step
+// (one entry per lane, several short lists per step), each entry one probe
+// of the set.  Work: sum_v d-(v) d+(v) probes + sum_u d+(u) inserts, against
+// sum over oriented edges of d+(u) + d+(v) merge steps for the merge path
+// (about 1.6x more on R-MAT), and the lists need no sorting.  Lane j of a
+// step finds its list from the start offsets of the next 32 lists: one OR
+// reduction of start bits and a popcount.
+constexpr uint32_t TCP_LIGHT = 128;            // d+(u) handled by one warp
+constexpr uint32_t TCP_WSET = 2 * TCP_LIGHT;   // per-warp set slots
+constexpr int TCP_THREADS = 512;
+constexpr int TCP_WARPS = TCP_THREADS / 32;
+constexpr uint32_t TCP_CHUNK = 2048;           // lists per CTA step (heavy u)
+constexpr uint32_t TCP_SSET = 8192;            // shared set slots of the heavy kernel
+
+struct TcpWarp {
+    uint32_t set[TCP_WSET];
+    uint32_t vl[TCP_LIGHT];
+    unsigned long long base[TCP_LIGHT];
+    uint32_t pref[TCP_LIGHT + 1];
+};
+
+template <int MODE>
+__device__ __forceinline__ void tcp_credit(TcCredit &cr, uint32_t u, uint32_t v, uint32_t w, uint32_t &cu) {
+    if (MODE == TC_TOTAL) {
         ++cu;
-        ++cv;
+    } else if (MODE == TC_INCIDENT) {
+        ++cu;
+        cr.add(v, 1ull);
         cr.add(w, 1ull);
     } else {
-        const uint32_t m = min(u, v);
-        if (w < m) cr.add(w, 1ull);
-        else if (u < v) ++cu;
-        else ++cv;
+        const uint32_t m = min(u, min(v, w));
+        if (m == u) ++cu;
+        else cr.add(m, 1ull);
     }
 }
 
-// Probes all v in N+(u) against the set `tab` (threads t of nt cooperate on
-// each v; `sync` separates nothing: the set is read-only here).
-template <bool INCIDENT>
-__device__ __forceinline__ unsigned long long tc_probe_all(const unsigned long long *__restrict__ off,
-                                                           const uint32_t *__restrict__ snap, uint32_t u,
-                                                           const uint32_t *A, uint32_t la, const uint32_t *tab,
-                                                           uint32_t mask, bool sorted, uint32_t v_first,
-                                                           uint32_t v_step, uint32_t t, uint32_t nt, TcCredit &cr,
-                                                           uint32_t &cu_tot) {
-    unsigned long long work = 0;  // list entries touched (counted once per pair)
-    for (uint32_t j = v_first; j < la; j += v_step) {
-        const uint32_t v = A[j];
-        const uint32_t *Bv = snap + off[v];
-        const uint32_t lb = (uint32_t)(off[v + 1] - off[v]);
-        uint32_t cu = 0, cv = 0;
-        if (lb > 16u * la) {
-            // long N+(v): binary-search the entries of N+(u) in it
-            const uint32_t lgB = 32 - __clz(lb);
-            for (uint32_t i = t; i < la; i += nt) {
-                const uint32_t w = A[i];
-                const uint32_t pos = lower_bound_u32(Bv, lb, w);
-                if (pos < lb && Bv[pos] == w) tc_credit<INCIDENT>(cr, u, v, w, cu, cv);
-            }
-            if (t == 0) work += (unsigned long long)la * (lgB + 1);
-        } else {
-            for (uint32_t k = t; k < lb; k += nt) {
-                const uint32_t w = __ldg(Bv + k);
-                if (set_has(tab, mask, w, sorted)) tc_credit<INCIDENT>(cr, u, v, w, cu, cv);
-            }
-            if (t == 0) work += lb;
-        }
-        cu_tot += cu;
-        if (cv) cr.add(v, cv);
+// One step of 32 positions [p0, p0 + 32) of the concatenated lists of N+(v):
+// list j covers positions [pref[j], pref[j + 1]), entry p of it sits at
+// snap[base[j] + p].  j0 = the list holding p0.  Returns the list holding
+// p0 + 32.
+template <int MODE>
+__device__ __forceinline__ uint32_t tcp_step(const uint32_t *__restrict__ snap, const uint32_t *set, uint32_t mask,
+                                             const uint32_t *vl, const unsigned long long *base, const uint32_t *pref,
+                                             uint32_t nv, uint32_t T, uint32_t p0, uint32_t j0, uint32_t u,
+                                             TcCredit &cr, uint32_t &cu) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t S = (j0 + lane < nv) ? pref[j0 + lane] : 0xFFFFFFFFu;
+    const uint32_t rel = S - p0;
+    const uint32_t F = __reduce_or_sync(GV_FULL_MASK, rel < 32u ? (1u << rel) : 0u);
+    const uint32_t G = F & ~1u;  // lists starting after p0 inside the step
+    const uint32_t lm = lane == 31 ? 0xFFFFFFFFu : ((2u << lane) - 1u);
+    const uint32_t j = j0 + __popc(G & lm);
+    const uint32_t p = p0 + lane;
+    if (p < T) {
+        const uint32_t w = __ldg(snap + (base[j] + p));
+        if (set_has(set, mask, w, false)) tcp_credit<MODE>(cr, u, vl[j], w, cu);
     }
-    return work;
+    const uint32_t jl = j0 + __popc(G);
+    return (jl + 1 <= nv && pref[jl + 1] <= p0 + 32) ? jl + 1 : jl;
 }
 
-template <bool INCIDENT>
-__global__ void __launch_bounds__(AN_THREADS) k_tc_hash(const unsigned long long *__restrict__ off,
-                                                        const uint32_t *__restrict__ snap, uint32_t n,
-                                                        unsigned long long *__restrict__ tcount,
-                                                        uint32_t *__restrict__ big_u, unsigned long long *nbig,
-                                                        unsigned long long *__restrict__ work) {
-    __shared__ uint32_t wtab[AN_THREADS / 32][TC_WARP_TAB];
-    __shared__ uint32_t ck[TC_CREDIT_HT];
-    __shared__ unsigned long long cval[TC_CREDIT_HT];
-    __shared__ unsigned long long wred[AN_THREADS / 32];
+// Compacts the lists v = A[i] (i in [i0, i0 + 32)) with d+(v) > 0 into
+// vl / base / pref at nv, running total T (one warp); inserts v into `set`
+// when it is given.
+__device__ __forceinline__ void tcp_gather32(const unsigned long long *__restrict__ off, const uint32_t *A, uint32_t la,
+                                             uint32_t i0, uint32_t *vl, unsigned long long *base, uint32_t *pref,
+                                             uint32_t &nv, uint32_t &T, uint32_t *set, uint32_t mask) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t i = i0 + lane;
+    uint32_t v = GV_NIL, dv = 0;
+    unsigned long long ov = 0;
+    if (i < la) {
+        v = A[i];
+        if (set) set_insert(set, mask, v);
+        ov = off[v];
+        dv = (uint32_t)(off[v + 1] - ov);
+    }
+    const bool keep = dv > 0;
+    const uint32_t bal = __ballot_sync(GV_FULL_MASK, keep);
+    uint32_t incl = dv;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(GV_FULL_MASK, incl, o);
+        if (lane >= (uint32_t)o) incl += t;
+    }
+    const uint32_t tot = __shfl_sync(GV_FULL_MASK, incl, 31);
+    if (keep) {
+        const uint32_t pos = nv + __popc(bal & ((1u << lane) - 1u));
+        const uint32_t start = T + incl - dv;
+        vl[pos] = v;
+        pref[pos] = start;
+        base[pos] = ov - start;
+    }
+    nv += __popc(bal);
+    T += tot;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(TCP_THREADS) k_tcp_light(const unsigned long long *__restrict__ off,
+                                                           const uint32_t *__restrict__ snap, uint32_t n,
+                                                           unsigned long long *__restrict__ tcount,
+                                                           unsigned long long *__restrict__ work) {
+    extern __shared__ unsigned char tcp_dyn[];
+    TcpWarp *ws = reinterpret_cast<TcpWarp *>(tcp_dyn);
+    uint32_t *ck = reinterpret_cast<uint32_t *>(ws + TCP_WARPS);
+    unsigned long long *cval = reinterpret_cast<unsigned long long *>(ck + TC_CREDIT_HT);
+    __shared__ unsigned long long wred[TCP_WARPS];
     for (uint32_t i = threadIdx.x; i < TC_CREDIT_HT; i += blockDim.x) {
         ck[i] = GV_NIL;
         cval[i] = 0;
     }
     __syncthreads();
     TcCredit cr{ck, cval, tcount};
-    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    uint32_t *tab = wtab[warp];
-    const uint32_t mask = TC_WARP_TAB - 1;
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    TcpWarp &W = ws[warp];
     unsigned long long my_work = 0;
-    const uint32_t nw = gridDim.x * (AN_THREADS / 32);
-    for (uint32_t u = blockIdx.x * (AN_THREADS / 32) + warp; u < n; u += nw) {
-        const uint32_t la = (uint32_t)(off[u + 1] - off[u]);
-        if (la < 2) continue;  // a triangle needs two out-neighbours of u
-        if (la > TC_WARP_TAB / 2) {
-            if (lane == 0) big_u[atomicAdd(nbig, 1ull)] = u;
-            continue;
-        }
-        const uint32_t *A = snap + off[u];
-        for (uint32_t i = lane; i < TC_WARP_TAB; i += 32) tab[i] = GV_NIL;
+    const uint32_t nw = gridDim.x * TCP_WARPS;
+    for (uint32_t u = blockIdx.x * TCP_WARPS + warp; u < n; u += nw) {
+        const unsigned long long ou = off[u];
+        const uint32_t la = (uint32_t)(off[u + 1] - ou);
+        if (la < 2 || la > TCP_LIGHT) continue;  // < 2: no triangle has u lowest; > TCP_LIGHT: k_tcp_heavy
+        const uint32_t *A = snap + ou;
+        uint32_t cap = 32;
+        while (cap < 2 * la) cap <<= 1;
+        const uint32_t mask = cap - 1;
+        for (uint32_t i = lane; i < cap; i += 32) W.set[i] = GV_NIL;
         __syncwarp();
-        for (uint32_t i = lane; i < la; i += 32) set_insert(tab, mask, A[i]);
+        uint32_t nv = 0, T = 0;
+        for (uint32_t i0 = 0; i0 < la; i0 += 32) tcp_gather32(off, A, la, i0, W.vl, W.base, W.pref, nv, T, W.set, mask);
+        if (lane == 0) W.pref[nv] = T;
         __syncwarp();
-        uint32_t cu = 0;
-        my_work += tc_probe_all<INCIDENT>(off, snap, u, A, la, tab, mask, false, 0, 1, lane, 32, cr, cu);
+        uint32_t cu = 0, j0 = 0;
+        for (uint32_t p0 = 0; p0 < T; p0 += 32)
+            j0 = tcp_step<MODE>(snap, W.set, mask, W.vl, W.base, W.pref, nv, T, p0, j0, u, cr, cu);
         cu = warp_sum(cu);
-        if (lane == 0 && cu) cr.add(u, cu);
+        if (lane == 0) {
+            if (cu) cr.add(u, cu);
+            my_work += (unsigned long long)T + la;
+        }
         __syncwarp();
     }
-    my_work = warp_sum(my_work);
     if (lane == 0) wred[warp] = my_work;
     __syncthreads();
     if (threadIdx.x == 0) {
         unsigned long long t = 0;
-        for (int i = 0; i < AN_THREADS / 32; ++i) t += wred[i];
+        for (int i = 0; i < TCP_WARPS; ++i) t += wred[i];
         if (t) atomicAdd(work, t);
     }
     cr.flush();
 }
 
-// Vertices with long N+(u): one CTA per vertex, set in dynamic shared memory.
-template <bool INCIDENT>
-__global__ void __launch_bounds__(512) k_tc_hash_big(const unsigned long long *__restrict__ off,
-                                                     const uint32_t *__restrict__ snap,
-                                                     unsigned long long *__restrict__ tcount,
-                                                     const uint32_t *__restrict__ big_u, const unsigned long long *nbig,
-                                                     uint32_t tab_size, unsigned long long *__restrict__ work) {
-    extern __shared__ uint32_t dyn[];
-    __shared__ uint32_t ck[TC_CREDIT_HT];
-    __shared__ unsigned long long cval[TC_CREDIT_HT];
-    __shared__ uint32_t cured[16];
-    __shared__ unsigned long long wred[16];
+// Vertices with d+(u) > TCP_LIGHT into list; cnt[1] = the longest d+.
+__global__ void k_tcp_heavy_list(const unsigned long long *__restrict__ off, uint32_t n, uint32_t *__restrict__ list,
+                                 unsigned long long *cnt) {
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        const uint32_t u = base + threadIdx.x;
+        uint32_t la = 0;
+        if (u < n) la = (uint32_t)(off[u + 1] - off[u]);
+        const bool heavy = la > TCP_LIGHT;
+        const uint32_t bal = __ballot_sync(GV_FULL_MASK, heavy);
+        unsigned long long at = 0;
+        if (lane == 0 && bal) at = atomicAdd(cnt, (unsigned long long)__popc(bal));
+        at = __shfl_sync(GV_FULL_MASK, at, 0);
+        if (heavy) {
+            list[at + __popc(bal & ((1u << lane) - 1u))] = u;
+            atomicMax(cnt + 1, (unsigned long long)la);
+        }
+    }
+}
+
+// One CTA per heavy u: the set of N+(u) in shared memory (global, per CTA,
+// above TCP_SSET / 2 entries); lists in chunks of TCP_CHUNK, warps over steps.
+template <int MODE>
+__global__ void __launch_bounds__(TCP_THREADS) k_tcp_heavy(const unsigned long long *__restrict__ off,
+                                                           const uint32_t *__restrict__ snap,
+                                                           unsigned long long *__restrict__ tcount,
+                                                           const uint32_t *__restrict__ list,
+                                                           const unsigned long long *cnt, uint32_t *__restrict__ gset,
+                                                           uint32_t gcap, unsigned long long *__restrict__ work) {
+    extern __shared__ unsigned char tcp_dyn[];
+    uint32_t *sset = reinterpret_cast<uint32_t *>(tcp_dyn);
+    uint32_t *vl = sset + TCP_SSET;
+    unsigned long long *base = reinterpret_cast<unsigned long long *>(vl + TCP_CHUNK);
+    uint32_t *pref = reinterpret_cast<uint32_t *>(base + TCP_CHUNK);
+    uint32_t *ck = pref + TCP_CHUNK + 32;
+    unsigned long long *cval = reinterpret_cast<unsigned long long *>(ck + TC_CREDIT_HT);
+    __shared__ uint32_t s_nv, s_T;
+    __shared__ uint32_t wsum[TCP_WARPS], wcnt[TCP_WARPS], cured[TCP_WARPS];
+    __shared__ unsigned long long wred[TCP_WARPS];
     for (uint32_t i = threadIdx.x; i < TC_CREDIT_HT; i += blockDim.x) {
         ck[i] = GV_NIL;
         cval[i] = 0;
     }
     __syncthreads();
     TcCredit cr{ck, cval, tcount};
-    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-    const uint32_t nb = (uint32_t)*nbig;
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    const uint32_t nh = (uint32_t)cnt[0];
     unsigned long long my_work = 0;
-    for (uint32_t bi = blockIdx.x; bi < nb; bi += gridDim.x) {
-        const uint32_t u = big_u[bi];
-        const uint32_t la = (uint32_t)(off[u + 1] - off[u]);
-        const uint32_t *A = snap + off[u];
-        // hash set when it fits at half load, else a sorted copy (la <= tab_size
-        // is guaranteed by the host)
-        const bool sorted = 2 * la > tab_size;
-        uint32_t mask;
-        if (sorted) {
-            for (uint32_t i = threadIdx.x; i < la; i += blockDim.x) dyn[i] = A[i];
-            mask = la;
-        } else {
-            uint32_t size = 1024;
-            while (size < 2 * la) size <<= 1;
-            mask = size - 1;
-            for (uint32_t i = threadIdx.x; i < size; i += blockDim.x) dyn[i] = GV_NIL;
-            __syncthreads();
-            for (uint32_t i = threadIdx.x; i < la; i += blockDim.x) set_insert(dyn, mask, A[i]);
-        }
+    for (uint32_t hi = blockIdx.x; hi < nh; hi += gridDim.x) {
+        const uint32_t u = list[hi];
+        const unsigned long long ou = off[u];
+        const uint32_t la = (uint32_t)(off[u + 1] - ou);
+        const uint32_t *A = snap + ou;
+        uint32_t cap = 1024;
+        while (cap < 2 * la) cap <<= 1;
+        uint32_t *set = cap <= TCP_SSET ? sset : gset + (size_t)blockIdx.x * gcap;
+        const uint32_t mask = cap - 1;
+        for (uint32_t i = threadIdx.x; i < cap; i += blockDim.x) set[i] = GV_NIL;
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < la; i += blockDim.x) set_insert(set, mask, A[i]);
         __syncthreads();
         uint32_t cu = 0;
-        my_work += tc_probe_all<INCIDENT>(off, snap, u, A, la, dyn, mask, sorted, warp, nwarps, lane, 32, cr, cu);
+        for (uint32_t c0 = 0; c0 < la; c0 += TCP_CHUNK) {
+            const uint32_t cn = min(TCP_CHUNK, la - c0);
+            // pass 1: lists kept and their entries per warp (warp w takes the
+            // 32-list slices w, w + TCP_WARPS, ...); thread 0 turns them into
+            // per-warp starting offsets
+            uint32_t nv_w = 0, T_w = 0;
+            for (uint32_t i0 = warp * 32; i0 < cn; i0 += TCP_THREADS) {
+                const uint32_t i = i0 + lane;
+                uint32_t dv = 0;
+                if (i < cn) {
+                    const uint32_t v = A[c0 + i];
+                    dv = (uint32_t)(off[v + 1] - off[v]);
+                }
+                nv_w += __popc(__ballot_sync(GV_FULL_MASK, dv > 0));
+                T_w += warp_sum(dv);
+            }
+            if (lane == 0) {
+                wcnt[warp] = nv_w;
+                wsum[warp] = T_w;
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                uint32_t a = 0, t = 0;
+                for (int w = 0; w < TCP_WARPS; ++w) {
+                    const uint32_t x = wcnt[w], y = wsum[w];
+                    wcnt[w] = a;
+                    wsum[w] = t;
+                    a += x;
+                    t += y;
+                }
+                s_nv = a;
+                s_T = t;
+                pref[a] = t;
+            }
+            __syncthreads();
+            // pass 2: place the same slices in the same order
+            uint32_t nv = wcnt[warp], T = wsum[warp];
+            for (uint32_t i0 = warp * 32; i0 < cn; i0 += TCP_THREADS)
+                tcp_gather32(off, A + c0, cn, i0, vl, base, pref, nv, T, nullptr, 0);
+            __syncthreads();
+            const uint32_t NV = s_nv, TT = s_T;
+            for (uint32_t p0 = warp * 32; p0 < TT; p0 += TCP_THREADS) {
+                uint32_t j0 = 0;
+                if (lane == 0) {  // last list starting at or before p0
+                    uint32_t lo = 0, hi2 = NV;
+                    while (hi2 - lo > 1) {
+                        const uint32_t mid = (lo + hi2) >> 1;
+                        if (pref[mid] <= p0) lo = mid;
+                        else hi2 = mid;
+                    }
+                    j0 = lo;
+                }
+                j0 = __shfl_sync(GV_FULL_MASK, j0, 0);
+                tcp_step<MODE>(snap, set, mask, vl, base, pref, NV, TT, p0, j0, u, cr, cu);
+            }
+            if (lane == 0 && warp == 0) my_work += TT;
+            __syncthreads();
+        }
         cu = warp_sum(cu);
         if (lane == 0) cured[warp] = cu;
         __syncthreads();
         if (threadIdx.x == 0) {
             uint32_t t = 0;
-            for (uint32_t i = 0; i < nwarps; ++i) t += cured[i];
+            for (int w = 0; w < TCP_WARPS; ++w) t += cured[w];
             if (t) cr.add(u, t);
+            my_work += la;
         }
         __syncthreads();
     }
@@ -1041,7 +1210,7 @@ __global__ void __launch_bounds__(512) k_tc_hash_big(const unsigned long long *_
     __syncthreads();
     if (threadIdx.x == 0) {
         unsigned long long t = 0;
-        for (uint32_t i = 0; i < nwarps; ++i) t += wred[i];
+        for (int i = 0; i < TCP_WARPS; ++i) t += wred[i];
         if (t) atomicAdd(work, t);
     }
     cr.flush();
@@ -1076,7 +1245,7 @@ struct TcBufs {
 
 // Builds the oriented sorted snapshot and counts.  tcount[n] receives the
 // per-vertex counts (owner or incident).  Returns m_plus via *mplus.
-gv_status tc_run(gv_graph *g, cudaStream_t s, bool incident, unsigned long long **tcount_out) {
+gv_status tc_run(gv_graph *g, cudaStream_t s, int mode, unsigned long long **tcount_out) {
     if (g->cfg.directed) { set_error("triangle counting needs an undirected store"); return GV_ERR_STATE; }
     DevGraph d = g->d;
     const uint32_t n = d.n;
@@ -1145,25 +1314,69 @@ gv_status tc_run(gv_graph *g, cudaStream_t s, bool incident, unsigned long long 
         if (it.nitems)
             GV_LAUNCH(k_tc_items<true>, PULL_GRID, AN_THREADS, 0, s, d, (const uint32_t *)deg, it, icnt,
                       (const uint32_t *)ioff, (const unsigned long long *)b.off, b.snap);
-        GV_LAUNCH(k_tc_classify, grid_for(n, 256), 256, 0, s, (const unsigned long long *)b.off, n, b.snap, b.mid, b.big,
-                  b.cnts);
-        GV_LAUNCH(k_tc_sort_mid, 148 * 4, AN_THREADS, 0, s, (const unsigned long long *)b.off, b.snap,
-                  (const uint32_t *)b.mid, (const unsigned long long *)b.cnts);
     }
+    // per-graph word (views own theirs), so concurrent counts on views do not share it
+    unsigned long long *work = (unsigned long long *)g->bs.tile_cnt + 1;
+    cudaMemsetAsync(work, 0, 8, s);
+    const char *packed_env = std::getenv("GV_TC_PACKED");
+    if (packed_env && packed_env[0] == '1') {
+        // packed hash probe: lists unsorted, u with d+ > TCP_LIGHT to one CTA each
+        unsigned long long *hc = b.cnts + 4;  // [0] heavy count, [1] longest d+
+        cudaMemsetAsync(hc, 0, 16, s);
+        GV_LAUNCH(k_tcp_heavy_list, grid_for(n, 256), 256, 0, s, (const unsigned long long *)b.off, n, b.mid, hc);
+        unsigned long long hh[2] = {0, 0};
+        cudaError_t e = cudaMemcpyAsync(hh, hc, 16, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return cuda_status(e, "tc plan");
+        const size_t light_smem = sizeof(TcpWarp) * TCP_WARPS + (size_t)TC_CREDIT_HT * 12;
+        const size_t heavy_smem = (size_t)TCP_SSET * 4 + (size_t)TCP_CHUNK * 12 + ((size_t)TCP_CHUNK + 32) * 4 +
+                                  (size_t)TC_CREDIT_HT * 12;
+        const unsigned heavy_grid = (unsigned)std::min<unsigned long long>(std::max<unsigned long long>(hh[0], 1), 148 * 2);
+        uint32_t gcap = 0;
+        uint32_t *gset = nullptr;
+        if (2 * hh[1] > TCP_SSET) {  // sets above the shared table live in global memory, one per CTA
+            gcap = 1024;
+            while (gcap < 2 * hh[1]) gcap <<= 1;
+            gset = (uint32_t *)aux_scratch(g, 7, (size_t)gcap * heavy_grid * 4);
+            if (!gset) return GV_ERR_NOMEM;
+        }
+        const unsigned light_grid = 148 * 3;
+        ProfScope ps(PROF_TC_COUNT, s);
+        const unsigned long long *off_c = b.off;
+        const uint32_t *snap_c = b.snap;
+        auto launch = [&](auto mode_c) {
+            constexpr int M = decltype(mode_c)::value;
+            cudaFuncSetAttribute(k_tcp_light<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)light_smem);
+            cudaFuncSetAttribute(k_tcp_heavy<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)heavy_smem);
+            GV_LAUNCH(k_tcp_light<M>, light_grid, TCP_THREADS, light_smem, s, off_c, snap_c, n, b.tcount, work);
+            if (hh[0])
+                GV_LAUNCH(k_tcp_heavy<M>, heavy_grid, TCP_THREADS, heavy_smem, s, off_c, snap_c, b.tcount,
+                          (const uint32_t *)b.mid, (const unsigned long long *)hc, gset, gcap, work);
+        };
+        if (mode == TC_INCIDENT) launch(std::integral_constant<int, TC_INCIDENT>{});
+        else if (mode == TC_TOTAL) launch(std::integral_constant<int, TC_TOTAL>{});
+        else launch(std::integral_constant<int, TC_OWNER>{});
+        g->last_tc_oriented = mplus;
+        *tcount_out = b.tcount;
+        return cuda_status(cudaGetLastError(), "tc launch");
+    }
+    // merge path (default): sorted lists, merge-path intersection per oriented edge
+    GV_LAUNCH(k_tc_classify, grid_for(n, 256), 256, 0, s, (const unsigned long long *)b.off, n, b.snap, b.mid, b.big,
+              b.cnts);
+    GV_LAUNCH(k_tc_sort_mid, 148 * 4, AN_THREADS, 0, s, (const unsigned long long *)b.off, b.snap,
+              (const uint32_t *)b.mid, (const unsigned long long *)b.cnts);
     // longest list bounds the CTA sort's shared memory
     unsigned long long h[2] = {0, 0};
     cudaMemcpyAsync(h, b.cnts, 16, cudaMemcpyDeviceToHost, s);
     cudaError_t e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_status(e, "tc");
-    uint64_t max_len = 1024;  // lists up to 1024 entries are sorted by warps
-    if (h[1]) {
+    if (h[1]) {  // lists above 1024 entries: one CTA sort each
         std::vector<uint32_t> bl(h[1]);
         std::vector<unsigned long long> hoff(n + 1);
         cudaMemcpy(hoff.data(), b.off, ((size_t)n + 1) * 8, cudaMemcpyDeviceToHost);
         cudaMemcpy(bl.data(), b.big, h[1] * 4, cudaMemcpyDeviceToHost);
         uint64_t mx = 0;
         for (uint32_t u : bl) mx = std::max<uint64_t>(mx, hoff[u + 1] - hoff[u]);
-        max_len = std::max<uint64_t>(max_len, mx);
         uint32_t P = 1024;
         while (P < mx) P <<= 1;
         const size_t smem = (size_t)P * 4;
@@ -1172,43 +1385,17 @@ gv_status tc_run(gv_graph *g, cudaStream_t s, bool incident, unsigned long long 
         GV_LAUNCH(k_tc_sort_big, 148, 1024, smem, s, (const unsigned long long *)b.off, b.snap,
                   (const uint32_t *)b.big, (const unsigned long long *)b.cnts, P);
     }
-    // per-graph word (views own theirs), so concurrent counts on views do not share it
-    unsigned long long *work = (unsigned long long *)g->bs.tile_cnt + 1;
-    cudaMemsetAsync(work, 0, 8, s);
-    const char *hash_env = std::getenv("GV_TC_HASH");
-    if (!(hash_env && hash_env[0] == '1')) {
-        // merge-path intersection per oriented edge (default; hash probe kept
-        // behind GV_TC_HASH=1 for comparison)
+    {
         GV_LAUNCH(k_tc_esrc, grid_for(n, 256), 256, 0, s, (const unsigned long long *)b.off, n, b.esrc);
         const unsigned cgrid = grid_for(mplus, AN_THREADS / 8, 148 * 16);
         ProfScope ps(PROF_TC_COUNT, s);
-        if (incident) GV_LAUNCH((k_tc_count<8, true>), cgrid, AN_THREADS, 0, s, (const unsigned long long *)b.off, b.snap, b.esrc, mplus, b.tcount, work);
-        else GV_LAUNCH((k_tc_count<8, false>), cgrid, AN_THREADS, 0, s, (const unsigned long long *)b.off, b.snap, b.esrc, mplus, b.tcount, work);
-    } else {
-        // hash-probe intersection; lists above 256 entries go to one CTA each
-        constexpr uint32_t TAB = 48 * 1024;  // entries of the CTA's shared set
-        if (max_len > TAB) { set_error("oriented out-degree exceeds the shared-memory set"); return GV_ERR_UNSUPPORTED; }
-        const size_t tab_bytes = (size_t)TAB * 4;
-        static bool attr = false;
-        if (!attr) {
-            cudaFuncSetAttribute(k_tc_hash_big<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tab_bytes);
-            cudaFuncSetAttribute(k_tc_hash_big<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tab_bytes);
-            attr = true;
-        }
-        unsigned long long *nbig = b.cnts + 4;
-        cudaMemsetAsync(nbig, 0, 8, s);
-        ProfScope ps(PROF_TC_COUNT, s);
-        if (incident) {
-            GV_LAUNCH(k_tc_hash<true>, PULL_GRID, AN_THREADS, 0, s, (const unsigned long long *)b.off, (const uint32_t *)b.snap,
-                      n, b.tcount, b.mid, nbig, work);
-            GV_LAUNCH(k_tc_hash_big<true>, 148, 512, tab_bytes, s, (const unsigned long long *)b.off,
-                      (const uint32_t *)b.snap, b.tcount, (const uint32_t *)b.mid, (const unsigned long long *)nbig, TAB, work);
-        } else {
-            GV_LAUNCH(k_tc_hash<false>, PULL_GRID, AN_THREADS, 0, s, (const unsigned long long *)b.off, (const uint32_t *)b.snap,
-                      n, b.tcount, b.mid, nbig, work);
-            GV_LAUNCH(k_tc_hash_big<false>, 148, 512, tab_bytes, s, (const unsigned long long *)b.off,
-                      (const uint32_t *)b.snap, b.tcount, (const uint32_t *)b.mid, (const unsigned long long *)nbig, TAB, work);
-        }
+        const unsigned long long *off_c = b.off;
+        if (mode == TC_INCIDENT)
+            GV_LAUNCH((k_tc_count<8, TC_INCIDENT>), cgrid, AN_THREADS, 0, s, off_c, b.snap, b.esrc, mplus, b.tcount, work);
+        else if (mode == TC_TOTAL)
+            GV_LAUNCH((k_tc_count<8, TC_TOTAL>), cgrid, AN_THREADS, 0, s, off_c, b.snap, b.esrc, mplus, b.tcount, work);
+        else
+            GV_LAUNCH((k_tc_count<8, TC_OWNER>), cgrid, AN_THREADS, 0, s, off_c, b.snap, b.esrc, mplus, b.tcount, work);
     }
     g->last_tc_oriented = mplus;
     *tcount_out = b.tcount;
@@ -1573,7 +1760,8 @@ gv_status gv_tc(gv_graph *g, uint64_t *per_vertex, uint64_t *total, int mem, voi
     if (!g || !total) return GV_ERR_INVALID;
     cudaStream_t s = (cudaStream_t)stream;
     unsigned long long *tc = nullptr;
-    gv_status st = tc_run(g, s, false, &tc);
+    // the total alone needs no per-vertex credit
+    gv_status st = tc_run(g, s, per_vertex ? TC_OWNER : TC_TOTAL, &tc);
     if (st != GV_OK) return st;
     const uint32_t n = g->d.n;
     unsigned long long *dtot = (unsigned long long *)g->bs.tile_cnt;  // 8 bytes of batch scratch
@@ -1624,7 +1812,7 @@ gv_status gv_tc_subset(gv_graph *g, const uint32_t *subset, uint64_t ns, uint64_
     g->last_tc_local = done ? 1 : 0;
     if (!done) {
         unsigned long long *tc = nullptr;
-        st = tc_run(g, s, true, &tc);
+        st = tc_run(g, s, TC_INCIDENT, &tc);
         if (st != GV_OK) return st;
         GV_LAUNCH(k_gather_u64, grid_for(ns, 256), 256, 0, s, (const unsigned long long *)tc, (const uint32_t *)didx, ns, dout);
     }

@@ -146,9 +146,12 @@ gv_status gv_clear_affected(gv_graph *g, void *stream);
 gv_status gv_check(gv_graph *g, uint64_t *violations, uint32_t *first_code,
                    uint32_t *first_vertex);
 
-/* Facts about the last analytics call on this graph: "tc_work" = sum over
- * oriented edges (u->v) of |N+(u)| + |N+(v)| merged by the last triangle
- * count, "tc_oriented_edges", "sweeps" (last PageRank).  Synchronous. */
+/* Facts about the last analytics call on this graph: "tc_work" = list
+ * entries the last whole-graph triangle count read (|N+(u)| + |N+(v)| merged
+ * per oriented edge; with GV_TC_PACKED=1 probes of N+(v) plus inserts of
+ * N+(u)), "tc_oriented_edges", "tc_subset_local" (1 if the last
+ * subset count took the neighbour-hash path), "sweeps" (last PageRank).
+ * Synchronous. */
 gv_status gv_last_stat(gv_graph *g, const char *key, double *value);
 
 /* ---- analytics ---------------------------------------------------------- */

@@ -118,9 +118,12 @@ def test_triangle_subset_incident(graph12):
     assert np.array_equal(g.tc_subset(sub), o.tc_incident(sub))
 
 
-def test_hub_triangles_use_cta_sort():
+@pytest.mark.parametrize("packed", ["0", "1"])
+def test_hub_triangles_use_cta_sort(packed, monkeypatch):
     # a 1100-clique: its lowest-ranked member has an oriented list of 1099
-    # entries, above the 1024-entry warp sort, so the CTA sort runs
+    # entries, above the 1024-entry warp sort, so the CTA sort runs (merge
+    # path) or one CTA takes the vertex (packed path)
+    monkeypatch.setenv("GV_TC_PACKED", packed)
     n = 1 << 13
     K = 1100
     iu, ju = np.triu_indices(K, 1)
@@ -240,3 +243,19 @@ def test_triangle_subset_paths_agree(mode, monkeypatch):
         assert g.last_stat("tc_subset_local") == 1
     elif mode == "global":
         assert g.last_stat("tc_subset_local") == 0
+
+
+@pytest.mark.parametrize("packed", ["0", "1"])
+def test_triangle_paths_total_only_and_incident(packed, monkeypatch, graph12):
+    """Merge and packed paths, the total-only mode (no per-vertex output) and
+    the incident counts of the whole-graph subset path all match the oracle."""
+    n, g, o = graph12
+    monkeypatch.setenv("GV_TC_PACKED", packed)
+    pv, tot = g.static_tc()
+    opv, otot = o.tc()
+    assert tot == otot and np.array_equal(pv, opv)
+    _, tot2 = g.static_tc(per_vertex=False)
+    assert tot2 == otot
+    monkeypatch.setenv("GV_TC_SUBSET", "global")
+    sub = np.random.default_rng(11).choice(n, 500, replace=False).astype(np.uint32)
+    assert np.array_equal(g.tc_subset(sub), o.tc_incident(sub))
