@@ -56,6 +56,9 @@ def parse():
     ap.add_argument("--no-batching", action="store_true", help="skip the scale-24 batched-vs-plain section")
     ap.add_argument("--batch-scale", type=int, default=24)
     ap.add_argument("--c3-batches", type=int, default=64)
+    ap.add_argument("--no-diff", action="store_true", help="skip the scale-20 differentiation section")
+    ap.add_argument("--diff-scale", type=int, default=20)
+    ap.add_argument("--fd-edges", type=int, default=64)
     ap.add_argument("--no-serving", action="store_true", help="skip the scale-25 serving section")
     ap.add_argument("--serve-scale", type=int, default=25)
     ap.add_argument("--serve-requests", type=int, default=120)
@@ -344,6 +347,76 @@ def run_batching(args, dev):
             "pagerank_gteps_plain": gteps_plain, "pagerank_gteps_batched": gteps_batched,
             "pagerank_speedup": pr_plain_ms / pr_batched_ms,
             "autotune_best": best, "autotune": tune}
+
+
+def run_differentiation(args):
+    """Differentiation workload: directed weighted R-MAT (weights uniform in
+    (0.1, 1], normalised per row), weighted PageRank forward, then the
+    gradient of sum(c_i x_i), c ~ N(0, 1), with respect to every raw edge
+    weight through the adjoint solve; the gradient of args.fd_edges random
+    edges is checked against fp64 central differences (h = 1e-6) of the
+    oracle on the host."""
+    import torch
+    import gv_b200
+    import oracle
+    scale = args.diff_scale
+    n = 1 << scale
+    seed = args.seed + 300
+    rng = np.random.default_rng(seed)
+    s, d = gv_b200.gen_rmat(scale, args.edge_factor << scale, seed)
+    w = (1.0 - 0.9 * rng.random(len(s))).astype(np.float32)
+    c = rng.standard_normal(n)
+    g = gv_b200.GraphVine(n, directed=True, weighted=True, hbm_budget_bytes=8 << 30, max_batch_pairs=len(s))
+    g.batch_insert(s, d, w)
+    g.synchronize()
+    m = g.num_edges()
+    tol, it = 1e-7, 200
+    g.wpr_forward(ALPHA, tol, it)  # warm-up (scratch)
+    c32 = c.astype(np.float32)
+    torch.cuda.synchronize()
+    gv_b200.profile_reset()
+    gv_b200.profile_enable(True)
+    t0 = time.perf_counter()
+    x, sw_f = g.wpr_forward(ALPHA, tol, it)
+    torch.cuda.synchronize()
+    fwd_s = time.perf_counter() - t0
+    g.wpr_backward(x, c32, ALPHA, tol, it, mode=0)  # warm-up
+    torch.cuda.synchronize()
+    prof_f = {k: gv_b200.profile_query(k) for k in ("wpr_build", "wpr_sweep")}
+    gv_b200.profile_reset()
+    t0 = time.perf_counter()
+    grad, lam, sw_b = g.wpr_backward(x, c32, ALPHA, tol, it, mode=0)
+    torch.cuda.synchronize()
+    bwd_s = time.perf_counter() - t0
+    prof_b = {k: gv_b200.profile_query(k) for k in ("pull", "wpr_grad")}
+    gv_b200.profile_enable(False)
+    off, dst, _ = g.export_csr()
+    g.close()
+    src = np.repeat(np.arange(n, dtype=np.uint32), np.diff(off).astype(np.int64))
+    ks = rng.choice(len(dst), args.fd_edges, replace=False)
+    o = oracle.OracleGraph(n, directed=True, weighted=True)
+    o.insert(s, d, w)
+    t0 = time.perf_counter()
+    fd = o.wpr_fd(c, src[ks], dst[ks], 1e-6)
+    fd_s = time.perf_counter() - t0
+    del o
+    err = np.abs(grad[ks].astype(np.float64) - fd)
+    scale_fd = float(np.abs(fd).max())
+    return {"workload": (f"directed R-MAT scale {scale} ef {args.edge_factor}, weights U(0.1, 1] normalised per row; "
+                         f"weighted PageRank (alpha {ALPHA}, L1 tol {tol}) and d(sum c_i x_i)/d(raw weight) for "
+                         f"every entry, c ~ N(0, 1)"),
+            "m_entries": m, "forward_ms": fwd_s * 1e3, "forward_sweeps": sw_f,
+            "forward_gteps": m * sw_f / fwd_s / 1e9,
+            "forward_device_ms": {"transpose_build": prof_f["wpr_build"][0], "sweeps": prof_f["wpr_sweep"][0]},
+            "forward_sweep_gteps": m * sw_f / (prof_f["wpr_sweep"][0] / 1e3) / 1e9 if prof_f["wpr_sweep"][0] else None,
+            "backward_ms": bwd_s * 1e3, "adjoint_sweeps": sw_b,
+            "backward_device_ms": {"adjoint_sweeps": prof_b["pull"][0], "gradient": prof_b["wpr_grad"][0]},
+            "adjoint_sweep_gteps": m * sw_b / (prof_b["pull"][0] / 1e3) / 1e9 if prof_b["pull"][0] else None,
+            "backward_note": "adjoint solve + one gradient entry per stored entry, returned to the host in export order",
+            "fd_check": {"edges": int(args.fd_edges), "h": 1e-6, "kind": "fp64 central differences (oracle, host)",
+                         "max_abs_err": float(err.max()), "max_abs_fd": scale_fd,
+                         "max_err_over_max_fd": float(err.max() / scale_fd) if scale_fd else None,
+                         "oracle_seconds": fd_s}}
 
 
 def make_serve_trace(n, s_dev, d_dev, nreq, seed):
@@ -665,6 +738,8 @@ def run_gv(args, rank, world, local_rank):
                        "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"]}
     if world == 1 and not args.no_batching:
         line["batching"] = run_batching(args, torch.device("cuda", local_rank))
+    if world == 1 and not args.no_diff:
+        line["differentiation"] = run_differentiation(args)
     if world == 1 and not args.no_serving:
         line["serving"] = run_serving(args, torch.device("cuda", local_rank))
     if world == 1 and not args.no_cpu_baseline:

@@ -69,7 +69,7 @@ def version() -> str:
 
 
 PROFILE_SLOTS = ("radix", "segment", "member", "apply", "compact", "pull", "tc_snapshot", "tc_count",
-                 "bfs_level", "bc_dep")
+                 "bfs_level", "bc_dep", "wpr_build", "wpr_sweep", "wpr_grad")
 
 
 def profile_enable(on: bool = True) -> None:

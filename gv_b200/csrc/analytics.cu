@@ -1420,40 +1420,93 @@ __global__ void k_row_sums(DevGraph g, float *__restrict__ rinv) {
 }
 
 // Transposed snapshot: in-edges of every v with the raw weight.
-__global__ void k_indeg(DevGraph g, uint32_t *__restrict__ indeg) {
-    for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < g.n; u += gridDim.x * blockDim.x) {
-        const uint4 rec = g.vtx[u];
-        const uint32_t fill = rec.y, nb = blocks_for(fill, g.logB);
-        for (uint32_t k = 0; k < nb; ++k) {
-            const uint32_t b = k == 0 ? rec.x : cbt_block(g.left, g.right, rec.x, k);
-            const uint32_t slots = min(g.B, fill - (k << g.logB));
-            const size_t base = (size_t)b << g.logB;
-            for (uint32_t i = 0; i < slots; ++i) {
-                const uint32_t v = g.pool[base + i];
-                if (v != GV_TOMB) atomicAdd(&indeg[v], 1u);
-            }
+// In-edge transpose for weighted PageRank: one key (v << bitsn | u) per
+// stored entry (found from the exported offsets), the weight's bits carried
+// as the value; a stable radix sort then groups in-edges by v, ordered by u,
+// so the transpose (and every sum over it) is the same on every call.
+__global__ void k_wpr_keys(const unsigned long long *__restrict__ off, const uint32_t *__restrict__ dst,
+                           const float *__restrict__ w, uint32_t n, uint64_t E, uint32_t bitsn,
+                           unsigned long long *__restrict__ keys, uint32_t *__restrict__ vals) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < E; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t lo = 0, hi = n;  // last u with off[u] <= i
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (off[mid] <= i) lo = mid;
+            else hi = mid;
         }
+        keys[i] = ((unsigned long long)dst[i] << bitsn) | lo;
+        vals[i] = __float_as_uint(w[i]);
     }
 }
 
-__global__ void k_fill_transpose(DevGraph g, const unsigned long long *__restrict__ toff, uint32_t *__restrict__ cursor,
-                                 uint32_t *__restrict__ tsrc, float *__restrict__ tw) {
-    for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < g.n; u += gridDim.x * blockDim.x) {
-        const uint4 rec = g.vtx[u];
-        const uint32_t fill = rec.y, nb = blocks_for(fill, g.logB);
-        for (uint32_t k = 0; k < nb; ++k) {
-            const uint32_t b = k == 0 ? rec.x : cbt_block(g.left, g.right, rec.x, k);
-            const uint32_t slots = min(g.B, fill - (k << g.logB));
-            const size_t base = (size_t)b << g.logB;
-            for (uint32_t i = 0; i < slots; ++i) {
-                const uint32_t v = g.pool[base + i];
-                if (v == GV_TOMB) continue;
-                const unsigned long long p = toff[v] + atomicAdd(&cursor[v], 1u);
-                tsrc[p] = u;
-                tw[p] = g.wpool[base + i];
-            }
+// toff[v] = first sorted key of destination v (v = 0..n).
+__global__ void k_wpr_toff(const unsigned long long *__restrict__ keys, uint64_t E, uint32_t n, uint32_t bitsn,
+                           unsigned long long *__restrict__ toff) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v <= n; v += gridDim.x * blockDim.x) {
+        const unsigned long long x = (unsigned long long)v << bitsn;
+        uint64_t lo = 0, hi = E;
+        while (lo < hi) {
+            const uint64_t mid = (lo + hi) >> 1;
+            if (keys[mid] < x) lo = mid + 1;
+            else hi = mid;
         }
+        toff[v] = lo;
     }
+}
+
+__global__ void k_wpr_unpack(const unsigned long long *__restrict__ keys, const uint32_t *__restrict__ vals, uint64_t E,
+                             unsigned long long mask, uint32_t *__restrict__ tsrc, float *__restrict__ tw) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < E; i += (uint64_t)gridDim.x * blockDim.x) {
+        tsrc[i] = (uint32_t)(keys[i] & mask);
+        tw[i] = __uint_as_float(vals[i]);
+    }
+}
+
+// Vertices with more than WPR_HEAVY in-edges (one CTA each in the sweeps).
+constexpr uint32_t WPR_HEAVY = 1024;
+constexpr unsigned WPR_HEAVY_GRID = FIN_GRID;
+
+__global__ void k_wpr_heavy_list(const unsigned long long *__restrict__ toff, uint32_t n, uint32_t *__restrict__ list,
+                                 uint32_t *cnt) {
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        const uint32_t v = base + threadIdx.x;
+        const bool heavy = v < n && toff[v + 1] - toff[v] > WPR_HEAVY;
+        const uint32_t bal = __ballot_sync(GV_FULL_MASK, heavy);
+        uint32_t at = 0;
+        if (lane == 0 && bal) at = atomicAdd(cnt, (uint32_t)__popc(bal));
+        at = __shfl_sync(GV_FULL_MASK, at, 0);
+        if (heavy) list[at + __popc(bal & ((1u << lane) - 1u))] = v;
+    }
+}
+
+// Heavy in-edge lists: the CTA's threads stride over the list, the block sum
+// is taken in a fixed order; partial slot part_base + blockIdx.x.
+__global__ void __launch_bounds__(AN_THREADS) k_wpr_fwd_heavy(const unsigned long long *__restrict__ toff,
+                                                              const uint32_t *__restrict__ tsrc,
+                                                              const float *__restrict__ tw,
+                                                              const uint32_t *__restrict__ list, const uint32_t *cnt,
+                                                              PullArgs a, uint32_t part_base) {
+    __shared__ float red[AN_THREADS / 32];
+    if (a.state[0]) return;
+    const uint32_t nh = *cnt;
+    double res = 0.0;
+    for (uint32_t h = blockIdx.x; h < nh; h += gridDim.x) {
+        const uint32_t v = list[h];
+        float sum = 0.f;
+        for (unsigned long long i = toff[v] + threadIdx.x; i < toff[v + 1]; i += AN_THREADS)
+            sum += tw[i] * __ldg(a.gather + tsrc[i]);
+        sum = warp_sum(sum);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = sum;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            float t = 0.f;
+            for (int i = 0; i < AN_THREADS / 32; ++i) t += red[i];
+            pull_finish(a, v, t, 0, res);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) a.partial[part_base + blockIdx.x] = res;
 }
 
 // Group per v over its in-edges: x'[v] = base + alpha * sum w_uv * contrib[u]
@@ -1468,6 +1521,7 @@ __global__ void __launch_bounds__(AN_THREADS) k_wpr_fwd(uint32_t n, const unsign
     double res = 0.0;
     const uint32_t ngroups = gridDim.x * GPC;
     for (uint32_t v = blockIdx.x * GPC + threadIdx.x / TPV; v < n; v += ngroups) {
+        if (toff[v + 1] - toff[v] > WPR_HEAVY) continue;  // k_wpr_fwd_heavy
         float sum = 0.f;
         for (unsigned long long i = toff[v] + G.gl; i < toff[v + 1]; i += TPV) sum += tw[i] * __ldg(a.gather + tsrc[i]);
         sum = G.sum(sum);
@@ -1487,39 +1541,23 @@ __global__ void k_mul(const float *__restrict__ x, const float *__restrict__ r, 
     for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) y[v] = x[v] * r[v];
 }
 
-// Gradient per live entry, in export order (offsets = exclusive scan of live degrees).
-template <int TPV>
-__global__ void __launch_bounds__(AN_THREADS) k_wpr_grad(DevGraph g, const unsigned long long *__restrict__ off,
-                                                         const float *__restrict__ x, const float *__restrict__ lam,
-                                                         const float *__restrict__ c, const float *__restrict__ rinv,
-                                                         float alpha, int mode, float *__restrict__ grad) {
-    Group<TPV> G;
-    constexpr int GPC = AN_THREADS / TPV;
-    const uint32_t ngroups = gridDim.x * GPC;
-    for (uint32_t u = blockIdx.x * GPC + threadIdx.x / TPV; u < g.n; u += ngroups) {
-        const uint4 rec = g.vtx[u];
-        const uint32_t fill = rec.y, nb = blocks_for(fill, g.logB);
-        unsigned long long w = off[u];
-        const unsigned long long wend = off[u + 1];
-        const float xu = x[u];
-        const float ku = mode == 1 ? 0.f : (c[u] - lam[u]);
-        const float ru = rinv[u];
-        for (uint32_t k = 0; k < nb; ++k) {
-            const uint32_t b = (k == 0) ? rec.x : cbt_block(g.left, g.right, rec.x, k);
-            const uint32_t slots = min(g.B, fill - (k << g.logB));
-            for (uint32_t c0 = 0; c0 < slots; c0 += TPV) {
-                const uint32_t i = c0 + G.gl;
-                const uint32_t v = (i < slots) ? g.pool[((size_t)b << g.logB) + i] : GV_TOMB;
-                const uint32_t keep = v != GV_TOMB;
-                uint32_t tot;
-                const uint32_t pre = G.excl_scan(keep, tot);
-                if (keep && w + pre < wend) {
-                    const float lv = lam[v];
-                    grad[w + pre] = (mode == 1) ? alpha * xu * lv : xu * (alpha * lv + ku) * ru;
-                }
-                w += tot;
-            }
+// Gradient per entry from the exported CSR (dst in export order): one thread
+// per entry, its source found by binary search in the offsets, so hubs cost
+// no more than any other vertex.
+__global__ void k_wpr_grad_flat(const unsigned long long *__restrict__ off, const uint32_t *__restrict__ dst,
+                                uint64_t E, uint32_t n, const float *__restrict__ x, const float *__restrict__ lam,
+                                const float *__restrict__ c, const float *__restrict__ rinv, float alpha, int mode,
+                                float *__restrict__ grad) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < E; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t lo = 0, hi = n;  // last u with off[u] <= i
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (off[mid] <= i) lo = mid;
+            else hi = mid;
         }
+        const uint32_t u = lo;
+        const float lv = lam[dst[i]];
+        grad[i] = (mode == 1) ? alpha * x[u] * lv : x[u] * (alpha * lv + (c[u] - lam[u])) * rinv[u];
     }
 }
 
@@ -1849,15 +1887,51 @@ gv_status gv_wpr_forward(gv_graph *g, float alpha, float tol, int32_t max_iter, 
     unsigned long long *toff = (unsigned long long *)p; p += ((size_t)n + 1) * 8;
     uint32_t *tsrc = (uint32_t *)p; p += (live + 1) * 4;
     float *tw = (float *)p;
+    uint32_t *heavy = cursor;  // list of vertices above WPR_HEAVY in-edges (n words)
     GV_LAUNCH(k_row_sums, grid_for(n, 256), 256, 0, s, d, rinv);
-    cudaMemsetAsync(indeg, 0, (size_t)n * 4, s);
-    cudaMemsetAsync(cursor, 0, (size_t)n * 4, s);
-    GV_LAUNCH(k_indeg, grid_for(n, 256), 256, 0, s, d, indeg);
-    scan_exclusive_u32_to_u64(indeg, toff, n, toff + n, g->bs.scan_tmp, s);
-    GV_LAUNCH(k_fill_transpose, grid_for(n, 256), 256, 0, s, d, (const unsigned long long *)toff, cursor, tsrc, tw);
+    {
+        ProfScope ps(PROF_WPR_BUILD, s);
+        // export (storage order), keys (v, u) with weight bits, stable radix sort by (v, u)
+        const uint64_t E = live;
+        const uint64_t rc = radix_counts_elems(std::max<uint64_t>(E, 1));
+        const size_t o_off = 0, o_dst = o_off + (((size_t)n + 1) * 8 + 255) / 256 * 256;
+        const size_t o_w = o_dst + (E * 4 + 255) / 256 * 256, o_k = o_w + (E * 4 + 255) / 256 * 256;
+        const size_t o_k2 = o_k + (E * 8 + 255) / 256 * 256, o_v = o_k2 + (E * 8 + 255) / 256 * 256;
+        const size_t o_v2 = o_v + (E * 4 + 255) / 256 * 256, o_c = o_v2 + (E * 4 + 255) / 256 * 256;
+        const size_t o_t = o_c + (rc * 4 + 255) / 256 * 256;
+        const size_t sbytes = o_t + scan_scratch_bytes(std::max<uint64_t>(rc, (uint64_t)n + 1)) + 256;
+        char *sb = (char *)aux_scratch(g, 5, sbytes);
+        if (!sb) return GV_ERR_NOMEM;
+        unsigned long long *eoff = (unsigned long long *)(sb + o_off);
+        uint32_t *edst = (uint32_t *)(sb + o_dst);
+        float *ew = (float *)(sb + o_w);
+        unsigned long long *k1 = (unsigned long long *)(sb + o_k), *k2 = (unsigned long long *)(sb + o_k2);
+        uint32_t *v1 = (uint32_t *)(sb + o_v), *v2 = (uint32_t *)(sb + o_v2), *cnts = (uint32_t *)(sb + o_c);
+        void *stmp = sb + o_t;
+        launch_degrees(g, indeg, s);
+        scan_exclusive_u32_to_u64(indeg, eoff, n, eoff + n, stmp, s);
+        gv_status est = run_export(g, eoff, edst, ew, s);
+        if (est != GV_OK) return est;
+        if (E) {
+            GV_LAUNCH(k_wpr_keys, grid_for(E, 256, 148 * 16), 256, 0, s, (const unsigned long long *)eoff,
+                      (const uint32_t *)edst, (const float *)ew, n, E, g->bitsn, k1, v1);
+            const int which = radix_sort_u64(k1, k2, v1, v2, E, 2 * (int)g->bitsn, cnts, stmp, s);
+            const unsigned long long *ks = which ? k2 : k1;
+            GV_LAUNCH(k_wpr_unpack, grid_for(E, 256, 148 * 16), 256, 0, s, ks, which ? v2 : v1, E,
+                      (1ull << g->bitsn) - 1, tsrc, tw);
+            GV_LAUNCH(k_wpr_toff, grid_for((uint64_t)n + 1, 256), 256, 0, s, ks, E, n, g->bitsn, toff);
+        } else {
+            cudaMemsetAsync(toff, 0, ((size_t)n + 1) * 8, s);
+        }
+    }
+    // count of the heavy list: the third word of the residual slot (the
+    // sweeps write only its first 8 bytes)
+    uint32_t *hcnt = reinterpret_cast<uint32_t *>(b.res) + 2;
+    cudaMemsetAsync(hcnt, 0, 4, s);
+    GV_LAUNCH(k_wpr_heavy_list, grid_for(n, 256), 256, 0, s, (const unsigned long long *)toff, n, heavy, hcnt);
     GV_LAUNCH(k_fill_f32, grid_for(n, 256), 256, 0, s, b.x0, n, 1.0f / (float)n, GV_NIL, 0.f);
     cudaMemsetAsync(b.state, 0, 16, s);
-    const uint32_t nparts = PULL_GRID;
+    const uint32_t nparts = PULL_GRID + WPR_HEAVY_GRID;
     float *xa = b.x0, *xb = b.x1;
     int h_state[2] = {0, 0};
     int launched = 0;
@@ -1874,11 +1948,17 @@ gv_status gv_wpr_forward(gv_graph *g, float alpha, float tol, int32_t max_iter, 
             a.gather = b.c0;
             a.xold = xa;
             a.xnew = xb;
-            dispatch_tpv(g->cfg.threads_per_vertex, [&](auto t) {
-                constexpr int T = decltype(t)::value;
-                GV_LAUNCH((k_wpr_fwd<T>), PULL_GRID, AN_THREADS, 0, s, n, (const unsigned long long *)toff,
-                          (const uint32_t *)tsrc, (const float *)tw, a);
-            });
+            {
+                ProfScope ps(PROF_WPR_SWEEP, s);
+                dispatch_tpv(g->cfg.threads_per_vertex, [&](auto t) {
+                    constexpr int T = decltype(t)::value;
+                    GV_LAUNCH((k_wpr_fwd<T>), PULL_GRID, AN_THREADS, 0, s, n, (const unsigned long long *)toff,
+                              (const uint32_t *)tsrc, (const float *)tw, a);
+                });
+                GV_LAUNCH(k_wpr_fwd_heavy, WPR_HEAVY_GRID, AN_THREADS, 0, s, (const unsigned long long *)toff,
+                          (const uint32_t *)tsrc, (const float *)tw, (const uint32_t *)heavy, (const uint32_t *)hcnt, a,
+                          PULL_GRID);
+            }
             GV_LAUNCH(k_iter_done, 1, 256, 0, s, b.partial, nparts, tol, b.state, b.res);
             std::swap(xa, xb);
         }
@@ -1945,11 +2025,16 @@ gv_status gv_wpr_backward(gv_graph *g, float alpha, float tol, int32_t max_iter,
     launch_degrees(g, deg, s);
     scan_exclusive_u32_to_u64(deg, off, n, off + n, g->bs.scan_tmp, s);
     float *gout = mem == GV_MEM_DEVICE ? grad : dgrad;
-    dispatch_tpv(g->cfg.threads_per_vertex, [&](auto t) {
-        constexpr int T = decltype(t)::value;
-        GV_LAUNCH((k_wpr_grad<T>), grid_for(n, AN_THREADS / T), AN_THREADS, 0, s, d, (const unsigned long long *)off,
-                  (const float *)dx, (const float *)lam, (const float *)dc, (const float *)rinv, alpha, mode, gout);
-    });
+    if (live) {
+        uint32_t *edst = (uint32_t *)aux_scratch(g, 5, live * 4 + 256);
+        if (!edst) return GV_ERR_NOMEM;
+        ProfScope ps(PROF_WPR_GRAD, s);
+        st = run_export(g, off, edst, nullptr, s);
+        if (st != GV_OK) return st;
+        GV_LAUNCH(k_wpr_grad_flat, grid_for(live, 256, 148 * 16), 256, 0, s, (const unsigned long long *)off,
+                  (const uint32_t *)edst, live, n, (const float *)dx, (const float *)lam, (const float *)dc,
+                  (const float *)rinv, alpha, mode, gout);
+    }
     cudaError_t e = cudaSuccess;
     if (mem != GV_MEM_DEVICE) e = cudaMemcpyAsync(grad, dgrad, live * 4, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);

@@ -200,7 +200,8 @@ gv_status read_ctl(gv_graph *g, Ctl *out, cudaStream_t s) {
 // ----------------------------------------------------------------- profiler
 namespace {
 const char *const kProfNames[PROF_NSLOTS] = {"radix", "segment", "member", "apply", "compact",
-                                             "pull", "tc_snapshot", "tc_count", "bfs_level", "bc_dep"};
+                                             "pull", "tc_snapshot", "tc_count", "bfs_level", "bc_dep",
+                                             "wpr_build", "wpr_sweep", "wpr_grad"};
 struct ProfRec {
     int slot;
     cudaEvent_t a, b;

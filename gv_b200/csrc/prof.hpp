@@ -18,6 +18,9 @@ enum ProfSlot {
     PROF_TC_COUNT,
     PROF_BFS_LEVEL,
     PROF_BC_DEP,
+    PROF_WPR_BUILD,
+    PROF_WPR_SWEEP,
+    PROF_WPR_GRAD,
     PROF_NSLOTS
 };
 

@@ -35,6 +35,7 @@ _SIG = {
     "or_wpr_adjoint": (C.c_int, [_P, C.c_double, C.c_double, C.c_int, _P, _P]),
     "or_wpr_gradient": (None, [_P, C.c_double, _P, _P, _P, C.c_int, _P]),
     "or_wpr_objective": (C.c_double, [_P, C.c_double, C.c_double, C.c_int, _P, C.c_uint32, C.c_uint32, C.c_double]),
+    "or_wpr_fd": (C.c_int, [_P, C.c_double, C.c_double, C.c_int, _P, _P, _P, C.c_uint32, C.c_double, _P]),
     "or_rmat_pairs": (None, [C.c_uint32, C.c_uint64, C.c_uint64, _P, _P]),
 }
 _lib = None
@@ -156,6 +157,15 @@ class OracleGraph:
         xa, la, ca = (np.ascontiguousarray(v, dtype=np.float64) for v in (x, lam, c))
         lib().or_wpr_gradient(self._h, alpha, xa.ctypes.data, la.ctypes.data, ca.ctypes.data, mode, g.ctypes.data)
         return g[: self.num_edges()]
+
+    def wpr_fd(self, c, eu, ev, h=1e-6, alpha=0.85, tol=1e-15, max_iter=2000):
+        """fp64 central differences of sum c_i x_i w.r.t. the raw weights of entries (eu[i], ev[i])."""
+        ca = np.ascontiguousarray(c, dtype=np.float64)
+        u, v = _u32(eu), _u32(ev)
+        out = np.empty(len(u), np.float64)
+        lib().or_wpr_fd(self._h, alpha, tol, max_iter, ca.ctypes.data, u.ctypes.data, v.ctypes.data, len(u), h,
+                        out.ctypes.data)
+        return out
 
     def wpr_objective(self, c, u, v, delta, alpha=0.85, tol=1e-15, max_iter=2000):
         ca = np.ascontiguousarray(c, dtype=np.float64)

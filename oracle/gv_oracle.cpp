@@ -558,6 +558,75 @@ double or_wpr_objective(const or_graph *g, double alpha, double tol, int max_ite
     return j;
 }
 
+int or_wpr_fd(const or_graph *g, double alpha, double tol, int max_iter, const double *c, const uint32_t *eu,
+              const uint32_t *ev, uint32_t k, double h, double *fd) {
+    const uint32_t n = g->n;
+    // transpose once; pos[u][i] = slot of out-entry i of u in the transpose
+    std::vector<uint64_t> toff(n + 1, 0);
+    for (uint32_t u = 0; u < n; ++u)
+        for (uint32_t v : g->adj[u]) toff[v + 1]++;
+    for (uint32_t v = 0; v < n; ++v) toff[v + 1] += toff[v];
+    std::vector<uint32_t> tsrc(toff[n]);
+    std::vector<double> tw(toff[n]);
+    std::vector<std::vector<uint64_t>> pos(n);
+    std::vector<uint64_t> cur(toff.begin(), toff.end() - 1);
+    const std::vector<double> rinv = row_inverse(g);
+    for (uint32_t u = 0; u < n; ++u) {
+        pos[u].resize(g->adj[u].size());
+        for (size_t i = 0; i < g->adj[u].size(); ++i) {
+            const uint64_t p = cur[g->adj[u][i]]++;
+            tsrc[p] = u;
+            tw[p] = (g->weighted ? (double)g->w[u][i] : 1.0) * rinv[u];
+            pos[u][i] = p;
+        }
+    }
+    const double base = (1.0 - alpha) / n;
+    auto solve = [&](std::vector<double> &x) {
+        std::vector<double> xn(n);
+        int sweeps = 0;
+        for (int it = 0; it < max_iter; ++it) {
+            double diff = 0.0;
+#pragma omp parallel for schedule(dynamic, 1024) reduction(+ : diff)
+            for (long v = 0; v < (long)n; ++v) {
+                double acc = 0.0;
+                for (uint64_t i = toff[v]; i < toff[v + 1]; ++i) acc += tw[i] * x[tsrc[i]];
+                xn[v] = base + alpha * acc;
+                diff += std::fabs(xn[v] - x[v]);
+            }
+            x.swap(xn);
+            ++sweeps;
+            if (diff < tol) break;
+        }
+        return sweeps;
+    };
+    auto objective = [&](const std::vector<double> &x) {
+        double j = 0.0;
+        for (uint32_t i = 0; i < n; ++i) j += c[i] * x[i];
+        return j;
+    };
+    std::vector<double> x0(n, 1.0 / n);
+    const int sweeps = solve(x0);
+    for (uint32_t e = 0; e < k; ++e) {
+        const uint32_t u = eu[e];
+        double jj[2] = {0.0, 0.0};
+        for (int side = 0; side < 2; ++side) {
+            const double delta = side == 0 ? h : -h;
+            double sum = 0.0;
+            for (size_t i = 0; i < g->adj[u].size(); ++i)
+                sum += (g->weighted ? (double)g->w[u][i] : 1.0) + (g->adj[u][i] == ev[e] ? delta : 0.0);
+            for (size_t i = 0; i < g->adj[u].size(); ++i)
+                tw[pos[u][i]] = ((g->weighted ? (double)g->w[u][i] : 1.0) + (g->adj[u][i] == ev[e] ? delta : 0.0)) / sum;
+            std::vector<double> x = x0;
+            solve(x);
+            jj[side] = objective(x);
+        }
+        for (size_t i = 0; i < g->adj[u].size(); ++i)
+            tw[pos[u][i]] = (g->weighted ? (double)g->w[u][i] : 1.0) * rinv[u];
+        fd[e] = (jj[0] - jj[1]) / (2.0 * h);
+    }
+    return sweeps;
+}
+
 void or_rmat_pairs(uint32_t scale, uint64_t num_pairs, uint64_t seed, uint32_t *src, uint32_t *dst) {
 #pragma omp parallel for schedule(static)
     for (long long i = 0; i < (long long)num_pairs; ++i) gv_rmat_pair(seed, (uint64_t)i, scale, &src[i], &dst[i]);

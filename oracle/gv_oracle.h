@@ -73,6 +73,15 @@ void or_wpr_gradient(const or_graph *g, double alpha, const double *x, const dou
 double or_wpr_objective(const or_graph *g, double alpha, double tol, int max_iter, const double *c,
                         uint32_t u, uint32_t v, double delta);
 
+/* Central finite differences (J(w + h) - J(w - h)) / 2h of J = sum c_i x_i
+ * with respect to the raw weights of the k entries (eu[i], ev[i]), in fp64.
+ * The transposed, normalised matrix is built once and only row eu[i] is
+ * re-weighted per evaluation; each perturbed solve starts from the converged
+ * unperturbed x and runs until the L1 step is below tol.  Returns the
+ * unperturbed sweeps. */
+int or_wpr_fd(const or_graph *g, double alpha, double tol, int max_iter, const double *c, const uint32_t *eu,
+              const uint32_t *ev, uint32_t k, double h, double *fd);
+
 /* Seeded R-MAT pairs, the same generator libgv uses (gv_b200/csrc/rmat.h). */
 void or_rmat_pairs(uint32_t scale, uint64_t num_pairs, uint64_t seed, uint32_t *src, uint32_t *dst);
 

@@ -259,3 +259,26 @@ def test_triangle_paths_total_only_and_incident(packed, monkeypatch, graph12):
     monkeypatch.setenv("GV_TC_SUBSET", "global")
     sub = np.random.default_rng(11).choice(n, 500, replace=False).astype(np.uint32)
     assert np.array_equal(g.tc_subset(sub), o.tc_incident(sub))
+
+
+def test_wpr_forward_hub_in_edges_and_repeatable():
+    """A vertex with 3000 in-edges takes the CTA-per-vertex sweep; the sorted
+    in-edge transpose makes two calls bit-for-bit equal."""
+    scale = 12
+    n = 1 << scale
+    s, d = rmat_graph(scale, 8, seed=13)
+    rng = np.random.default_rng(13)
+    hs = rng.choice(n, 3000, replace=False).astype(np.uint32)
+    hs = hs[hs != 5]
+    s = np.concatenate([s, hs])
+    d = np.concatenate([d, np.full(len(hs), 5, np.uint32)])
+    w = rng.uniform(0.1, 1.0, len(s)).astype(np.float32)
+    g = make_graph(n, directed=True, weighted=True)
+    g.batch_insert(s, d, w)
+    o = oracle.OracleGraph(n, directed=True, weighted=True)
+    o.insert(s, d, w)
+    x1, _ = g.wpr_forward(0.85, 1e-9, 300)
+    x2, _ = g.wpr_forward(0.85, 1e-9, 300)
+    xo, _ = o.wpr_forward(0.85)
+    assert np.abs(x1 - xo).sum() < PR_L1
+    assert np.array_equal(x1, x2)

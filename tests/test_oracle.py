@@ -195,6 +195,31 @@ def test_wpr_gradient_matches_finite_differences():
         assert abs(fd - grad[k]) <= 1e-7 * max(1.0, abs(grad[k])) + 1e-9, (k, fd, grad[k])
 
 
+def test_batched_finite_differences_match_single_ones():
+    """or_wpr_fd (one transpose, warm-started perturbed solves) agrees with
+    the one-edge objective and with the adjoint gradient."""
+    n = 1 << 9
+    s, d = rmat_graph(9, 8, seed=12)
+    rng = np.random.default_rng(5)
+    w = rng.uniform(0.1, 1.0, len(s)).astype(np.float32)
+    g = oracle.OracleGraph(n, directed=True, weighted=True)
+    g.insert(s, d, w)
+    off, dst, _ = g.export()
+    c = rng.standard_normal(n)
+    x, _ = g.wpr_forward()
+    lam, _ = g.wpr_adjoint(c)
+    grad = g.wpr_gradient(x, lam, c, mode=0)
+    src = np.repeat(np.arange(n), np.diff(off).astype(np.int64))
+    ks = rng.choice(len(dst), 12, replace=False)
+    h = 1e-6
+    fd = g.wpr_fd(c, src[ks], dst[ks], h)
+    for i, k in enumerate(ks):
+        u, v = int(src[k]), int(dst[k])
+        single = (g.wpr_objective(c, u, v, h) - g.wpr_objective(c, u, v, -h)) / (2 * h)
+        assert abs(fd[i] - single) <= 1e-8 * max(1.0, abs(single)) + 1e-10, (k, fd[i], single)
+        assert abs(fd[i] - grad[k]) <= 1e-7 * max(1.0, abs(grad[k])) + 1e-9, (k, fd[i], grad[k])
+
+
 def test_generator_is_shared_with_libgv():
     import gv_b200
     s1, d1 = oracle.rmat_pairs(12, 5000, 77)
