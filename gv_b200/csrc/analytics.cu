@@ -83,11 +83,12 @@ __device__ __forceinline__ float pull_finish(const PullArgs &a, uint32_t v, floa
 // chain vertex -> block -> neighbours is paid once per thread instead of
 // once per vertex by a whole lane group.
 template <bool W>
-__global__ void __launch_bounds__(AN_THREADS) k_pull_tiny(DevGraph g, PullArgs a, uint32_t part_base) {
+__device__ __forceinline__ void pull_tiny_body(const DevGraph &g, const PullArgs &a, uint32_t part_base, uint32_t vb,
+                                               uint32_t vg) {
     __shared__ double red[AN_THREADS / 32];
     if (a.state[0]) return;
     double res = 0.0;
-    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < g.n; v += gridDim.x * blockDim.x) {
+    for (uint32_t v = vb * blockDim.x + threadIdx.x; v < g.n; v += vg * blockDim.x) {
         const uint4 rec = g.vtx[v];
         const uint32_t fill = rec.y;
         if (fill > TINY_FILL) continue;  // k_pull / k_pull_items
@@ -117,21 +118,21 @@ __global__ void __launch_bounds__(AN_THREADS) k_pull_tiny(DevGraph g, PullArgs a
     if (threadIdx.x == 0) {
         double t = 0.0;
         for (int i = 0; i < AN_THREADS / 32; ++i) t += red[i];
-        a.partial[part_base + blockIdx.x] = t;
+        a.partial[part_base + vb] = t;
     }
 }
 
 template <int TPV, bool W>
-__global__ void __launch_bounds__(AN_THREADS) k_pull(DevGraph g, PullArgs a) {
+__device__ __forceinline__ void pull_body(const DevGraph &g, const PullArgs &a, uint32_t vb, uint32_t vg) {
     __shared__ double red[AN_THREADS / 32];
     if (a.state[0]) return;
     constexpr int GPC = AN_THREADS / TPV;
     __shared__ uint32_t tabs[GPC][BIG_BLOCKS];
     Group<TPV> G;
     uint32_t *tab = tabs[threadIdx.x / TPV];
-    const uint32_t ngroups = gridDim.x * GPC;
+    const uint32_t ngroups = vg * GPC;
     double res = 0.0;
-    for (uint32_t v = blockIdx.x * GPC + threadIdx.x / TPV; v < g.n; v += ngroups) {
+    for (uint32_t v = vb * GPC + threadIdx.x / TPV; v < g.n; v += ngroups) {
         const uint4 rec = g.vtx[v];
         const uint32_t fill = rec.y, nb = blocks_for(fill, g.logB);
         if (fill > LIGHT_FILL || fill <= TINY_FILL) continue;  // k_pull_items / k_pull_tiny
@@ -175,7 +176,7 @@ __global__ void __launch_bounds__(AN_THREADS) k_pull(DevGraph g, PullArgs a) {
     if (threadIdx.x == 0) {
         double t = 0.0;
         for (int i = 0; i < AN_THREADS / 32; ++i) t += red[i];
-        a.partial[blockIdx.x] = t;
+        a.partial[vb] = t;
     }
 }
 
@@ -218,11 +219,12 @@ __device__ __forceinline__ uint32_t item_block(const DevGraph &g, uint4 rec, uin
 }
 
 template <bool W>
-__global__ void __launch_bounds__(AN_THREADS) k_pull_items(DevGraph g, PullArgs a, Items it, float *__restrict__ ipart) {
+__device__ __forceinline__ void pull_items_body(const DevGraph &g, const PullArgs &a, const Items &it,
+                                                float *__restrict__ ipart, uint32_t vb, uint32_t vg) {
     if (a.state[0]) return;
     const uint32_t lane = threadIdx.x & 31;
-    const uint32_t nw = gridDim.x * (AN_THREADS / 32);
-    for (uint32_t i = blockIdx.x * (AN_THREADS / 32) + (threadIdx.x >> 5); i < it.nitems; i += nw) {
+    const uint32_t nw = vg * (AN_THREADS / 32);
+    for (uint32_t i = vb * (AN_THREADS / 32) + (threadIdx.x >> 5); i < it.nitems; i += nw) {
         const uint32_t v = it.item_vertex[i];
         const uint32_t c = i - it.item_first[v];
         const uint4 rec = g.vtx[v];
@@ -252,6 +254,18 @@ __global__ void __launch_bounds__(AN_THREADS) k_pull_items(DevGraph g, PullArgs 
         sum = warp_sum(sum);
         if (lane == 0) ipart[i] = sum;
     }
+}
+
+// One launch for the three tiers of a sweep, CTAs interleaved (CTA i runs
+// tier i % 3) so the thread-per-vertex, lane-group and hub-item work share
+// every wave instead of running one after another.
+template <int TPV, bool W>
+__global__ void __launch_bounds__(AN_THREADS) k_pull_fused(DevGraph g, PullArgs a, Items it, float *__restrict__ ipart,
+                                                           uint32_t tiny_base) {
+    const uint32_t part = blockIdx.x % 3u, vb = blockIdx.x / 3u, vg = gridDim.x / 3u;
+    if (part == 0) pull_body<TPV, W>(g, a, vb, vg);
+    else if (part == 1) pull_tiny_body<W>(g, a, tiny_base, vb, vg);
+    else pull_items_body<W>(g, a, it, ipart, vb, vg);
 }
 
 __global__ void __launch_bounds__(AN_THREADS) k_pull_items_fin(DevGraph g, PullArgs a, Items it,
@@ -411,18 +425,16 @@ gv_status run_sweeps(gv_graph *g, cudaStream_t s, IterBufs &b, PullArgs proto, b
             a.state = b.state;
             if (!contrib_pr && !weighted) a.gather = ca;
             ProfScope ps(PROF_PULL, s);
+            static_assert(TINY_GRID == PULL_GRID, "the fused sweep gives each tier the same CTA count");
             dispatch_tpv(g->cfg.threads_per_vertex, [&](auto t) {
                 constexpr int T = decltype(t)::value;
-                if (weighted) GV_LAUNCH((k_pull<T, true>), PULL_GRID, AN_THREADS, 0, s, d, a);
-                else GV_LAUNCH((k_pull<T, false>), PULL_GRID, AN_THREADS, 0, s, d, a);
+                if (weighted)
+                    GV_LAUNCH((k_pull_fused<T, true>), 3 * PULL_GRID, AN_THREADS, 0, s, d, a, it, ipart, PULL_GRID + FIN_GRID);
+                else
+                    GV_LAUNCH((k_pull_fused<T, false>), 3 * PULL_GRID, AN_THREADS, 0, s, d, a, it, ipart, PULL_GRID + FIN_GRID);
             });
-            if (weighted) GV_LAUNCH(k_pull_tiny<true>, TINY_GRID, AN_THREADS, 0, s, d, a, PULL_GRID + FIN_GRID);
-            else GV_LAUNCH(k_pull_tiny<false>, TINY_GRID, AN_THREADS, 0, s, d, a, PULL_GRID + FIN_GRID);
-            if (it.nitems) {
-                if (weighted) GV_LAUNCH(k_pull_items<true>, PULL_GRID, AN_THREADS, 0, s, d, a, it, ipart);
-                else GV_LAUNCH(k_pull_items<false>, PULL_GRID, AN_THREADS, 0, s, d, a, it, ipart);
+            if (it.nitems)
                 GV_LAUNCH(k_pull_items_fin, FIN_GRID, AN_THREADS, 0, s, d, a, it, (const float *)ipart, PULL_GRID);
-            }
             GV_LAUNCH(k_iter_done, 1, 256, 0, s, b.partial, nparts, eps, b.state, b.res);
             std::swap(xa, xb);
             std::swap(ca, cb);
