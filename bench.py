@@ -56,6 +56,7 @@ def parse():
     ap.add_argument("--no-batching", action="store_true", help="skip the scale-24 batched-vs-plain section")
     ap.add_argument("--batch-scale", type=int, default=24)
     ap.add_argument("--c3-batches", type=int, default=64)
+    ap.add_argument("--no-incremental", action="store_true", help="skip the incremental triangle-count section")
     ap.add_argument("--no-diff", action="store_true", help="skip the scale-20 differentiation section")
     ap.add_argument("--diff-scale", type=int, default=20)
     ap.add_argument("--fd-edges", type=int, default=64)
@@ -593,7 +594,8 @@ def run_gv(args, rank, world, local_rank):
     m0 = int(off[-1])
     half = args.batch // 2
     total_steps = args.warmup + args.steps + (0 if args.no_e2e else args.steps)
-    batches = make_batches(n, off, dst, total_steps, half, seed)
+    n_incr = 0 if (args.no_incremental or world > 1) else 4
+    batches = make_batches(n, off, dst, total_steps + n_incr, half, seed)
     srcs = bc_sources(n, args.bc_sources, seed)
     dev_batches = [tuple(torch.from_numpy(a.astype(np.int32)).to(dev) for a in b) for b in batches]
     x_dev = torch.empty(n, dtype=torch.float32, device=dev)
@@ -684,6 +686,31 @@ def run_gv(args, rank, world, local_rank):
         d2h = n * 4 + 8 + (n * 4 * n_bc) // max(1, len(pin))
         e2e = {"ms": e2e_ms, "h2d": h2d, "d2h": d2h}
 
+    # incremental triangle counts (single GPU): batches alternate between
+    # gv_update_tc (exact delta) and update + whole-graph count
+    incr = None
+    if n_incr:
+        incr = {"batch_updates": args.batch, "update_tc_ms": [], "update_then_static_tc_ms": [], "exact": True}
+        _, t_ref = g.static_tc(per_vertex=False)
+        for j in range(n_incr):
+            ins_s, ins_d, del_s, del_d = dev_batches[total_steps + j]
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            if j % 2 == 0:
+                dt, _ = g.update_tc(ins_s, ins_d, del_s, del_d, compact=True)
+                torch.cuda.synchronize()
+                incr["update_tc_ms"].append((time.perf_counter() - t0) * 1e3)
+                _, t_chk = g.static_tc(per_vertex=False)
+                incr["exact"] = incr["exact"] and (t_chk == t_ref + dt)
+                t_ref = t_chk
+            else:
+                g.batch_insert(ins_s, ins_d)
+                g.batch_delete(del_s, del_d)
+                g.compaction()
+                _, t_ref = g.static_tc(per_vertex=False)
+                torch.cuda.synchronize()
+                incr["update_then_static_tc_ms"].append((time.perf_counter() - t0) * 1e3)
+        incr["triangles_after"] = int(t_ref)
     # max over ranks
     t = torch.tensor([elapsed_ms, e2e["ms"] if e2e else 0.0], dtype=torch.float64, device=dev)
     if dist is not None:
@@ -734,6 +761,13 @@ def run_gv(args, rank, world, local_rank):
             "config": workload_config(args, n, m0),
             "pagerank_gteps": pr_gteps, "pagerank_sweeps_avg": avg_sweeps, "m_entries": m_now,
             "kernel_ms": phases, "roofline": roof, "gpu_launches": launches, "clocks": clocks}
+    if incr:
+        line["incremental_tc"] = {
+            "workload": ("same graph and batch size as the steps; gv_update_tc (inserts, deletes, compaction and "
+                         "the exact triangle delta) against insert + delete + compaction + whole-graph count"),
+            "update_tc_ms": statistics.mean(incr["update_tc_ms"]),
+            "update_then_static_tc_ms": statistics.mean(incr["update_then_static_tc_ms"]),
+            "exact": incr["exact"], "triangles_after": incr["triangles_after"]}
     if e2e:
         line["e2e"] = {"value": updates / (e2e_ms / 1e3), "unit": "edge updates/s",
                        "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"]}

@@ -356,6 +356,37 @@ class GraphVine:
                                 _stream(stream)), "gv_tc")
         return pv, tot.value
 
+    def update_tc(self, ins_src, ins_dst, del_src, del_dst, ins_weights=None, compact: bool = True,
+                  per_vertex: bool = False, stream=None):
+        """Applies inserts, then deletes (then compaction) and returns the exact
+        change of the triangle count, and per vertex of its owned triangles
+        when per_vertex=True: (delta_total, delta_owner or None)."""
+        pis, mem, k1 = _ptr(ins_src, np.uint32)
+        pid, _, k2 = _ptr(ins_dst, np.uint32)
+        pds, mem2, k3 = _ptr(del_src, np.uint32)
+        pdd, _, k4 = _ptr(del_dst, np.uint32)
+        pw, _, k5 = _ptr(ins_weights, np.float32)
+        if ins_src is None:
+            mem = mem2
+        elif del_src is not None and mem != mem2:
+            raise ValueError("inserts and deletes must live in the same kind of memory")
+        ni = len(ins_src) if ins_src is not None else 0
+        nd = len(del_src) if del_src is not None else 0
+        tot = C.c_int64()
+        owner = None
+        po = None
+        if per_vertex:
+            if mem == GV_MEM_DEVICE:
+                import torch
+                owner = torch.empty(self.n, dtype=torch.int64, device=ins_src.device)
+                po = owner.data_ptr()
+            else:
+                owner = np.empty(self.n, np.int64)
+                po = owner.ctypes.data
+        _check(_lib.lib().gv_update_tc(self._h, pis, pid, pw, ni, pds, pdd, nd, 1 if compact else 0, C.byref(tot),
+                                       po, mem, _stream(stream)), "gv_update_tc")
+        return tot.value, owner
+
     def tc_subset(self, subset, stream=None) -> np.ndarray:
         s = np.ascontiguousarray(subset, dtype=np.uint32)
         out = np.empty(len(s), np.uint64)

@@ -408,3 +408,437 @@ gv_status tc_local_subset(gv_graph *g, const uint32_t *d_sub, uint64_t ns, unsig
 }
 
 }  // namespace gv
+
+// ------------------------------------------------------- batch deltas
+// Exact change of the triangle counts across one batch (inserts, then
+// deletes, as gv_insert_edges / gv_delete_edges apply them).  With A the
+// inserted pairs that were not in the graph and R the deleted pairs that were
+// in it after the inserts, both counted on the graph between the two steps
+// (G_mid):
+//   created   = triangles of G_mid with at least one edge in A,
+//   destroyed = triangles of G_mid with at least one edge in R,
+//   T_after = T_before + created - destroyed.
+// A triangle is counted once, at its smallest changed edge (pairs ordered by
+// their canonical key min << bitsn | max): for a changed pair (a, b) and a
+// common neighbour w, (a, w) or (b, w) being a smaller changed pair skips it.
+// Work: sum over changed pairs of the shorter list (plus one table of each
+// heavy endpoint), against a whole-graph count.
+namespace gv {
+namespace {
+
+constexpr int TD_THREADS = 256;
+constexpr int TD_WARPS = TD_THREADS / 32;
+constexpr unsigned long long TD_NONE = ~0ull;
+
+__device__ __forceinline__ unsigned long long td_key(uint32_t a, uint32_t b, uint32_t bitsn) {
+    return a < b ? ((unsigned long long)a << bitsn) | b : ((unsigned long long)b << bitsn) | a;
+}
+
+__global__ void k_td_keys(const uint32_t *__restrict__ src, const uint32_t *__restrict__ dst, uint64_t k, uint32_t n,
+                          uint32_t bitsn, unsigned long long *__restrict__ keys, uint32_t *bad) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < k; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t a = src[i], b = dst[i];
+        if (a >= n || b >= n) {
+            atomicOr(bad, 1u);
+            keys[i] = TD_NONE;
+        } else {
+            keys[i] = a == b ? TD_NONE : td_key(a, b, bitsn);  // self-loops are never stored
+        }
+    }
+}
+
+// flag[i] = 1 for the first copy of each real key (keys sorted).
+__global__ void k_td_first(const unsigned long long *__restrict__ keys, uint64_t k, uint32_t *__restrict__ flag) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < k; i += (uint64_t)gridDim.x * blockDim.x)
+        flag[i] = keys[i] != TD_NONE && (i == 0 || keys[i - 1] != keys[i]);
+}
+
+__global__ void k_td_compact(const unsigned long long *__restrict__ keys, const uint32_t *__restrict__ flag,
+                             const uint32_t *__restrict__ pos, uint64_t k, unsigned long long *__restrict__ out) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < k; i += (uint64_t)gridDim.x * blockDim.x)
+        if (flag[i]) out[pos[i]] = keys[i];
+}
+
+// present[i] = pair i is in the graph: the warp scans the shorter list.
+__global__ void __launch_bounds__(TD_THREADS) k_td_member(DevGraph g, const unsigned long long *__restrict__ keys,
+                                                          uint32_t cnt, uint32_t bitsn, uint32_t *__restrict__ present) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const unsigned long long mask = (1ull << bitsn) - 1;
+    for (uint32_t i = blockIdx.x * TD_WARPS + (threadIdx.x >> 5); i < cnt; i += gridDim.x * TD_WARPS) {
+        const uint32_t a = (uint32_t)(keys[i] >> bitsn), b = (uint32_t)(keys[i] & mask);
+        const uint4 ra = g.vtx[a], rb = g.vtx[b];
+        const bool a_short = ra.y <= rb.y;
+        const uint4 rs = a_short ? ra : rb;
+        const uint32_t want = a_short ? b : a;
+        const uint32_t fill = rs.y, nb = blocks_for(fill, g.logB);
+        uint32_t hit = 0;
+        for (uint32_t kb = 0; kb < nb && !hit; kb += TL_PIECE_BLOCKS) {  // warp-uniform
+            const uint32_t blk = tl_lane_block(g, rs.x, kb, nb);
+            uint32_t mine = 0;
+            tl_scan_blocks(g, blk, kb, 0, min(TL_PIECE_BLOCKS, nb - kb), fill, [&](uint32_t w) { mine |= (w == want); });
+            hit = __any_sync(GV_FULL_MASK, mine);
+        }
+        if (lane == 0) present[i] = hit;
+    }
+}
+
+// keep[i] = present[i] == want (A: pairs not yet in the graph; R: pairs in it).
+__global__ void k_td_select(const uint32_t *__restrict__ present, uint32_t cnt, uint32_t want, uint32_t *__restrict__ keep) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x)
+        keep[i] = present[i] == want;
+}
+
+__device__ __forceinline__ uint32_t td_slot(unsigned long long key, uint32_t log) {
+    return (uint32_t)((key * 0x9E3779B97F4A7C15ull) >> (64 - log));
+}
+
+__global__ void k_td_set_build(const unsigned long long *__restrict__ keys, uint32_t cnt, unsigned long long *set,
+                               uint32_t log, uint32_t *err) {
+    const uint32_t mask = (1u << log) - 1u;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
+        uint32_t h = td_slot(keys[i], log);
+        uint32_t p = 0;
+        for (; p <= mask; ++p) {
+            const unsigned long long old = atomicCAS(set + h, TD_NONE, keys[i]);
+            if (old == TD_NONE || old == keys[i]) break;
+            h = (h + 1u) & mask;
+        }
+        if (p > mask) atomicOr(err, 4u);
+    }
+}
+
+__device__ __forceinline__ bool td_set_has(const unsigned long long *set, uint32_t log, unsigned long long key) {
+    const uint32_t mask = (1u << log) - 1u;
+    uint32_t h = td_slot(key, log);
+    for (uint32_t p = 0; p <= mask; ++p) {
+        const unsigned long long x = set[h];
+        if (x == key) return true;
+        if (x == TD_NONE) return false;
+        h = (h + 1u) & mask;
+    }
+    return false;
+}
+
+// Heavy endpoints (more than TD_LIGHT live entries) of the changed pairs get a
+// hash table of their whole list in global memory, built once per call, so
+// a pair costs its shorter list: the warp streams it against the longer
+// endpoint's table (its own shared table when that list is light too).
+constexpr uint32_t TD_LIGHT = 256;
+constexpr uint32_t TD_WLOG = 9;  // per-warp shared table: 512 slots
+
+__global__ void k_td_mark(DevGraph g, const unsigned long long *__restrict__ keys, uint32_t cnt, uint32_t bitsn,
+                          uint32_t *__restrict__ flag, uint32_t *__restrict__ hlist, uint32_t *nh) {
+    const unsigned long long mask = (1ull << bitsn) - 1;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
+        const uint32_t ends[2] = {(uint32_t)(keys[i] >> bitsn), (uint32_t)(keys[i] & mask)};
+        for (int e = 0; e < 2; ++e) {
+            const uint32_t v = ends[e];
+            if (g.vtx[v].z > TD_LIGHT && atomicCAS(flag + v, 0u, 1u) == 0u) hlist[atomicAdd(nh, 1u)] = v;
+        }
+    }
+}
+
+__global__ void k_td_caps(DevGraph g, const uint32_t *__restrict__ hlist, const uint32_t *nh,
+                          unsigned long long *__restrict__ cap, uint32_t *__restrict__ hlog, uint32_t *__restrict__ hidx) {
+    const uint32_t nhv = *nh;
+    for (uint32_t h = blockIdx.x * blockDim.x + threadIdx.x; h < nhv; h += gridDim.x * blockDim.x) {
+        const uint32_t v = hlist[h];
+        const uint32_t live = g.vtx[v].z;
+        uint32_t l = 10;
+        while ((1ull << l) < 2ull * live) ++l;
+        cap[h] = 1ull << l;
+        hlog[h] = l;
+        hidx[v] = h;
+    }
+}
+
+__global__ void __launch_bounds__(TD_THREADS) k_td_build(DevGraph g, const uint32_t *__restrict__ hlist, const uint32_t *nh,
+                                                         const unsigned long long *__restrict__ hoff,
+                                                         const uint32_t *__restrict__ hlog, uint32_t *gtab, uint32_t *err) {
+    const uint32_t nhv = *nh;
+    for (uint32_t h = blockIdx.x; h < nhv; h += gridDim.x) {
+        const uint32_t v = hlist[h];
+        const uint4 rec = g.vtx[v];
+        const uint32_t nb = blocks_for(rec.y, g.logB);
+        uint32_t *tab = gtab + hoff[h];
+        for (uint32_t kb = (threadIdx.x >> 5) * TL_PIECE_BLOCKS; kb < nb; kb += TD_WARPS * TL_PIECE_BLOCKS) {
+            const uint32_t blk = tl_lane_block(g, rec.x, kb, nb);
+            tl_scan_blocks(g, blk, kb, 0, min(TL_PIECE_BLOCKS, nb - kb), rec.y,
+                           [&](uint32_t w) { tl_insert(tab, hlog[h], w, err); });
+        }
+    }
+}
+
+// Triangles through each changed pair (a, b), counted at their smallest
+// changed edge.
+__global__ void __launch_bounds__(TD_THREADS) k_td_count(DevGraph g, const unsigned long long *__restrict__ keys,
+                                                         uint32_t cnt, uint32_t bitsn, const unsigned long long *set,
+                                                         uint32_t set_log, const uint32_t *__restrict__ hidx,
+                                                         const unsigned long long *__restrict__ hoff,
+                                                         const uint32_t *__restrict__ hlog, const uint32_t *gtab,
+                                                         unsigned long long *total, long long *__restrict__ owner,
+                                                         long long sign, uint32_t *err) {
+    __shared__ uint32_t wtab[TD_WARPS][1u << TD_WLOG];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const unsigned long long mask = (1ull << bitsn) - 1;
+    unsigned long long mine = 0;
+    for (uint32_t i = blockIdx.x * TD_WARPS + warp; i < cnt; i += gridDim.x * TD_WARPS) {
+        const unsigned long long ke = keys[i];
+        const uint32_t a = (uint32_t)(ke >> bitsn), b = (uint32_t)(ke & mask);
+        const uint4 ra = g.vtx[a], rb = g.vtx[b];
+        const bool a_long = ra.z >= rb.z;
+        const uint4 rl = a_long ? ra : rb, rs = a_long ? rb : ra;
+        const uint32_t l = a_long ? a : b;
+        const uint32_t *tab;
+        uint32_t tlog;
+        if (rl.z > TD_LIGHT) {  // warp-uniform
+            const uint32_t h = hidx[l];
+            tab = gtab + hoff[h];
+            tlog = hlog[h];
+        } else {
+            uint32_t *wt = wtab[warp];
+            for (uint32_t t = lane; t < (1u << TD_WLOG); t += 32) wt[t] = GV_NIL;
+            __syncwarp();
+            const uint32_t nbl = blocks_for(rl.y, g.logB);
+            for (uint32_t kb = 0; kb < nbl; kb += TL_PIECE_BLOCKS) {
+                const uint32_t blk = tl_lane_block(g, rl.x, kb, nbl);
+                tl_scan_blocks(g, blk, kb, 0, min(TL_PIECE_BLOCKS, nbl - kb), rl.y,
+                               [&](uint32_t w) { tl_insert(wt, TD_WLOG, w, err); });
+            }
+            __syncwarp();
+            tab = wt;
+            tlog = TD_WLOG;
+        }
+        const uint32_t nbs = blocks_for(rs.y, g.logB);
+        for (uint32_t kb = 0; kb < nbs; kb += TL_PIECE_BLOCKS) {
+            const uint32_t blk = tl_lane_block(g, rs.x, kb, nbs);
+            tl_scan_blocks(g, blk, kb, 0, min(TL_PIECE_BLOCKS, nbs - kb), rs.y, [&](uint32_t w) {
+                if (!tl_probe(tab, tlog, w)) return;
+                const unsigned long long k1 = td_key(a, w, bitsn), k2 = td_key(b, w, bitsn);
+                if (k1 < ke && td_set_has(set, set_log, k1)) return;
+                if (k2 < ke && td_set_has(set, set_log, k2)) return;
+                ++mine;
+                if (owner)  // two's complement: adding (u64)-1 subtracts one
+                    atomicAdd(reinterpret_cast<unsigned long long *>(owner) + min(w, min(a, b)),
+                              (unsigned long long)sign);
+            });
+        }
+        __syncwarp();
+    }
+    mine = warp_sum(mine);
+    if (lane == 0 && mine) atomicAdd(total, mine);
+}
+
+}  // namespace
+
+// Changed pairs of one side of the batch: canonical, deduplicated, and kept
+// when their presence in the graph now equals `want_present`.  Returns the
+// count; the keys sit in *out (scratch slot 4).
+static gv_status td_pairs(gv_graph *g, const uint32_t *dsrc, const uint32_t *ddst, uint64_t k, uint32_t want_present,
+                          unsigned long long **out, uint32_t *count, cudaStream_t s, bool ids_only = false) {
+    const uint32_t n = g->d.n, bitsn = g->bitsn;
+    *count = 0;
+    if (k == 0) return GV_OK;
+    const uint64_t rc = radix_counts_elems(k);
+    auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+    const size_t o_k1 = 0, o_k2 = o_k1 + al(k * 8), o_out = o_k2 + al(k * 8), o_f = o_out + al(k * 8);
+    const size_t o_p = o_f + al(k * 4), o_c = o_p + al((k + 1) * 4), o_t = o_c + al(rc * 4);
+    const size_t bytes = o_t + al(scan_scratch_bytes(std::max<uint64_t>(rc, k + 1))) + 256;
+    char *b = (char *)aux_scratch(g, 4, bytes);
+    if (!b) return GV_ERR_NOMEM;
+    unsigned long long *k1 = (unsigned long long *)(b + o_k1), *k2 = (unsigned long long *)(b + o_k2);
+    unsigned long long *outk = (unsigned long long *)(b + o_out);
+    uint32_t *flag = (uint32_t *)(b + o_f), *pos = (uint32_t *)(b + o_p), *cnts = (uint32_t *)(b + o_c);
+    void *tmp = b + o_t;
+    uint32_t *bad = flag;  // checked before the flags are written
+    cudaMemsetAsync(bad, 0, 4, s);
+    GV_LAUNCH(k_td_keys, grid_for(k, 256, 148 * 16), 256, 0, s, dsrc, ddst, k, n, bitsn, k1, bad);
+    uint32_t hbad = 0;
+    cudaError_t e = cudaMemcpyAsync(&hbad, bad, 4, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_status(e, "tc delta keys");
+    if (hbad) {
+        set_error("vertex id out of range");
+        return GV_ERR_INVALID;
+    }
+    if (ids_only) return GV_OK;
+    const int which = radix_sort_u64(k1, k2, nullptr, nullptr, k, 2 * (int)bitsn, cnts, tmp, s);
+    const unsigned long long *sk = which ? k2 : k1;
+    GV_LAUNCH(k_td_first, grid_for(k, 256, 148 * 16), 256, 0, s, sk, k, flag);
+    scan_exclusive_u32(flag, pos, k, pos + k, tmp, s);
+    GV_LAUNCH(k_td_compact, grid_for(k, 256, 148 * 16), 256, 0, s, sk, (const uint32_t *)flag, (const uint32_t *)pos, k,
+              outk);
+    uint32_t nu = 0;
+    e = cudaMemcpyAsync(&nu, pos + k, 4, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_status(e, "tc delta unique");
+    if (nu == 0) return GV_OK;
+    // presence in the graph as it is now, then keep the wanted side
+    uint32_t *present = flag;  // reuse (nu <= k)
+    GV_LAUNCH(k_td_member, grid_for(nu, TD_WARPS, 148 * 8), TD_THREADS, 0, s, g->d, (const unsigned long long *)outk, nu,
+              bitsn, present);
+    GV_LAUNCH(k_td_select, grid_for(nu, 256), 256, 0, s, (const uint32_t *)present, nu, want_present, present);
+    scan_exclusive_u32(present, pos, nu, pos + nu, tmp, s);
+    GV_LAUNCH(k_td_compact, grid_for(nu, 256), 256, 0, s, (const unsigned long long *)outk, (const uint32_t *)present,
+              (const uint32_t *)pos, nu, k1);  // k1 is free again
+    e = cudaMemcpyAsync(count, pos + nu, 4, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_status(e, "tc delta select");
+    *out = k1;
+    return GV_OK;
+}
+
+// Counts the triangles of the current graph through the `cnt` changed pairs.
+static gv_status td_count(gv_graph *g, const unsigned long long *pairs, uint32_t cnt, unsigned long long *total,
+                          long long *owner, long long sign, uint32_t *err, cudaStream_t s) {
+    if (cnt == 0) return GV_OK;
+    const uint32_t n = g->d.n;
+    uint32_t log = 10;
+    while ((1ull << log) < 2ull * cnt) ++log;
+    unsigned long long *set = (unsigned long long *)aux_scratch(g, 5, (8ull << log) + 256);
+    if (!set) return GV_ERR_NOMEM;
+    cudaMemsetAsync(set, 0xFF, 8ull << log, s);
+    GV_LAUNCH(k_td_set_build, grid_for(cnt, 256), 256, 0, s, pairs, cnt, set, log, err);
+    // heavy endpoints: flag, list, table sizes and offsets (slot 8), tables (slot 9)
+    auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+    const size_t o_flag = 0, o_list = al((size_t)n * 4), o_hidx = o_list + al((size_t)n * 4);
+    const size_t o_log = o_hidx + al((size_t)n * 4), o_cap = o_log + al((size_t)n * 4);
+    const size_t o_off = o_cap + al(((size_t)n + 1) * 8), o_tmp = o_off + al(((size_t)n + 1) * 8);
+    const size_t bytes = o_tmp + al(scan_scratch_bytes((uint64_t)n + 1)) + 256;
+    char *b8 = (char *)aux_scratch(g, 8, bytes);
+    if (!b8) return GV_ERR_NOMEM;
+    uint32_t *flag = (uint32_t *)(b8 + o_flag), *hlist = (uint32_t *)(b8 + o_list);
+    uint32_t *hidx = (uint32_t *)(b8 + o_hidx), *hlog = (uint32_t *)(b8 + o_log);
+    unsigned long long *cap = (unsigned long long *)(b8 + o_cap), *hoff = (unsigned long long *)(b8 + o_off);
+    uint32_t *nh = reinterpret_cast<uint32_t *>(hoff + n);  // scratch word until the scan writes the offsets
+    cudaMemsetAsync(flag, 0, (size_t)n * 4, s);
+    cudaMemsetAsync(nh, 0, 4, s);
+    GV_LAUNCH(k_td_mark, grid_for(cnt, 256), 256, 0, s, g->d, pairs, cnt, g->bitsn, flag, hlist, nh);
+    uint32_t hn = 0;
+    cudaError_t e = cudaMemcpyAsync(&hn, nh, 4, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_status(e, "tc delta heavy");
+    uint32_t *dn = flag;  // the count, in a word the scan does not touch
+    cudaMemcpyAsync(dn, nh, 4, cudaMemcpyDeviceToDevice, s);
+    uint32_t *gtab = nullptr;
+    if (hn) {
+        GV_LAUNCH(k_td_caps, grid_for(hn, 256), 256, 0, s, g->d, (const uint32_t *)hlist, (const uint32_t *)dn, cap,
+                  hlog, hidx);
+        scan_exclusive_u64(cap, hoff, hn, hoff + hn, b8 + o_tmp, s);
+        unsigned long long slots = 0;
+        e = cudaMemcpyAsync(&slots, hoff + hn, 8, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return cuda_status(e, "tc delta tables");
+        gtab = (uint32_t *)aux_scratch(g, 9, slots * 4 + 256);
+        if (!gtab) return GV_ERR_NOMEM;
+        cudaMemsetAsync(gtab, 0xFF, slots * 4, s);
+        GV_LAUNCH(k_td_build, std::min<uint32_t>(hn, 148 * 8), TD_THREADS, 0, s, g->d, (const uint32_t *)hlist,
+                  (const uint32_t *)dn, (const unsigned long long *)hoff, (const uint32_t *)hlog, gtab, err);
+    }
+    GV_LAUNCH(k_td_count, grid_for(cnt, TD_WARPS, 148 * 8), TD_THREADS, 0, s, g->d, pairs, cnt, g->bitsn,
+              (const unsigned long long *)set, log, (const uint32_t *)hidx, (const unsigned long long *)hoff,
+              (const uint32_t *)hlog, (const uint32_t *)gtab, total, owner, sign, err);
+    return cuda_status(cudaGetLastError(), "tc delta count");
+}
+
+}  // namespace gv
+
+using namespace gv;
+
+extern "C" gv_status gv_update_tc(gv_graph *g, const uint32_t *ins_src, const uint32_t *ins_dst, const float *ins_w,
+                                  uint64_t n_ins, const uint32_t *del_src, const uint32_t *del_dst, uint64_t n_del,
+                                  uint32_t flags, int64_t *delta_total, int64_t *delta_owner, int mem, void *stream) {
+    if (!g || !delta_total || (n_ins && (!ins_src || !ins_dst)) || (n_del && (!del_src || !del_dst))) {
+        set_error("null argument");
+        return GV_ERR_INVALID;
+    }
+    if (g->parent) { set_error("a view is read-only"); return GV_ERR_STATE; }
+    if (g->cfg.directed) { set_error("triangle counting needs an undirected store"); return GV_ERR_STATE; }
+    if (mem != GV_MEM_HOST && mem != GV_MEM_DEVICE) { set_error("bad mem flag"); return GV_ERR_INVALID; }
+    cudaSetDevice(g->cfg.device);
+    cudaStream_t s = (cudaStream_t)stream;
+    const uint32_t n = g->d.n;
+    // device copies of the pairs (slot 6 is free outside betweenness)
+    const uint64_t tot_pairs = n_ins + n_del;
+    const bool weighted = g->cfg.weighted && ins_w;
+    if (g->cfg.weighted && n_ins && !ins_w) { set_error("weighted store needs weights"); return GV_ERR_INVALID; }
+    uint32_t *dp = nullptr;
+    const float *iw = ins_w;
+    if (mem == GV_MEM_HOST && tot_pairs) {
+        dp = (uint32_t *)aux_scratch(g, 6, tot_pairs * 8 + (weighted ? n_ins * 4 : 0) + 256);
+        if (!dp) return GV_ERR_NOMEM;
+        cudaError_t e = cudaSuccess;
+        if (weighted) {
+            float *dw = (float *)(dp + 2 * tot_pairs);
+            e = cudaMemcpyAsync(dw, ins_w, n_ins * 4, cudaMemcpyHostToDevice, s);
+            iw = dw;
+        }
+        if (n_ins) e = cudaMemcpyAsync(dp, ins_src, n_ins * 4, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess && n_ins) e = cudaMemcpyAsync(dp + n_ins, ins_dst, n_ins * 4, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess && n_del) e = cudaMemcpyAsync(dp + 2 * n_ins, del_src, n_del * 4, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess && n_del)
+            e = cudaMemcpyAsync(dp + 2 * n_ins + n_del, del_dst, n_del * 4, cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess) return cuda_status(e, "tc delta input");
+    }
+    const uint32_t *is = mem == GV_MEM_HOST ? dp : ins_src, *id = mem == GV_MEM_HOST ? dp + n_ins : ins_dst;
+    const uint32_t *ds = mem == GV_MEM_HOST ? dp + 2 * n_ins : del_src;
+    const uint32_t *dd = mem == GV_MEM_HOST ? dp + 2 * n_ins + n_del : del_dst;
+    // words: [0] created, [1] destroyed, [2] error flags
+    unsigned long long *words = (unsigned long long *)aux_scratch(g, 3, 64);
+    if (!words) return GV_ERR_NOMEM;
+    cudaMemsetAsync(words, 0, 24, s);
+    uint32_t *err = (uint32_t *)(words + 2);
+    long long *owner = nullptr;
+    if (delta_owner) {
+        owner = (long long *)(mem == GV_MEM_DEVICE ? (void *)delta_owner : aux_scratch(g, 7, (size_t)n * 8));
+        if (!owner) return GV_ERR_NOMEM;
+        cudaMemsetAsync(owner, 0, (size_t)n * 8, s);
+    }
+    // inserts: the new pairs A (absent now), applied, then the triangles through A
+    unsigned long long *pairs = nullptr;
+    uint32_t cnt = 0;
+    gv_status st = GV_OK;
+    // delete ids are checked before anything changes, so a bad id rejects the whole call
+    if (n_del) {
+        unsigned long long *unused = nullptr;
+        uint32_t unused_cnt = 0;
+        st = td_pairs(g, ds, dd, n_del, 1u, &unused, &unused_cnt, s, true);
+        if (st != GV_OK) return st;
+    }
+    st = td_pairs(g, is, id, n_ins, 0u, &pairs, &cnt, s);
+    if (st != GV_OK) return st;
+    if (n_ins) {
+        st = gv_insert_edges(g, is, id, iw, n_ins, GV_MEM_DEVICE, stream);
+        if (st == GV_OK) st = gv_synchronize(g, stream);
+        if (st != GV_OK) return st;
+    }
+    st = td_count(g, pairs, cnt, words + 0, owner, 1, err, s);
+    if (st != GV_OK) return st;
+    // deletes: the pairs present now R, the triangles through R, then applied
+    if (n_del) {
+        st = td_pairs(g, ds, dd, n_del, 1u, &pairs, &cnt, s);
+        if (st != GV_OK) return st;
+        st = td_count(g, pairs, cnt, words + 1, owner, -1, err, s);
+        if (st != GV_OK) return st;
+        st = gv_delete_edges(g, ds, dd, n_del, GV_MEM_DEVICE, stream);
+        if (st == GV_OK) st = gv_synchronize(g, stream);
+        if (st != GV_OK) return st;
+    }
+    if (flags & 1u) {
+        st = gv_compact(g, stream);
+        if (st == GV_OK) st = gv_synchronize(g, stream);
+        if (st != GV_OK) return st;
+    }
+    unsigned long long h[3] = {0, 0, 0};
+    cudaError_t e = cudaMemcpyAsync(h, words, 24, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && delta_owner && mem == GV_MEM_HOST)
+        e = cudaMemcpyAsync(delta_owner, owner, (size_t)n * 8, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_status(e, "tc delta out");
+    if ((uint32_t)h[2]) {
+        set_error("tc delta: a neighbour table overflowed (live counts and stored entries disagree)");
+        return GV_ERR_STATE;
+    }
+    *delta_total = (int64_t)h[0] - (int64_t)h[1];
+    return GV_OK;
+}

@@ -127,6 +127,21 @@ gv_status gv_degrees(gv_graph *g, uint32_t *deg, int mem, void *stream);
 gv_status gv_export_csr(gv_graph *g, uint64_t *offsets, uint32_t *dst, float *weights,
                         uint64_t cap, int mem, void *stream);
 
+/* Applies one batch as gv_insert_edges, gv_delete_edges and (flags &
+ * GV_UPDATE_COMPACT) gv_compact would, and returns the exact change of the
+ * triangle counts it causes: *delta_total, and optionally delta_owner[n], the
+ * change of the triangles each vertex owns (smallest id, as gv_tc counts
+ * them).  Work is proportional to the degrees of the pairs that really
+ * changed, not to the graph.  Undirected stores; the whole call is rejected
+ * (graph unchanged) on an id >= n.  Replaces dynamic_tc
+ * (src/algorithm/tc/tc.cu:29-64, tc_kernel.cu:76-147), which recounts only
+ * the owned triangles of vertices touched by the batch and so misses
+ * triangles whose owner was not touched.  Synchronous. */
+#define GV_UPDATE_COMPACT 1u
+gv_status gv_update_tc(gv_graph *g, const uint32_t *ins_src, const uint32_t *ins_dst, const float *ins_w,
+                       uint64_t n_ins, const uint32_t *del_src, const uint32_t *del_dst, uint64_t n_del,
+                       uint32_t flags, int64_t *delta_total, int64_t *delta_owner, int mem, void *stream);
+
 /* Vertices touched by updates since the last gv_clear_affected (endpoints of
  * every inserted or deleted entry, duplicates included).  affected[n] uint8.
  * Replaces find_affected_nodes (src/dynamicStructure/kernels/insert_kernels.cu:182-198)

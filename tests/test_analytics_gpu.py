@@ -12,7 +12,7 @@ import numpy as np
 import pytest
 
 import oracle
-from tests.helpers import make_graph, rmat_graph, sample_existing
+from tests.helpers import assert_same_adjacency, make_graph, rmat_graph, sample_existing
 
 gv_b200 = pytest.importorskip("gv_b200")
 pytestmark = pytest.mark.gpu
@@ -282,3 +282,58 @@ def test_wpr_forward_hub_in_edges_and_repeatable():
     xo, _ = o.wpr_forward(0.85)
     assert np.abs(x1 - xo).sum() < PR_L1
     assert np.array_equal(x1, x2)
+
+
+def _mixed_batch(g, n, rng, n_new=3000, n_del=2000):
+    """Inserts: new uniform pairs, duplicates, self-loops, pairs already in the
+    graph; deletes: existing pairs, some of this batch's inserts, absent pairs."""
+    off, dst, _ = g.export_csr()
+    ins_s, ins_d = gv_b200.gen_uniform(n, n_new, seed=int(rng.integers(1 << 30)))
+    es, ed = sample_existing(off, dst, 300, rng)
+    loops = rng.integers(0, n, 40).astype(np.uint32)
+    ins_s = np.concatenate([ins_s, ins_s[:100], es, loops])
+    ins_d = np.concatenate([ins_d, ins_d[:100], ed, loops])
+    ds, dd = sample_existing(off, dst, n_del, rng)
+    absent_s, absent_d = gv_b200.gen_uniform(n, 100, seed=int(rng.integers(1 << 30)))
+    del_s = np.concatenate([ds, ins_d[:150], absent_s, dd[:50]])
+    del_d = np.concatenate([dd, ins_s[:150], absent_d, ds[:50]])
+    return ins_s.astype(np.uint32), ins_d.astype(np.uint32), del_s.astype(np.uint32), del_d.astype(np.uint32)
+
+
+@pytest.mark.parametrize("block,scale,ef", [(128, 12, 16), (32, 14, 8)])
+def test_update_tc_deltas_are_exact(block, scale, ef):
+    """gv_update_tc's total and per-vertex deltas equal the difference of two
+    whole-graph counts, batch after batch, and the graph ends as the oracle's."""
+    n = 1 << scale
+    s, d = rmat_graph(scale, ef, seed=17)
+    g = make_graph(n, block_size=block)
+    g.batch_insert(s, d)
+    o = oracle.OracleGraph(n)
+    o.insert(s, d)
+    rng = np.random.default_rng(23)
+    pv0, t0 = g.static_tc()
+    for _ in range(3):
+        ins_s, ins_d, del_s, del_d = _mixed_batch(g, n, rng)
+        dt, dpv = g.update_tc(ins_s, ins_d, del_s, del_d, per_vertex=True)
+        o.insert(ins_s, ins_d)
+        o.delete(del_s, del_d)
+        pv1, t1 = g.static_tc()
+        assert t1 == t0 + dt
+        assert np.array_equal(pv1.astype(np.int64), pv0.astype(np.int64) + dpv)
+        pv0, t0 = pv1, t1
+    opv, otot = o.tc()
+    assert otot == t0 and np.array_equal(opv, pv0)
+    assert_same_adjacency(g, o)
+
+
+def test_update_tc_rejects_bad_ids_and_keeps_graph():
+    n = 1 << 10
+    s, d = rmat_graph(10, 8, seed=3)
+    g = make_graph(n)
+    g.batch_insert(s, d)
+    before = g.export_csr()
+    with pytest.raises(gv_b200.GvError):
+        g.update_tc(np.array([1, 2], np.uint32), np.array([3, 4], np.uint32),
+                    np.array([5, n + 7], np.uint32), np.array([6, 1], np.uint32))
+    after = g.export_csr()
+    assert np.array_equal(before[0], after[0])
