@@ -16,7 +16,7 @@ import numpy as np
 from . import _lib
 from ._lib import GV_MEM_DEVICE, GV_MEM_HOST, GV_OK, STATUS_NAMES, gv_config
 
-__all__ = ["GraphVine", "GvError", "gen_rmat", "gen_uniform", "kernel_launches", "version"]
+__all__ = ["GraphVine", "GvError", "gen_rmat", "gen_uniform", "kernel_launches", "mtx_parse", "version"]
 
 
 class GvError(RuntimeError):
@@ -148,6 +148,37 @@ def autotune(num_vertices: int, src0, dst0, batches, *, device: int = 0, hbm_bud
     return {"block_size": best.block_size, "threads_per_vertex": best.threads_per_vertex}, results
 
 
+def mtx_parse(text, with_values: bool = False):
+    """Parses Matrix-Market coordinate text (bytes, or a torch CUDA uint8
+    tensor) on the device: (info dict, src, dst, values or None), 0-based."""
+    L = _lib.lib()
+    info = _lib.gv_mtx_info()
+    cnt = C.c_uint64()
+    if _is_torch_cuda(text):
+        import torch
+        ptr, mem, n = text.data_ptr(), GV_MEM_DEVICE, text.numel()
+    else:
+        buf = np.frombuffer(bytes(text), dtype=np.uint8)
+        ptr, mem, n = buf.ctypes.data, GV_MEM_HOST, len(buf)
+    _check(L.gv_mtx_parse(ptr, n, mem, C.byref(info), None, None, None, 0, C.byref(cnt), None), "gv_mtx_parse")
+    cap = int(info.entries) + 16
+    if mem == GV_MEM_DEVICE:
+        import torch
+        src = torch.empty(cap, dtype=torch.int32, device=text.device)
+        dst = torch.empty(cap, dtype=torch.int32, device=text.device)
+        val = torch.empty(cap, dtype=torch.float32, device=text.device) if with_values else None
+        ps, pd, pv = src.data_ptr(), dst.data_ptr(), (val.data_ptr() if val is not None else None)
+    else:
+        src, dst = np.empty(cap, np.uint32), np.empty(cap, np.uint32)
+        val = np.empty(cap, np.float32) if with_values else None
+        ps, pd, pv = src.ctypes.data, dst.ctypes.data, (val.ctypes.data if val is not None else None)
+    _check(L.gv_mtx_parse(ptr, n, mem, C.byref(info), ps, pd, pv, cap, C.byref(cnt), None), "gv_mtx_parse")
+    k = cnt.value
+    meta = {"rows": info.rows, "cols": info.cols, "entries": info.entries, "pattern": bool(info.pattern),
+            "symmetric": bool(info.symmetric)}
+    return meta, src[:k], dst[:k], (val[:k] if val is not None else None)
+
+
 class GraphVine:
     """A dynamic graph resident on one GPU (edge-block CBT store)."""
 
@@ -194,6 +225,44 @@ class GraphVine:
     @property
     def handle(self) -> int:
         return self._h.value
+
+    @classmethod
+    def _wrap(cls, h: C.c_void_p) -> "GraphVine":
+        cfg = gv_config()
+        _check(_lib.lib().gv_get_config(h, C.byref(cfg)), "gv_get_config")
+        g = cls.__new__(cls)
+        g._h, g.n, g.weighted, g.directed, g.device = h, cfg.num_vertices, bool(cfg.weighted), bool(cfg.directed), cfg.device
+        return g
+
+    @classmethod
+    def from_mtx(cls, path: str, *, weighted: bool = False, directed: bool = False, hbm_budget_bytes: int = 0,
+                 block_size: int = 128) -> "GraphVine":
+        """Builds a graph from a Matrix-Market file parsed on the device."""
+        L = _lib.lib()
+        cfg = gv_config()
+        _check(L.gv_config_init(C.byref(cfg), 1), "gv_config_init")
+        cfg.weighted, cfg.directed, cfg.hbm_budget_bytes, cfg.block_size = int(weighted), int(directed), \
+            hbm_budget_bytes, block_size
+        h = C.c_void_p()
+        _check(L.gv_graph_from_mtx(str(path).encode(), C.byref(cfg), C.byref(h)), "gv_graph_from_mtx")
+        return cls._wrap(h)
+
+    @classmethod
+    def snapshot_load(cls, path: str, *, hbm_budget_bytes: int = 0) -> "GraphVine":
+        """A new graph from a snapshot written by snapshot_save."""
+        L = _lib.lib()
+        h = C.c_void_p()
+        if hbm_budget_bytes:
+            cfg = gv_config()
+            _check(L.gv_config_init(C.byref(cfg), 1), "gv_config_init")
+            cfg.hbm_budget_bytes = hbm_budget_bytes
+            _check(L.gv_snapshot_load(str(path).encode(), C.byref(cfg), C.byref(h)), "gv_snapshot_load")
+        else:
+            _check(L.gv_snapshot_load(str(path).encode(), None, C.byref(h)), "gv_snapshot_load")
+        return cls._wrap(h)
+
+    def snapshot_save(self, path: str) -> None:
+        _check(_lib.lib().gv_snapshot_save(self._h, str(path).encode()), "gv_snapshot_save")
 
     def view(self) -> "GraphVine":
         """A read-only view: shares this graph's store and owns its analytics

@@ -44,6 +44,11 @@ GV_BATCH_COMPACT, GV_BATCH_GRAPH = 1, 2
 GV_REQ_UPDATE, GV_REQ_PPR, GV_REQ_TC, GV_REQ_BC = range(4)
 
 
+class gv_mtx_info(C.Structure):
+    _fields_ = [("rows", C.c_uint64), ("cols", C.c_uint64), ("entries", C.c_uint64), ("pattern", C.c_uint32),
+                ("symmetric", C.c_uint32)]
+
+
 class gv_request(C.Structure):
     _fields_ = [("kind", C.c_uint32), ("count0", C.c_uint32), ("count1", C.c_uint32), ("source", C.c_uint32),
                 ("offset", C.c_uint64), ("arrival_s", C.c_double)]
@@ -112,6 +117,10 @@ SIGNATURES = {
     "gv_serve_config_init": (C.c_int, [C.POINTER(gv_serve_config)]),
     "gv_serve_trace": (C.c_int, [P, C.POINTER(gv_serve_config), C.POINTER(gv_request), u32, P, P, P,
                                  C.POINTER(gv_request_result), C.POINTER(gv_serve_outputs)]),
+    "gv_mtx_parse": (C.c_int, [C.c_void_p, u64, C.c_int, C.POINTER(gv_mtx_info), P, P, P, u64, pu64, P]),
+    "gv_graph_from_mtx": (C.c_int, [C.c_char_p, C.POINTER(gv_config), C.POINTER(P)]),
+    "gv_snapshot_save": (C.c_int, [P, C.c_char_p]),
+    "gv_snapshot_load": (C.c_int, [C.c_char_p, C.POINTER(gv_config), C.POINTER(P)]),
     "gv_gen_rmat": (C.c_int, [u32, u64, u64, u64, P, P, C.c_int, P]),
     "gv_gen_uniform": (C.c_int, [u32, u64, u64, P, P, C.c_int, P]),
 }

@@ -78,3 +78,17 @@ def test_serve_config_defaults_and_null_graph():
     reqs = (_lib.gv_request * 1)()
     assert L.gv_serve_trace(None, C.byref(cfg), reqs, 1, None, None, None, res, None) == _lib.GV_ERR_INVALID
     assert L.gv_view_create(None, None) == _lib.GV_ERR_INVALID
+
+
+def test_mtx_header_parse_without_gpu():
+    from gv_b200 import _lib
+    L = _lib.lib()
+    info = _lib.gv_mtx_info()
+    cnt = C.c_uint64()
+    text = b"%%MatrixMarket matrix coordinate pattern symmetric\n% a comment\n\n 5 6 3\n1 2\n2 3\n3 1\n"
+    buf = C.create_string_buffer(text, len(text))
+    assert L.gv_mtx_parse(buf, len(text), 0, C.byref(info), None, None, None, 0, C.byref(cnt), None) == 0
+    assert (info.rows, info.cols, info.entries, info.pattern, info.symmetric) == (5, 6, 3, 1, 1)
+    bad = b"%%MatrixMarket matrix coordinate real general\nnot a size line\n"
+    buf = C.create_string_buffer(bad, len(bad))
+    assert L.gv_mtx_parse(buf, len(bad), 0, C.byref(info), None, None, None, 0, C.byref(cnt), None) == _lib.GV_ERR_INVALID
