@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--batch-scale", type=int, default=24)
     ap.add_argument("--c3-batches", type=int, default=64)
     ap.add_argument("--no-incremental", action="store_true", help="skip the incremental triangle-count section")
+    ap.add_argument("--no-ingest", action="store_true", help="skip the Matrix-Market / snapshot section")
+    ap.add_argument("--ingest-scale", type=int, default=20)
     ap.add_argument("--no-diff", action="store_true", help="skip the scale-20 differentiation section")
     ap.add_argument("--diff-scale", type=int, default=20)
     ap.add_argument("--fd-edges", type=int, default=64)
@@ -420,6 +422,63 @@ def run_differentiation(args):
                          "oracle_seconds": fd_s}}
 
 
+def run_ingest(args):
+    """Ingest workload: R-MAT scale args.ingest_scale written as Matrix-Market
+    text (1-based \"src dst\" lines), parsed on the device from host memory
+    (copy included) and from device memory; then a snapshot of the built graph
+    saved and loaded back."""
+    import tempfile
+    import torch
+    import gv_b200
+    scale = args.ingest_scale
+    n = 1 << scale
+    s, d = gv_b200.gen_rmat(scale, args.edge_factor << scale, args.seed + 400)
+    # fixed-width, zero-padded ids (valid decimal), built as a byte matrix
+    width = len(str(n))
+    rows = np.empty((len(s), 2 * width + 2), np.uint8)
+    for col, ids in ((0, s.astype(np.int64) + 1), (width + 1, d.astype(np.int64) + 1)):
+        for j in range(width):
+            rows[:, col + width - 1 - j] = ord("0") + (ids // 10 ** j) % 10
+    rows[:, width] = ord(" ")
+    rows[:, -1] = ord("\n")
+    text = f"%%MatrixMarket matrix coordinate pattern general\n{n} {n} {len(s)}\n".encode() + rows.tobytes()
+    del rows
+    host = torch.frombuffer(bytearray(text), dtype=torch.uint8).pin_memory()
+    dev = host.cuda()
+    gv_b200.mtx_parse(dev)  # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    meta, src, dst, _ = gv_b200.mtx_parse(dev)
+    torch.cuda.synchronize()
+    dev_s = time.perf_counter() - t0
+    ok = bool(np.array_equal(src[:1000].cpu().numpy().view(np.uint32), s[:1000]))
+    t0 = time.perf_counter()
+    gv_b200.mtx_parse(host.numpy().tobytes())
+    host_s = time.perf_counter() - t0
+    out = {"workload": f"R-MAT scale {scale} ef {args.edge_factor} as Matrix-Market text",
+           "text_bytes": len(text), "entries": int(meta["entries"]), "first_entries_match": ok,
+           "device_text_gb_s": len(text) / dev_s / 1e9, "device_text_entries_per_s": meta["entries"] / dev_s,
+           "host_text_gb_s": len(text) / host_s / 1e9,
+           "host_note": "host text: pageable copy, host header read, device parse and copy back of the ids"}
+    with tempfile.TemporaryDirectory() as td:
+        g = gv_b200.GraphVine(n, max_batch_pairs=len(s))
+        g.batch_insert(s, d)
+        g.synchronize()
+        path = f"{td}/g.snap"
+        t0 = time.perf_counter()
+        g.snapshot_save(path)
+        save_s = time.perf_counter() - t0
+        m = g.num_edges()
+        g.close()
+        t0 = time.perf_counter()
+        h = gv_b200.GraphVine.snapshot_load(path)
+        load_s = time.perf_counter() - t0
+        same = h.num_edges() == m
+        h.close()
+    out.update({"snapshot_entries": m, "snapshot_save_s": save_s, "snapshot_load_s": load_s, "snapshot_same_m": same})
+    return out
+
+
 def make_serve_trace(n, s_dev, d_dev, nreq, seed):
     """Serving requests: 60% update batches (log-uniform 1K-1M updates, half
     inserts of uniform-random pairs, half deletes sampled from the graph's
@@ -773,6 +832,8 @@ def run_gv(args, rank, world, local_rank):
                        "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"]}
     if world == 1 and not args.no_batching:
         line["batching"] = run_batching(args, torch.device("cuda", local_rank))
+    if world == 1 and not args.no_ingest:
+        line["ingest"] = run_ingest(args)
     if world == 1 and not args.no_diff:
         line["differentiation"] = run_differentiation(args)
     if world == 1 and not args.no_serving:
