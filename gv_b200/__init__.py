@@ -301,6 +301,20 @@ class GraphVine:
     def compaction(self, stream=None) -> None:
         _check(_lib.lib().gv_compact(self._h, _stream(stream)), "gv_compact")
 
+    def add_vertices(self, k: int, stream=None) -> int:
+        """Adds k isolated vertices; returns the first new id."""
+        first = C.c_uint32()
+        _check(_lib.lib().gv_add_vertices(self._h, k, C.byref(first), _stream(stream)), "gv_add_vertices")
+        self.n += k
+        return first.value
+
+    def delete_vertices(self, ids, compact: bool = True, stream=None) -> None:
+        """Removes every edge incident to the given vertices (ids stay valid)."""
+        pi, mem, keep = _ptr(ids, np.uint32)
+        k = len(ids)
+        _check(_lib.lib().gv_delete_vertices(self._h, pi, k, 1 if compact else 0, mem, _stream(stream)),
+               "gv_delete_vertices")
+
     def synchronize(self, stream=None) -> None:
         _check(_lib.lib().gv_synchronize(self._h, _stream(stream)), "gv_synchronize")
 

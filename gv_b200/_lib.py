@@ -82,6 +82,8 @@ SIGNATURES = {
     "gv_insert_edges": (C.c_int, [P, P, P, P, u64, C.c_int, P]),
     "gv_delete_edges": (C.c_int, [P, P, P, u64, C.c_int, P]),
     "gv_compact": (C.c_int, [P, P]),
+    "gv_add_vertices": (C.c_int, [P, u32, pu32, P]),
+    "gv_delete_vertices": (C.c_int, [P, P, u64, u32, C.c_int, P]),
     "gv_synchronize": (C.c_int, [P, P]),
     "gv_num_vertices": (C.c_int, [P, pu32]),
     "gv_num_edges": (C.c_int, [P, pu64]),

@@ -459,10 +459,19 @@ gv_status copy_out_f32(const float *src, float *dst, uint32_t n, int mem, cudaSt
     return cuda_status(e, "copy out");
 }
 
+gv_status transpose_pagerank(gv_graph *g, float alpha, float tol, int32_t max_iter, bool unit, const float *x_init,
+                             int init_mem, uint32_t source, float *x_out, int32_t *sweeps, int mem, cudaStream_t s);
+
 gv_status pagerank_impl(gv_graph *g, float alpha, float eps, int max_iter, const float *x_init, int init_mem,
                         uint32_t source, float *x_out, int32_t *sweeps, int mem, cudaStream_t s) {
     const uint32_t n = g->d.n;
-    if (g->cfg.directed) { set_error("PageRank pull needs an undirected (symmetric) store"); return GV_ERR_STATE; }
+    if (g->cfg.directed) {  // pull over the in-edges: the sorted transpose, unit weights
+        int32_t sw = 0;
+        gv_status st = transpose_pagerank(g, alpha, eps, max_iter, true, x_init, init_mem, source, x_out, &sw, mem, s);
+        g->last_sweeps = sw;
+        if (sweeps) *sweeps = sw;
+        return st;
+    }
     const uint32_t parts = SWEEP_PARTS;
     void *buf = analytics_scratch(g, iter_bytes(n, parts));
     if (!buf) return GV_ERR_NOMEM;
@@ -1415,6 +1424,13 @@ gv_status tc_run(gv_graph *g, cudaStream_t s, int mode, unsigned long long **tco
 }
 
 // ------------------------------------------------------- weighted PageRank
+__global__ void k_row_inv_deg(DevGraph g, float *__restrict__ rinv) {
+    for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < g.n; u += gridDim.x * blockDim.x) {
+        const uint32_t dl = g.vtx[u].z;
+        rinv[u] = dl ? 1.0f / (float)dl : 0.f;
+    }
+}
+
 __global__ void k_row_sums(DevGraph g, float *__restrict__ rinv) {
     for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < g.n; u += gridDim.x * blockDim.x) {
         const uint4 rec = g.vtx[u];
@@ -1447,7 +1463,7 @@ __global__ void k_wpr_keys(const unsigned long long *__restrict__ off, const uin
             else hi = mid;
         }
         keys[i] = ((unsigned long long)dst[i] << bitsn) | lo;
-        vals[i] = __float_as_uint(w[i]);
+        vals[i] = __float_as_uint(w ? w[i] : 1.0f);
     }
 }
 
@@ -1781,7 +1797,7 @@ extern "C" {
 gv_status gv_ppr_batch(gv_graph *g, const uint32_t *sources, uint32_t k, float alpha, float epsilon, int32_t max_iter,
                        float *x_out, int32_t *sweeps, int mem, void *stream) {
     if (!g || !sources || !x_out || k == 0 || k > 32 || max_iter < 0) { set_error("bad argument"); return GV_ERR_INVALID; }
-    if (g->cfg.directed) { set_error("PageRank pull needs an undirected (symmetric) store"); return GV_ERR_STATE; }
+    if (g->cfg.directed) { set_error("batched PPR needs an undirected (symmetric) store"); return GV_ERR_STATE; }
     if (mem == GV_MEM_HOST)
         for (uint32_t j = 0; j < k; ++j)
             if (sources[j] >= g->d.n) { set_error("source out of range"); return GV_ERR_INVALID; }
@@ -1872,11 +1888,17 @@ gv_status gv_tc_subset(gv_graph *g, const uint32_t *subset, uint64_t ns, uint64_
     return cuda_status(e, "tc subset");
 }
 
-gv_status gv_wpr_forward(gv_graph *g, float alpha, float tol, int32_t max_iter, float *x_out, int32_t *sweeps, int mem,
-                         void *stream) {
-    if (!g || !x_out || max_iter < 0) return GV_ERR_INVALID;
-    if (!g->cfg.weighted) { set_error("weighted PageRank needs a weighted store"); return GV_ERR_STATE; }
-    cudaStream_t s = (cudaStream_t)stream;
+}  // extern "C"
+
+namespace gv {
+namespace {
+
+// PageRank over the sorted in-edge transpose of the store: weighted (raw
+// weights normalised per row) or, with `unit`, plain PageRank on a directed
+// store (every out-entry of u weighs 1 / outdeg(u)).  x_init (warm start) or
+// a personalisation source as pagerank_impl takes them.
+gv_status transpose_pagerank(gv_graph *g, float alpha, float tol, int32_t max_iter, bool unit, const float *x_init,
+                             int init_mem, uint32_t source, float *x_out, int32_t *sweeps, int mem, cudaStream_t s) {
     DevGraph d = g->d;
     const uint32_t n = d.n;
     uint64_t live = 0;
@@ -1900,7 +1922,8 @@ gv_status gv_wpr_forward(gv_graph *g, float alpha, float tol, int32_t max_iter, 
     uint32_t *tsrc = (uint32_t *)p; p += (live + 1) * 4;
     float *tw = (float *)p;
     uint32_t *heavy = cursor;  // list of vertices above WPR_HEAVY in-edges (n words)
-    GV_LAUNCH(k_row_sums, grid_for(n, 256), 256, 0, s, d, rinv);
+    if (unit) GV_LAUNCH(k_row_inv_deg, grid_for(n, 256), 256, 0, s, d, rinv);
+    else GV_LAUNCH(k_row_sums, grid_for(n, 256), 256, 0, s, d, rinv);
     {
         ProfScope ps(PROF_WPR_BUILD, s);
         // export (storage order), keys (v, u) with weight bits, stable radix sort by (v, u)
@@ -1922,11 +1945,11 @@ gv_status gv_wpr_forward(gv_graph *g, float alpha, float tol, int32_t max_iter, 
         void *stmp = sb + o_t;
         launch_degrees(g, indeg, s);
         scan_exclusive_u32_to_u64(indeg, eoff, n, eoff + n, stmp, s);
-        gv_status est = run_export(g, eoff, edst, ew, s);
+        gv_status est = run_export(g, eoff, edst, unit ? nullptr : ew, s);
         if (est != GV_OK) return est;
         if (E) {
             GV_LAUNCH(k_wpr_keys, grid_for(E, 256, 148 * 16), 256, 0, s, (const unsigned long long *)eoff,
-                      (const uint32_t *)edst, (const float *)ew, n, E, g->bitsn, k1, v1);
+                      (const uint32_t *)edst, unit ? (const float *)nullptr : (const float *)ew, n, E, g->bitsn, k1, v1);
             const int which = radix_sort_u64(k1, k2, v1, v2, E, 2 * (int)g->bitsn, cnts, stmp, s);
             const unsigned long long *ks = which ? k2 : k1;
             GV_LAUNCH(k_wpr_unpack, grid_for(E, 256, 148 * 16), 256, 0, s, ks, which ? v2 : v1, E,
@@ -1941,7 +1964,15 @@ gv_status gv_wpr_forward(gv_graph *g, float alpha, float tol, int32_t max_iter, 
     uint32_t *hcnt = reinterpret_cast<uint32_t *>(b.res) + 2;
     cudaMemsetAsync(hcnt, 0, 4, s);
     GV_LAUNCH(k_wpr_heavy_list, grid_for(n, 256), 256, 0, s, (const unsigned long long *)toff, n, heavy, hcnt);
-    GV_LAUNCH(k_fill_f32, grid_for(n, 256), 256, 0, s, b.x0, n, 1.0f / (float)n, GV_NIL, 0.f);
+    if (x_init) {
+        cudaError_t ei = cudaMemcpyAsync(b.x0, x_init, (size_t)n * 4,
+                                         init_mem == GV_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s);
+        if (ei != cudaSuccess) return cuda_status(ei, "pagerank init");
+    } else if (source == GV_NIL) {
+        GV_LAUNCH(k_fill_f32, grid_for(n, 256), 256, 0, s, b.x0, n, 1.0f / (float)n, GV_NIL, 0.f);
+    } else {
+        GV_LAUNCH(k_fill_f32, grid_for(n, 256), 256, 0, s, b.x0, n, 0.f, source, 1.f);
+    }
     cudaMemsetAsync(b.state, 0, 16, s);
     const uint32_t nparts = PULL_GRID + WPR_HEAVY_GRID;
     float *xa = b.x0, *xb = b.x1;
@@ -1949,8 +1980,14 @@ gv_status gv_wpr_forward(gv_graph *g, float alpha, float tol, int32_t max_iter, 
     int launched = 0;
     PullArgs a{};
     a.alpha = alpha;
-    a.base_all = (1.0f - alpha) / (float)n;
-    a.base_src = GV_NIL;
+    if (source == GV_NIL) {
+        a.base_all = (1.0f - alpha) / (float)n;
+        a.base_src = GV_NIL;
+    } else {
+        a.base_all = 0.f;
+        a.base_src = source;
+        a.base_src_val = 1.0f - alpha;
+    }
     a.partial = b.partial;
     a.state = b.state;
     while (launched < max_iter) {
@@ -1982,6 +2019,19 @@ gv_status gv_wpr_forward(gv_graph *g, float alpha, float tol, int32_t max_iter, 
     }
     if (sweeps) *sweeps = h_state[1];
     return copy_out_f32((h_state[1] & 1) ? b.x1 : b.x0, x_out, n, mem, s);
+}
+
+}  // namespace
+}  // namespace gv
+
+extern "C" {
+
+gv_status gv_wpr_forward(gv_graph *g, float alpha, float tol, int32_t max_iter, float *x_out, int32_t *sweeps, int mem,
+                         void *stream) {
+    if (!g || !x_out || max_iter < 0) return GV_ERR_INVALID;
+    if (!g->cfg.weighted) { set_error("weighted PageRank needs a weighted store"); return GV_ERR_STATE; }
+    return transpose_pagerank(g, alpha, tol, max_iter, false, nullptr, 0, GV_NIL, x_out, sweeps, mem,
+                              (cudaStream_t)stream);
 }
 
 gv_status gv_wpr_backward(gv_graph *g, float alpha, float tol, int32_t max_iter, const float *x, const float *c,

@@ -349,6 +349,7 @@ gv_status gv_create(const gv_config *cfg, gv_graph **out) {
     if (P == 0) { delete g; set_error("HBM budget leaves no room for edge blocks"); return GV_ERR_NOMEM; }
     DevGraph &d = g->d;
     d.n = n;
+    g->n_cap = n;
     d.B = B;
     d.logB = (uint32_t)__builtin_ctz(B);
     d.weighted = cfg->weighted ? 1 : 0;
@@ -398,6 +399,7 @@ gv_status gv_view_create(gv_graph *g, gv_graph **out) {
     v->bitsn = g->bitsn;
     v->d = g->d;
     v->parent = g;
+    g->nviews.fetch_add(1);
     v->weighted_alloc = g->weighted_alloc;
     // analytics need a scan scratch and a few words of their own
     const uint64_t elems = (uint64_t)g->d.n + 2;
@@ -416,6 +418,7 @@ gv_status gv_destroy(gv_graph *g) {
     if (!g) return GV_OK;
     DeviceGuard dg(g->cfg.device);
     if (g->parent) {  // a view: free only its own scratch
+        g->parent->nviews.fetch_sub(1);
         dfree(g->bs.scan_tmp);
         dfree(g->bs.tile_cnt);
         if (g->an_buf) cudaFree(g->an_buf);
@@ -524,6 +527,95 @@ gv_status gv_bulk_build_csr(gv_graph *g, const uint64_t *offsets, const uint32_t
     cudaStreamSynchronize(s);
     cudaFree(src);
     return st;
+}
+
+// Per-vertex arrays grow to the next power of two (the reference sizes its
+// dictionary with computeNearestPowerOf2, graphvine.cu:42, but cannot grow).
+gv_status gv_add_vertices(gv_graph *g, uint32_t k, uint32_t *first, void *stream) {
+    if (!g) { set_error("null argument"); return GV_ERR_INVALID; }
+    if (g->parent) { set_error("a view is read-only"); return GV_ERR_STATE; }
+    if (g->nviews.load() > 0) { set_error("destroy the graph's views before adding vertices"); return GV_ERR_STATE; }
+    DeviceGuard dg(g->cfg.device);
+    cudaStream_t s = (cudaStream_t)stream;
+    DevGraph &d = g->d;
+    const uint64_t n = d.n, nn = n + k;
+    if (nn > 0xFFFFFFF0ull) { set_error("vertex count out of range"); return GV_ERR_INVALID; }
+    if (first) *first = (uint32_t)n;
+    if (k == 0) return GV_OK;
+    cudaError_t e = cudaStreamSynchronize(s);  // work in flight still uses the old arrays
+    if (e != cudaSuccess) return cuda_status(e, "add vertices");
+    if (nn > g->n_cap) {
+        uint64_t cap = 1;
+        while (cap < nn) cap <<= 1;
+        if (cap > 0xFFFFFFF0ull) cap = nn;
+        uint4 *vtx = nullptr;
+        uint8_t *aff = nullptr, *dirty = nullptr;
+        uint32_t *dl = nullptr, *vb = nullptr;
+        gv_status st = dmalloc(&vtx, cap * sizeof(uint4), "vtx");
+        if (st == GV_OK) st = dmalloc(&aff, cap, "affected");
+        if (st == GV_OK) st = dmalloc(&dirty, cap, "dirty");
+        if (st == GV_OK) st = dmalloc(&dl, cap * 4, "dirty_list");
+        if (st == GV_OK) st = dmalloc(&vb, cap * 4, "vbig_list");
+        if (st != GV_OK) {
+            dfree(vtx); dfree(aff); dfree(dirty); dfree(dl); dfree(vb);
+            return st;
+        }
+        e = cudaMemcpy(vtx, d.vtx, n * sizeof(uint4), cudaMemcpyDeviceToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(aff, d.affected, n, cudaMemcpyDeviceToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(dirty, d.dirty, n, cudaMemcpyDeviceToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(dl, d.dirty_list, n * 4, cudaMemcpyDeviceToDevice);
+        if (e != cudaSuccess) {
+            dfree(vtx); dfree(aff); dfree(dirty); dfree(dl); dfree(vb);
+            return cuda_status(e, "add vertices copy");
+        }
+        dfree(d.vtx); dfree(d.affected); dfree(d.dirty); dfree(d.dirty_list); dfree(d.vbig_list);
+        d.vtx = vtx; d.affected = aff; d.dirty = dirty; d.dirty_list = dl; d.vbig_list = vb;
+        g->n_cap = (uint32_t)cap;
+    }
+    GV_LAUNCH(k_init_store, grid_for(k, 256, 148 * 16), 256, 0, s, d.vtx + n, k, nullptr, 0ull);
+    cudaMemsetAsync(d.affected + n, 0, k, s);
+    cudaMemsetAsync(d.dirty + n, 0, k, s);
+    d.n = (uint32_t)nn;
+    g->bitsn = (nn <= 1) ? 1u : (uint32_t)(32 - __builtin_clz((uint32_t)(nn - 1)));
+    // the scan scratch is sized for n + 1 elements: rebuild the batch scratch
+    const uint64_t cap_e = g->bs.cap, cap_p = g->bs.in_cap;
+    free_batch_entries(g->bs);
+    g->bs.cap = 0;
+    gv_status st = ensure_batch_scratch(g, std::max<uint64_t>(cap_e, 1), std::max<uint64_t>(cap_p, 1));
+    if (st != GV_OK) return st;
+    e = cudaStreamSynchronize(s);
+    return cuda_status(e, "add vertices");
+}
+
+gv_status gv_delete_vertices(gv_graph *g, const uint32_t *ids, uint64_t k, uint32_t flags, int mem, void *stream) {
+    if (!g || (k && !ids)) { set_error("null argument"); return GV_ERR_INVALID; }
+    if (g->parent) { set_error("a view is read-only"); return GV_ERR_STATE; }
+    DeviceGuard dg(g->cfg.device);
+    cudaStream_t s = (cudaStream_t)stream;
+    const uint32_t n = g->d.n;
+    std::vector<uint32_t> h;
+    const uint32_t *hid = ids;
+    if (mem == GV_MEM_DEVICE && k) {
+        h.resize(k);
+        cudaError_t e = cudaMemcpyAsync(h.data(), ids, k * 4, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return cuda_status(e, "delete vertices ids");
+        hid = h.data();
+    }
+    std::vector<uint8_t> mark(n, 0);
+    for (uint64_t i = 0; i < k; ++i) {
+        if (hid[i] >= n) { set_error("vertex id out of range"); return GV_ERR_INVALID; }
+        mark[hid[i]] = 1;
+    }
+    if (k == 0) return GV_OK;
+    uint8_t *del = (uint8_t *)aux_scratch(g, 0, n);
+    if (!del) return GV_ERR_NOMEM;
+    cudaError_t e = cudaMemcpyAsync(del, mark.data(), n, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return cuda_status(e, "delete vertices flags");
+    gv_status st = run_vertex_delete(g, del, s);
+    if (st == GV_OK && (flags & GV_UPDATE_COMPACT)) st = run_compact(g, s);
+    if (st != GV_OK) return st;
+    return cuda_status(cudaStreamSynchronize(s), "delete vertices");
 }
 
 gv_status gv_compact(gv_graph *g, void *stream) {

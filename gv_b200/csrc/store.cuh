@@ -1,6 +1,7 @@
 // Host-side definition of a graph and the launch helpers the C ABI calls.
 #pragma once
 #include <cstdint>
+#include <atomic>
 #include <string>
 #include <cuda_runtime.h>
 #include "../../include/gv.h"
@@ -53,6 +54,8 @@ struct gv_graph {
     size_t aux_bytes[AUX_SLOTS] = {};
     // a view shares the parent's store and owns only analytics scratch
     gv_graph *parent = nullptr;
+    std::atomic<int> nviews{0};  // live views of this graph (growth waits for none)
+    uint32_t n_cap = 0;          // vertices the per-vertex arrays hold
 };
 
 namespace gv {
@@ -77,6 +80,8 @@ void launch_commit_keep_abort(gv_graph *g, cudaStream_t s);
 void launch_finish(gv_graph *g, cudaStream_t s);
 void release_window(gv_graph *g);
 gv_status run_compact(gv_graph *g, cudaStream_t s);
+// Tombstones every entry whose source or destination is flagged in del[n].
+gv_status run_vertex_delete(gv_graph *g, const uint8_t *del, cudaStream_t s);
 gv_status run_export(gv_graph *g, unsigned long long *offsets, uint32_t *dst, float *w,
                      cudaStream_t s);
 gv_status run_check(gv_graph *g, uint64_t *violations, uint32_t *code, uint32_t *vertex);

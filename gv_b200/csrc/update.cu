@@ -657,6 +657,47 @@ __global__ void k_compact_done(Ctl *ctl) {
     ctl->nbig = 0;
 }
 
+// --------------------------------------------------------- vertex delete
+// Every entry of a flagged vertex, and every entry pointing at one, becomes
+// a tombstone; live counts, the control block and the dirty list change as a
+// batch delete changes them, so gv_compact reclaims the blocks.
+template <int TPV>
+__global__ void __launch_bounds__(UPD_THREADS) k_vertex_delete(DevGraph g, const uint8_t *__restrict__ del) {
+    Group<TPV> G;
+    constexpr int GPC = UPD_THREADS / TPV;
+    const uint32_t ngroups = gridDim.x * GPC;
+    for (uint32_t u = blockIdx.x * GPC + threadIdx.x / TPV; u < g.n; u += ngroups) {
+        const uint4 rec = g.vtx[u];
+        const uint32_t fill = rec.y, nb = blocks_for(fill, g.logB);
+        if (rec.z == 0) continue;
+        const bool all = del[u] != 0;
+        uint32_t cnt = 0;
+        for (uint32_t k = 0; k < nb; ++k) {
+            const uint32_t b = (k == 0) ? rec.x : cbt_block(g.left, g.right, rec.x, k);
+            const uint32_t slots = min(g.B, fill - (k << g.logB));
+            uint32_t *blk = g.pool + ((size_t)b << g.logB);
+            for (uint32_t i = G.gl; i < slots; i += TPV) {
+                const uint32_t v = blk[i];
+                if (v != GV_TOMB && (all || del[v])) {
+                    blk[i] = GV_TOMB;
+                    g.affected[v] = 1;
+                    ++cnt;
+                }
+            }
+        }
+        cnt = G.sum(cnt);
+        if (G.gl == 0 && cnt) {
+            g.vtx[u].z = rec.z - cnt;
+            g.affected[u] = 1;
+            atomicAdd(&g.ctl->live_edges, (unsigned long long)(-(long long)cnt));
+            if (!g.dirty[u]) {
+                g.dirty[u] = 1;
+                g.dirty_list[atomicAdd(&g.ctl->ndirty, 1ull)] = u;
+            }
+        }
+    }
+}
+
 // ------------------------------------------------------------------ export
 template <int TPV>
 __global__ void __launch_bounds__(UPD_THREADS) k_export(DevGraph g, const unsigned long long *__restrict__ off,
@@ -869,6 +910,15 @@ gv_status run_export(gv_graph *g, unsigned long long *offsets, uint32_t *dst, fl
         GV_LAUNCH((k_export<T>), grid_for(g->d.n, UPD_THREADS / T), UPD_THREADS, 0, s, d, offsets, dst, w);
     });
     return cuda_status(cudaGetLastError(), "export launch");
+}
+
+gv_status run_vertex_delete(gv_graph *g, const uint8_t *del, cudaStream_t s) {
+    DevGraph d = g->d;
+    dispatch_tpv(g->cfg.threads_per_vertex, [&](auto t) {
+        constexpr int T = decltype(t)::value;
+        GV_LAUNCH((k_vertex_delete<T>), grid_for(g->d.n, UPD_THREADS / T), UPD_THREADS, 0, s, d, del);
+    });
+    return cuda_status(cudaGetLastError(), "vertex delete launch");
 }
 
 void launch_degrees(gv_graph *g, uint32_t *deg, cudaStream_t s) {

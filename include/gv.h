@@ -48,6 +48,9 @@ typedef enum gv_status {
 
 enum { GV_MEM_HOST = 0, GV_MEM_DEVICE = 1 };
 
+/* Update flag: compact after the deletes (gv_update_tc, gv_delete_vertices). */
+#define GV_UPDATE_COMPACT 1u
+
 /* Store configuration.  Replaces the reference's compile-time constants
  * (include/dynamicStructure/constants.cuh:4-19: EDGE_BLOCK_SIZE,
  * THREADS_PER_BLOCK, DIRECTED) and its "half of device memory" pool sizing
@@ -104,6 +107,20 @@ gv_status gv_insert_edges(gv_graph *g, const uint32_t *src, const uint32_t *dst,
 gv_status gv_delete_edges(gv_graph *g, const uint32_t *src, const uint32_t *dst,
                           uint64_t k, int mem, void *stream);
 
+/* Adds k isolated vertices with ids n .. n + k - 1 (*first = n).  The vertex
+ * table grows to the next power of two when it is full; the store's blocks
+ * stay where they are.  The reference has no vertex insert (its menu option
+ * 3, src/main.cu:80, :122-124, is empty) and sizes its dictionary once
+ * (computeNearestPowerOf2, graphvine.cu:42).  Fails with GV_ERR_STATE while
+ * views of g exist.  Synchronous. */
+gv_status gv_add_vertices(gv_graph *g, uint32_t k, uint32_t *first, void *stream);
+
+/* Removes every edge incident to the k listed vertices (their own entries
+ * and every entry pointing at them, on directed stores too); the ids stay
+ * valid, isolated.  flags & GV_UPDATE_COMPACT compacts afterwards.  No
+ * reference counterpart (src/main.cu:122-124).  Synchronous. */
+gv_status gv_delete_vertices(gv_graph *g, const uint32_t *ids, uint64_t k, uint32_t flags, int mem, void *stream);
+
 /* Fills tombstone holes, returns emptied tail blocks to the pool and unlinks
  * them from their CBT parents; the neighbour set is unchanged.  Replaces
  * GraphVine::compaction (src/dynamicStructure/graphvine.cu:453-464). */
@@ -137,7 +154,6 @@ gv_status gv_export_csr(gv_graph *g, uint64_t *offsets, uint32_t *dst, float *we
  * (src/algorithm/tc/tc.cu:29-64, tc_kernel.cu:76-147), which recounts only
  * the owned triangles of vertices touched by the batch and so misses
  * triangles whose owner was not touched.  Synchronous. */
-#define GV_UPDATE_COMPACT 1u
 gv_status gv_update_tc(gv_graph *g, const uint32_t *ins_src, const uint32_t *ins_dst, const float *ins_w,
                        uint64_t n_ins, const uint32_t *del_src, const uint32_t *del_dst, uint64_t n_del,
                        uint32_t flags, int64_t *delta_total, int64_t *delta_owner, int mem, void *stream);

@@ -209,3 +209,38 @@ def test_affected_flags():
     assert set(np.nonzero(a)[0]) == {1, 2, 3, 4}
     g.clear_affected()
     assert g.affected().sum() == 0
+
+
+@pytest.mark.parametrize("directed", [False, True])
+def test_add_and_delete_vertices(directed):
+    """Vertices added past the table's capacity take edges like any other;
+    deleting vertices removes exactly their incident edges; analytics run on
+    the grown graph."""
+    n0, k = 1000, 1500
+    s, d = rmat_graph(10, 8, seed=12)
+    s, d = s % n0, d % n0
+    g = make_graph(n0, directed=directed)
+    g.batch_insert(s, d)
+    first = g.add_vertices(k)
+    assert first == n0 and g.n == n0 + k
+    n = n0 + k
+    rng = np.random.default_rng(4)
+    ns = rng.integers(0, n, 6000).astype(np.uint32)
+    nd = rng.integers(n0, n, 6000).astype(np.uint32)
+    g.batch_insert(ns, nd)
+    o = oracle.OracleGraph(n, directed=directed)
+    o.insert(s, d)
+    o.insert(ns, nd)
+    assert_same_adjacency(g, o)
+    assert_sound(g)
+    dead = np.unique(np.concatenate([rng.integers(0, n0, 30), rng.integers(n0, n, 30)])).astype(np.uint32)
+    g.delete_vertices(dead)
+    off, dst, _ = o.export()
+    src = np.repeat(np.arange(n, dtype=np.uint32), np.diff(off).astype(np.int64))
+    hit = np.isin(src, dead) | np.isin(dst, dead)
+    o.delete(src[hit], dst[hit])
+    assert_same_adjacency(g, o)
+    assert_sound(g)
+    x, sw = g.static_pagerank(0.85, 1e-6, 100)
+    xo, _ = o.pagerank(0.85, 1e-6, 100, fixed_sweeps=sw)
+    assert np.abs(x - xo).sum() < 1e-6
