@@ -67,11 +67,17 @@ __device__ __forceinline__ uint32_t ms_block(const DevGraph &g, uint32_t root, u
 }
 
 // Walks the entries of one block 32 at a time: lane j loads entry e0 + j and
-// pre(w) for it; then body(w, pre) runs for each entry with the whole warp.
+// its source mask pre(w) (0: nothing to do for any source); the entries with
+// a non-zero mask are packed into the warp's shared slots, and body(w, mask)
+// runs for each of them with the whole warp (lane = source).  In most levels
+// few entries need work, so the warp skips the rest without touching them.
+__shared__ uint2 ms_pack[MS_WARPS][32];  // one row of slots per warp (the kernels run MS_THREADS threads)
+
 template <typename Pre, typename Body>
 __device__ __forceinline__ void ms_block_entries(const DevGraph &g, uint32_t b, uint32_t slots, Pre &&pre,
                                                  Body &&body) {
     const uint32_t lane = threadIdx.x & 31u;
+    uint2 *pack = ms_pack[threadIdx.x >> 5];
     const uint32_t *bp = g.pool + ((size_t)b << g.logB);
     for (uint32_t e0 = 0; e0 < slots; e0 += 32) {
         const uint32_t e = e0 + lane;
@@ -80,12 +86,16 @@ __device__ __forceinline__ void ms_block_entries(const DevGraph &g, uint32_t b, 
             w = bp[e];
             if (w != GV_TOMB) pv = pre(w);
         }
-        const uint32_t c = min(32u, slots - e0);
+        const uint32_t bal = __ballot_sync(GV_FULL_MASK, pv != 0);
+        if (!bal) continue;  // warp-uniform
+        if (pv) pack[__popc(bal & ((1u << lane) - 1u))] = make_uint2(w, pv);
+        __syncwarp();
+        const uint32_t c = __popc(bal);
         for (uint32_t j = 0; j < c; ++j) {
-            const uint32_t wj = __shfl_sync(GV_FULL_MASK, w, j);
-            const uint32_t pj = __shfl_sync(GV_FULL_MASK, pv, j);
-            if (wj != GV_TOMB) body(wj, pj);
+            const uint2 x = pack[j];
+            body(x.x, x.y);
         }
+        __syncwarp();
     }
 }
 
@@ -158,10 +168,9 @@ struct FwdBody {
     MsBufs b;
     uint32_t F;
     unsigned long long sig;
-    __device__ __forceinline__ uint32_t operator()(uint32_t w) const { return b.vis[w]; }
-    __device__ __forceinline__ void visit(uint32_t w, uint32_t vw) const {
-        const uint32_t want = F & ~vw;
-        if (!want) return;
+    // sources that reach w first through this level
+    __device__ __forceinline__ uint32_t operator()(uint32_t w) const { return F & ~b.vis[w]; }
+    __device__ __forceinline__ void visit(uint32_t w, uint32_t want) const {
         const uint32_t lane = threadIdx.x & 31u;
         if (lane == 0) atomicOr(&b.nxt[w], want);
         if ((want >> lane) & 1u) atomicAdd(&b.row[(size_t)w * 32 + lane], sig);
@@ -230,15 +239,23 @@ __device__ __forceinline__ double ms_bwd_block(const DevGraph &g, const MsBufs &
             if (w != GV_TOMB) mw = deeper[w] & A;
             else w = 0;
         }
-        if (!__any_sync(GV_FULL_MASK, mw != 0)) continue;
-#pragma unroll 8
-        for (uint32_t j = 0; j < 32; ++j) {
-            const uint32_t wj = __shfl_sync(GV_FULL_MASK, w, j);
-            const uint32_t cj = __shfl_sync(GV_FULL_MASK, mw, j);
-            const bool take = (cj >> lane) & 1u;
-            const unsigned long long x = take ? __ldg(row + (size_t)wj * 32 + lane) : 0ull;
-            acc += as_f64(x);
+        const uint32_t bal = __ballot_sync(GV_FULL_MASK, mw != 0);
+        if (!bal) continue;  // warp-uniform
+        uint2 *pack = ms_pack[threadIdx.x >> 5];
+        if (mw) pack[__popc(bal & ((1u << lane) - 1u))] = make_uint2(w, mw);
+        __syncwarp();
+        const uint32_t c = __popc(bal);
+        for (uint32_t j0 = 0; j0 < c; j0 += 8) {  // eight gathers in flight, summed in entry order
+            uint2 x[8];
+#pragma unroll
+            for (int t = 0; t < 8; ++t) x[t] = (j0 + t < c) ? pack[j0 + t] : make_uint2(0u, 0u);
+            unsigned long long v[8];
+#pragma unroll
+            for (int t = 0; t < 8; ++t) v[t] = ((x[t].y >> lane) & 1u) ? __ldg(row + (size_t)x[t].x * 32 + lane) : 0ull;
+#pragma unroll
+            for (int t = 0; t < 8; ++t) acc += as_f64(v[t]);
         }
+        __syncwarp();
     }
     return acc;
 }
