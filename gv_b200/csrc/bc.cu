@@ -177,10 +177,11 @@ struct FwdBody {
     }
 };
 
-__global__ void __launch_bounds__(MS_THREADS) k_ms_fwd_light(DevGraph g, MsBufs b, const uint32_t *__restrict__ mask) {
+__device__ __forceinline__ void ms_fwd_light(const DevGraph &g, const MsBufs &b, const uint32_t *__restrict__ mask,
+                                             uint32_t vb, uint32_t vg) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t nl = b.cnt[0];
-    for (uint32_t i = blockIdx.x * MS_WARPS + (threadIdx.x >> 5); i < nl; i += gridDim.x * MS_WARPS) {
+    for (uint32_t i = vb * MS_WARPS + (threadIdx.x >> 5); i < nl; i += vg * MS_WARPS) {
         const uint32_t u = b.light[i];
         FwdBody f{b, mask[u], 0ull};
         if ((f.F >> lane) & 1u) f.sig = b.row[(size_t)u * 32 + lane];
@@ -188,16 +189,38 @@ __global__ void __launch_bounds__(MS_THREADS) k_ms_fwd_light(DevGraph g, MsBufs 
     }
 }
 
-__global__ void __launch_bounds__(MS_THREADS) k_ms_fwd_heavy(DevGraph g, MsBufs b, const uint32_t *__restrict__ mask) {
+__device__ __forceinline__ void ms_fwd_heavy(const DevGraph &g, const MsBufs &b, const uint32_t *__restrict__ mask,
+                                             uint32_t vb, uint32_t vg) {
     __shared__ uint32_t tab[MS_TAB];
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t nh = b.cnt[1];
-    for (uint32_t i = blockIdx.x; i < nh; i += gridDim.x) {
+    for (uint32_t i = vb; i < nh; i += vg) {
         const uint32_t u = b.heavy[i];
         FwdBody f{b, mask[u], 0ull};
         if ((f.F >> lane) & 1u) f.sig = b.row[(size_t)u * 32 + lane];
         ms_walk_heavy(g, g.vtx[u], tab, f, [&](uint32_t w, uint32_t vw) { f.visit(w, vw); });
     }
+}
+
+// One launch per level and direction: CTA i runs the heavy-vertex part when
+// i % 5 == 4, the light part otherwise, so hub CTAs and light warps share
+// every wave.
+__device__ __forceinline__ bool ms_split_cta(uint32_t &vb, uint32_t &vg_light, uint32_t &vg_heavy) {
+    const uint32_t bi = blockIdx.x;
+    vg_heavy = gridDim.x / 5;
+    vg_light = gridDim.x - vg_heavy;
+    if (bi % 5 == 4) {
+        vb = bi / 5;
+        return true;
+    }
+    vb = (bi / 5) * 4 + bi % 5;
+    return false;
+}
+
+__global__ void __launch_bounds__(MS_THREADS) k_ms_fwd(DevGraph g, MsBufs b, const uint32_t *__restrict__ mask) {
+    uint32_t vb, vgl, vgh;
+    if (ms_split_cta(vb, vgl, vgh)) ms_fwd_heavy(g, b, mask, vb, vgh);
+    else ms_fwd_light(g, b, mask, vb, vgl);
 }
 
 // Closes level L: masks[L+1] = nxt, vis |= nxt, flags[L+1] = any.
@@ -285,11 +308,11 @@ __device__ __forceinline__ double ms_finish(MsBufs &b, uint32_t v, uint32_t A, u
     return delta;
 }
 
-__global__ void __launch_bounds__(MS_THREADS) k_ms_bwd_light(DevGraph g, MsBufs b, const uint32_t *__restrict__ mask,
-                                                             const uint32_t *__restrict__ deeper) {
+__device__ __forceinline__ void ms_bwd_light_v(const DevGraph &g, MsBufs b, const uint32_t *__restrict__ mask,
+                                               const uint32_t *__restrict__ deeper, uint32_t vb, uint32_t vg) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t nl = b.cnt[0];
-    for (uint32_t i = blockIdx.x * MS_WARPS + (threadIdx.x >> 5); i < nl; i += gridDim.x * MS_WARPS) {
+    for (uint32_t i = vb * MS_WARPS + (threadIdx.x >> 5); i < nl; i += vg * MS_WARPS) {
         const uint32_t v = b.light[i];
         const uint32_t A = mask[v];
         const unsigned long long sig = ((A >> lane) & 1u) ? b.row[(size_t)v * 32 + lane] : 0ull;
@@ -300,13 +323,13 @@ __global__ void __launch_bounds__(MS_THREADS) k_ms_bwd_light(DevGraph g, MsBufs 
     }
 }
 
-__global__ void __launch_bounds__(MS_THREADS) k_ms_bwd_heavy(DevGraph g, MsBufs b, const uint32_t *__restrict__ mask,
-                                                             const uint32_t *__restrict__ deeper) {
+__device__ __forceinline__ void ms_bwd_heavy_v(const DevGraph &g, MsBufs b, const uint32_t *__restrict__ mask,
+                                               const uint32_t *__restrict__ deeper, uint32_t vb, uint32_t vg) {
     __shared__ uint32_t tab[MS_TAB];
     __shared__ double red[MS_WARPS][32];
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t nh = b.cnt[1];
-    for (uint32_t i = blockIdx.x; i < nh; i += gridDim.x) {
+    for (uint32_t i = vb; i < nh; i += vg) {
         const uint32_t v = b.heavy[i];
         const uint32_t A = mask[v];
         const unsigned long long sig = ((A >> lane) & 1u) ? b.row[(size_t)v * 32 + lane] : 0ull;
@@ -332,6 +355,13 @@ __global__ void __launch_bounds__(MS_THREADS) k_ms_bwd_heavy(DevGraph g, MsBufs 
         }
         __syncthreads();
     }
+}
+
+__global__ void __launch_bounds__(MS_THREADS) k_ms_bwd(DevGraph g, MsBufs b, const uint32_t *__restrict__ mask,
+                                                       const uint32_t *__restrict__ deeper) {
+    uint32_t vb, vgl, vgh;
+    if (ms_split_cta(vb, vgl, vgh)) ms_bwd_heavy_v(g, b, mask, deeper, vb, vgh);
+    else ms_bwd_light_v(g, b, mask, deeper, vb, vgl);
 }
 
 __global__ void k_ms_to_f32(const double *__restrict__ x, float *__restrict__ y, uint32_t n) {
@@ -406,8 +436,8 @@ gv_status ms_forward(gv_graph *g, MsBufs &b, uint32_t &cap, uint32_t *h_flags, u
             ProfScope ps(PROF_BFS_LEVEL, s);
             cudaMemsetAsync(b.cnt, 0, 8, s);
             GV_LAUNCH(k_ms_split, grid_for(n, 256), 256, 0, s, d, b, mask);
-            GV_LAUNCH(k_ms_fwd_light, MS_LIGHT_GRID, MS_THREADS, 0, s, d, b, mask);
-            GV_LAUNCH(k_ms_fwd_heavy, MS_HEAVY_GRID, MS_THREADS, 0, s, d, b, mask);
+            static_assert(MS_LIGHT_GRID == 4 * MS_HEAVY_GRID, "the fused launch interleaves 4 light CTAs per heavy one");
+            GV_LAUNCH(k_ms_fwd, MS_LIGHT_GRID + MS_HEAVY_GRID, MS_THREADS, 0, s, d, b, mask);
             GV_LAUNCH(k_ms_close, grid_for(n, 256), 256, 0, s, b, b.masks + (size_t)(L + 1) * n, b.flags + L + 1);
         }
         cudaError_t e = cudaMemcpyAsync(h_flags, b.flags + L - chunk + 1, chunk * 4, cudaMemcpyDeviceToHost, s);
@@ -430,8 +460,7 @@ gv_status ms_backward(gv_graph *g, MsBufs &b, uint32_t depth, cudaStream_t s) {
         ProfScope ps(PROF_BC_DEP, s);
         cudaMemsetAsync(b.cnt, 0, 8, s);
         GV_LAUNCH(k_ms_split, grid_for(n, 256), 256, 0, s, d, b, mask);
-        GV_LAUNCH(k_ms_bwd_light, MS_LIGHT_GRID, MS_THREADS, 0, s, d, b, mask, deeper);
-        GV_LAUNCH(k_ms_bwd_heavy, MS_HEAVY_GRID, MS_THREADS, 0, s, d, b, mask, deeper);
+        GV_LAUNCH(k_ms_bwd, MS_LIGHT_GRID + MS_HEAVY_GRID, MS_THREADS, 0, s, d, b, mask, deeper);
     }
     return cuda_status(cudaGetLastError(), "bc dependencies");
 }
