@@ -487,6 +487,18 @@ class GraphVine:
         _check(_lib.lib().gv_bc(self._h, ps, ns, out.ctypes.data, GV_MEM_HOST, _stream(stream)), "gv_bc")
         return out
 
+    def bc_multi(self, requests, stream=None) -> np.ndarray:
+        """Scores of several source sets at once (gv_bc_multi): row r of the
+        result is bc(requests[r]); an empty set means every vertex."""
+        sets = [np.ascontiguousarray(r, dtype=np.uint32) for r in requests]
+        off = np.zeros(len(sets) + 1, np.uint64)
+        off[1:] = np.cumsum([len(r) for r in sets])
+        flat = np.ascontiguousarray(np.concatenate(sets) if sets else np.empty(0, np.uint32), dtype=np.uint32)
+        out = np.empty((len(sets), self.n), np.float32)
+        _check(_lib.lib().gv_bc_multi(self._h, flat.ctypes.data if len(flat) else None, off.ctypes.data,
+                                      len(sets), out.ctypes.data, GV_MEM_HOST, _stream(stream)), "gv_bc_multi")
+        return out
+
     def bfs_sigma(self, source: int, stream=None):
         dist = np.empty(self.n, np.int32)
         sigma = np.empty(self.n, np.uint64)

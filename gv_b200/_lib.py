@@ -103,6 +103,7 @@ SIGNATURES = {
     "gv_tc_subset": (C.c_int, [P, P, u64, P, C.c_int, P]),
     "gv_update_tc": (C.c_int, [P, P, P, P, u64, P, P, u64, u32, C.POINTER(C.c_int64), P, C.c_int, P]),
     "gv_bc": (C.c_int, [P, P, u64, P, C.c_int, P]),
+    "gv_bc_multi": (C.c_int, [P, P, P, u32, P, C.c_int, P]),
     "gv_bfs_sigma": (C.c_int, [P, u32, P, P, C.c_int, P]),
     "gv_wpr_forward": (C.c_int, [P, f32, f32, i32, P, pi32, C.c_int, P]),
     "gv_wpr_backward": (C.c_int, [P, f32, f32, i32, P, P, i32, P, u64, P, pi32, C.c_int, P]),

@@ -4,7 +4,8 @@
 // run of arrived update requests becomes one coalesced window, applied once
 // every query of the current epoch has finished.  Arrived queries are
 // grouped (PPR queries into batched launches of up to ppr_batch, triangle
-// subsets into one shared count, one BC per request) and handed to worker
+// subsets into one shared count, BC requests in pairs that share their BFS
+// passes) and handed to worker
 // threads; each worker owns a read-only view of the graph and a stream, so
 // groups run concurrently on the device.  A group is admitted when a worker
 // is free and its scratch estimate fits the HBM budget.
@@ -57,7 +58,7 @@ struct Server {
         switch (kind) {
             case GV_REQ_PPR: return 20ull * n * k + 16ull * n;  // 4 iterate blocks + the result block
             case GV_REQ_TC: return 64ull * n + 8ull * g->d.P * g->d.B / 2;
-            default: return 256ull * n + 4ull * 32 * n + 40ull * n;  // BC: sigma rows, 32 level masks, lists
+            default: return 512ull * n + 8ull * 32 * n + 32ull * n + 12ull * n * k;  // BC: sigma rows, 32 level masks, lists, scores
         }
     }
 
@@ -124,22 +125,27 @@ struct Server {
                 if (out && st == GV_OK) std::memcpy(out, cnt.data() + p, reqs[r].count0 * sizeof(uint64_t));
                 p += reqs[r].count0;
             }
-        } else {  // BC: one request per job
-            const gv_request &q = reqs[jb.reqs[0]];
-            // sources to the device behind the score vector (gv_bc reads them
-            // with the same memory kind as its output)
-            const size_t at = ((size_t)n * 4 + 255) & ~size_t(255);
-            float *b = (float *)buf.get(at + (size_t)q.count0 * 4 + 4);
+        } else {  // BC: up to two requests per job, sharing 64-source passes
+            const uint32_t k = (uint32_t)jb.reqs.size();
+            std::vector<uint64_t> off{0};
+            for (uint32_t r : jb.reqs) off.push_back(off.back() + reqs[r].count0);
+            // sources to the device behind the k score rows (gv_bc_multi reads
+            // them with the same memory kind as its output)
+            const size_t at = ((size_t)n * 4 * k + 255) & ~size_t(255);
+            float *b = (float *)buf.get(at + (size_t)off.back() * 4 + 4);
             if (!b) st = GV_ERR_NOMEM;
             uint32_t *dsrc = b ? (uint32_t *)((char *)b + at) : nullptr;
-            if (st == GV_OK && q.count0) {
-                e = cudaMemcpyAsync(dsrc, qvert + q.offset, (size_t)q.count0 * 4, cudaMemcpyHostToDevice, s);
+            for (uint32_t j = 0; j < k && st == GV_OK; ++j) {
+                const gv_request &q = reqs[jb.reqs[j]];
+                if (!q.count0) continue;
+                e = cudaMemcpyAsync(dsrc + off[j], qvert + q.offset, (size_t)q.count0 * 4, cudaMemcpyHostToDevice, s);
                 if (e != cudaSuccess) st = cuda_status(e, "serve bc sources");
             }
-            if (st == GV_OK) st = gv_bc(view, q.count0 ? dsrc : nullptr, q.count0, b, GV_MEM_DEVICE, s);
-            float *out = (outs && outs->bc) ? outs->bc[jb.reqs[0]] : nullptr;
-            if (out && st == GV_OK) {
-                e = cudaMemcpyAsync(out, b, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost, s);
+            if (st == GV_OK) st = gv_bc_multi(view, dsrc, off.data(), k, b, GV_MEM_DEVICE, s);
+            for (uint32_t j = 0; j < k && st == GV_OK; ++j) {
+                float *out = (outs && outs->bc) ? outs->bc[jb.reqs[j]] : nullptr;
+                if (!out) continue;
+                e = cudaMemcpyAsync(out, b + (size_t)j * n, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost, s);
                 if (e != cudaSuccess) st = cuda_status(e, "serve bc out");
             }
         }
@@ -296,13 +302,14 @@ extern "C" gv_status gv_serve_trace(gv_graph *g, const gv_serve_config *cfg, con
     };
 
     // Groups queries idx (PPR into batches of at most ppr_batch, triangle
-    // subsets into one count, one BC each) and hands the groups to free
+    // subsets into one count, BC in pairs) and hands the groups to free
     // workers as slots and HBM budget allow.
     auto dispatch_queries = [&](const std::vector<uint32_t> &idx) {
         std::vector<Job> jobs;
-        Job ppr, tc;
+        Job ppr, tc, bc;
         ppr.kind = GV_REQ_PPR;
         tc.kind = GV_REQ_TC;
+        bc.kind = GV_REQ_BC;
         for (uint32_t i : idx) {
             if (reqs[i].kind == GV_REQ_PPR) {
                 ppr.reqs.push_back(i);
@@ -313,12 +320,14 @@ extern "C" gv_status gv_serve_trace(gv_graph *g, const gv_serve_config *cfg, con
             } else if (reqs[i].kind == GV_REQ_TC) {
                 tc.reqs.push_back(i);
             } else {
-                Job b;
-                b.kind = GV_REQ_BC;
-                b.reqs.push_back(i);
-                jobs.push_back(b);
+                bc.reqs.push_back(i);
+                if (bc.reqs.size() == 2) {
+                    jobs.push_back(bc);
+                    bc.reqs.clear();
+                }
             }
         }
+        if (!bc.reqs.empty()) jobs.push_back(bc);
         if (!ppr.reqs.empty()) jobs.push_back(ppr);
         if (!tc.reqs.empty()) jobs.push_back(tc);
         for (Job &jb : jobs) {

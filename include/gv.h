@@ -239,6 +239,17 @@ gv_status gv_tc_subset(gv_graph *g, const uint32_t *subset, uint64_t ns, uint64_
 gv_status gv_bc(gv_graph *g, const uint32_t *sources, uint64_t ns, float *bc_out,
                 int mem, void *stream);
 
+/* gv_bc for nreq requests at once: request r takes the sources
+ * sources[offsets[r] .. offsets[r+1]) (an empty range: every vertex) and
+ * gets bc_out[r*n .. (r+1)*n).  Sources run in passes of 64 that may hold
+ * two requests (32 sources each), so two small requests share one set of
+ * BFS sweeps; each request's scores equal its own gv_bc up to the order of
+ * fp64 additions.  offsets (nreq + 1 entries, offsets[0] = 0) is host
+ * memory; sources and bc_out follow mem.  New entry point: the reference
+ * runs one bc call per request (src/algorithm/bc/bc.cu:3-88). */
+gv_status gv_bc_multi(gv_graph *g, const uint32_t *sources, const uint64_t *offsets,
+                      uint32_t nreq, float *bc_out, int mem, void *stream);
+
 /* Single-source BFS level and exact shortest-path counts (the forward half
  * of gv_bc): dist[n] int32 (-1 unreachable), sigma[n] uint64. */
 gv_status gv_bfs_sigma(gv_graph *g, uint32_t source, int32_t *dist, uint64_t *sigma,

@@ -8,7 +8,8 @@
  * estimate fits the HBM budget.  Queries that arrive while others run are
  * admitted as slots free up (continuous batching): arrived PPR queries are
  * merged into batched launches, arrived triangle-subset queries share one
- * triangle count.  Epochs: with fresh = 0 a query sees exactly the updates
+ * triangle count, arrived BC queries run in pairs whose sources share one
+ * set of BFS passes (gv_bc_multi).  Epochs: with fresh = 0 a query sees exactly the updates
  * that arrived before it; with fresh = 1 (the default) it sees at least
  * those, so queries that arrive behind an update wait for it and run
  * together after it.  results[i].epoch names the updates each query saw (the

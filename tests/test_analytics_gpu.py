@@ -160,6 +160,50 @@ def test_bc_sampled_sources(graph12):
     assert np.all(b[ob == 0] == 0)
 
 
+@pytest.mark.parametrize("count", [1, 31, 33, 63, 65, 100])
+def test_bc_pass_widths(graph12, count):
+    """Source counts that leave a 32-source pass, partial halves of a
+    64-source pass, or both."""
+    n, g, o = graph12
+    src = np.random.default_rng(count).choice(n, count, replace=False).astype(np.uint32)
+    b = g.bc(src)
+    ob = o.bc(src)
+    rel = np.max(np.abs(b - ob) / np.maximum(np.abs(ob), 1e-300) * (ob != 0))
+    assert rel < BC_REL
+    assert np.all(b[ob == 0] == 0)
+
+
+def test_bc_multi_matches_single(graph12):
+    """Requests paired into shared passes score as they do alone."""
+    n, g, o = graph12
+    rng = np.random.default_rng(8)
+    reqs = [rng.choice(n, k, replace=False).astype(np.uint32) for k in (5, 32, 40, 1, 17)]
+    reqs.append(np.array([7, 7, 300], np.uint32))  # a repeated source counts twice
+    got = g.bc_multi(reqs)
+    assert got.shape == (len(reqs), n)
+    for r, src in enumerate(reqs):
+        alone = g.bc(src)
+        assert np.allclose(got[r], alone, rtol=1e-6, atol=0), r
+        ob = o.bc(src)
+        rel = np.max(np.abs(got[r] - ob) / np.maximum(np.abs(ob), 1e-300) * (ob != 0))
+        assert rel < BC_REL, r
+    again = g.bc_multi(reqs)
+    assert np.array_equal(got, again)  # repeatable bit for bit
+
+
+def test_bc_multi_every_vertex_and_rejects():
+    scale = 9
+    n = 1 << scale
+    s, d = rmat_graph(scale, 16, seed=13)
+    g = make_graph(n)
+    g.batch_insert(s, d)
+    got = g.bc_multi([np.array([], np.uint32), np.array([3, 4], np.uint32)])
+    assert np.allclose(got[0], g.bc(), rtol=1e-6, atol=0)
+    assert np.allclose(got[1], g.bc(np.array([3, 4], np.uint32)), rtol=1e-6, atol=0)
+    with pytest.raises(RuntimeError):
+        g.bc_multi([np.array([n], np.uint32)])
+
+
 def test_bc_all_sources_small():
     scale = 9
     n = 1 << scale

@@ -151,6 +151,21 @@ def test_budget_of_one_byte_runs_groups_one_at_a_time():
     g.close()
 
 
+def test_bc_queries_run_in_pairs():
+    scale = 11
+    n = 1 << scale
+    s, d = rmat_graph(scale, 8, seed=12)
+    rng = np.random.default_rng(31)
+    trace = [("bc", rng.choice(n, k, replace=False).astype(np.uint32), 0.0) for k in (3, 32, 20)]
+    g = make_graph(n)
+    g.batch_insert(s, d)
+    res, outs = g.serve(trace, slots=2, pace=False, outputs=True)
+    assert res["group"][0] == res["group"][1] != res["group"][2]
+    for i, item in enumerate(trace):
+        assert np.allclose(outs[i], g.bc(item[1]), rtol=BC_REL, atol=BC_REL), i
+    g.close()
+
+
 def test_serve_rejects_bad_config_and_views():
     n = 256
     g = make_graph(n)
