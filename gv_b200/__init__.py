@@ -69,7 +69,8 @@ def version() -> str:
 
 
 PROFILE_SLOTS = ("radix", "segment", "member", "apply", "compact", "pull", "tc_snapshot", "tc_count",
-                 "bfs_level", "bc_dep", "wpr_build", "wpr_sweep", "wpr_grad")
+                 "bfs_level", "bc_dep", "wpr_build", "wpr_sweep", "wpr_grad", "tc_core", "tc_probe",
+                 "tc_sort")
 
 
 def profile_enable(on: bool = True) -> None:

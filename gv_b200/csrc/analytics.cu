@@ -650,13 +650,20 @@ __global__ void __launch_bounds__(AN_THREADS) k_tc_write(DevGraph g, const uint3
     }
 }
 
-// Sorts tiny lists in place (one thread) and routes the rest to the sorts.
+// Sorts tiny lists in place (one thread) and routes the rest to the sorts
+// (cnts[0] mid lists, cnts[1] big lists, cnts[2] longest big list).  Lists
+// of core vertices (core_of != GV_NIL) are read by no merge and stay as they
+// are.
 __global__ void k_tc_classify(const unsigned long long *__restrict__ off, uint32_t n, uint32_t *__restrict__ snap,
                               uint32_t *__restrict__ mid_list, uint32_t *__restrict__ big_list,
-                              unsigned long long *cnts) {
+                              unsigned long long *cnts, const uint32_t *__restrict__ core_of) {
     for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x) {
+        if (core_of && core_of[u] != GV_NIL) continue;
         const uint32_t len = (uint32_t)(off[u + 1] - off[u]);
-        if (len > 1024) big_list[atomicAdd(&cnts[1], 1ull)] = u;
+        if (len > 1024) {
+            big_list[atomicAdd(&cnts[1], 1ull)] = u;
+            atomicMax(&cnts[2], (unsigned long long)len);
+        }
         else if (len > 16) mid_list[atomicAdd(&cnts[0], 1ull)] = u;
         else if (len > 1) {
             uint32_t *a = snap + off[u];
@@ -743,7 +750,8 @@ __global__ void __launch_bounds__(AN_THREADS) k_tc_count(const unsigned long lon
                                                          const uint32_t *__restrict__ snap,
                                                          const uint32_t *__restrict__ esrc, uint64_t m_plus,
                                                          unsigned long long *__restrict__ tcount,
-                                                         unsigned long long *__restrict__ work) {
+                                                         unsigned long long *__restrict__ work,
+                                                         const uint32_t *__restrict__ core_of) {
     constexpr int GPC = AN_THREADS / TPV;
     constexpr uint32_t HT = 2048;  // per-CTA credit table: hubs collect many credits
     __shared__ unsigned long long wred[AN_THREADS / 32];
@@ -772,6 +780,7 @@ __global__ void __launch_bounds__(AN_THREADS) k_tc_count(const unsigned long lon
     unsigned long long my_work = 0;  // list entries this group touched
     for (uint64_t ei = (uint64_t)blockIdx.x * GPC + threadIdx.x / TPV; ei < m_plus; ei += ngroups) {
         const uint32_t u = esrc[ei], v = snap[ei];
+        if (core_of && core_of[v] != GV_NIL) continue;  // counted by the core probes (group-uniform)
         const uint32_t *A = snap + off[u];
         const uint32_t la = (uint32_t)(off[u + 1] - off[u]);
         const uint32_t *Bv = snap + off[v];
@@ -871,6 +880,267 @@ __global__ void __launch_bounds__(AN_THREADS) k_tc_count(const unsigned long lon
     }
     for (uint32_t i = threadIdx.x; i < HT; i += blockDim.x)
         if (ht_key[i] != GV_NIL && ht_val[i]) atomicAdd(&tcount[ht_key[i]], ht_val[i]);
+}
+
+// ------------------------------------------------ dense-core bit probes
+// Total-only counts split the oriented edges u -> v by whether v lies in the
+// dense core K = {v : deg v > D}, D the smallest degree that leaves at most
+// core_max vertices above it.  K is an upper set of the orientation order, so
+// N+(v) lies inside K for every v in K and is kept as a bitmap row over core
+// indices.  An edge into the core counts |N+(u) & N+(v)| by testing the core
+// entries of N+(u) against v's row; a CTA stages one row in shared memory and
+// streams the core lists of a chunk of v's in-neighbours, one bit test per
+// entry.  On R-MAT graphs the core edges carry most of the merge work (a few
+// thousand hub-to-hub lists of several hundred entries), and a bit test costs
+// one shared-memory load where a merge step waits on the previous one; the
+// edges outside the core keep the merge path.
+constexpr uint32_t TCC_BINS = 65536;   // degree histogram; the last bin holds every degree above
+constexpr uint32_t TCC_CHUNK = 256;    // in-neighbours of one core vertex per work item
+constexpr uint32_t TCC_THREADS = 256;
+constexpr uint32_t TCC_DEFAULT = 65504;  // default core size bound
+constexpr uint32_t TCC_MAX = 65504;      // core indices stay below TCC_DEAD
+constexpr uint16_t TCC_DEAD = 0xFFFF;    // list padding: a bit no row sets
+constexpr uint32_t TCC_SROW = 2048;      // staged row words (holds TCC_DEAD's word)
+constexpr int TCC_UNROLL = 4;            // 16-byte loads in flight per lane
+
+struct TcCore {
+    uint32_t *hist;                 // [TCC_BINS]
+    uint32_t *cidx;                 // [n] core index or GV_NIL
+    uint32_t *ccnt;                 // [n] core entries of N+(u); then write cursors
+    unsigned long long *coff;       // [n + 1]
+    uint32_t *icnt;                 // [cmax + 1] in-neighbours per core vertex; then cursors
+    unsigned long long *ioff;       // [cmax + 1]
+    uint32_t *itcnt;                // [cmax + 1] work items per core vertex
+    uint32_t *itoff;                // [cmax + 1]
+    uint32_t *itc;                  // [items] core vertex of each work item
+    uint32_t *rows;                 // [cmax][wmax] bitmap rows
+    uint16_t *clist;                // core entries of every N+(u) as core indices, each list padded
+                                    // with TCC_DEAD to a multiple of 8 (16-byte aligned starts)
+    uint32_t *inl;                  // [m+] in-neighbours of every core vertex
+    uint32_t *ctl;                  // [0] D (GV_NIL: no core), [1] core size
+    uint32_t cmax, wmax;
+};
+
+// Degree histogram, lanes with the same bin merged before the atomic.
+__global__ void k_tcc_hist(const uint32_t *__restrict__ deg, uint32_t n, uint32_t *__restrict__ hist) {
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        const uint32_t v = base + threadIdx.x;
+        const uint32_t bin = v < n ? min(deg[v], TCC_BINS - 1) : GV_NIL;
+        const uint32_t peers = __match_any_sync(GV_FULL_MASK, bin);
+        if (bin != GV_NIL && lane == (uint32_t)(__ffs(peers) - 1)) atomicAdd(&hist[bin], __popc(peers));
+    }
+}
+
+// One CTA of 1024 threads: D = the smallest d <= TCC_BINS - 2 with
+// #{v : deg v > d} <= cmax (ctl[0]; GV_NIL when there is none or nothing
+// lies above it).  Thread t owns bins [PER r, PER (r + 1)), r = 1023 - t, so
+// the exclusive scan over threads counts the vertices in the bins above.
+__global__ void __launch_bounds__(1024) k_tcc_pick(const uint32_t *__restrict__ hist, uint32_t cmax,
+                                                   uint32_t *__restrict__ ctl) {
+    constexpr uint32_t PER = TCC_BINS / 1024;
+    __shared__ unsigned long long wtot[33];
+    __shared__ unsigned long long best;  // (d << 32) | #{deg > d}: the smallest valid d wins
+    const uint32_t t = threadIdx.x, r = 1023 - t;
+    if (t == 0) best = ~0ull;
+    unsigned long long local = 0;
+    for (uint32_t i = 0; i < PER; ++i) local += hist[PER * r + i];
+    unsigned long long tot;
+    unsigned long long s = cta_excl_scan<unsigned long long, 1024>(local, wtot, tot);  // #{deg > last bin of r}
+    unsigned long long mine = ~0ull;
+    for (int i = (int)PER - 1; i >= 0; --i) {
+        const uint32_t d = PER * r + (uint32_t)i;
+        if (d <= TCC_BINS - 2 && s <= cmax) mine = ((unsigned long long)d << 32) | s;
+        s += hist[d];
+    }
+    if (mine != ~0ull) atomicMin(&best, mine);
+    __syncthreads();
+    if (t == 0) {
+        const bool ok = best != ~0ull && (uint32_t)best != 0;
+        ctl[0] = ok ? (uint32_t)(best >> 32) : GV_NIL;
+        ctl[1] = 0;
+    }
+}
+
+// Core indices (warp-aggregated; the order does not change any count).
+__global__ void k_tcc_index(const uint32_t *__restrict__ deg, uint32_t n, uint32_t *__restrict__ ctl,
+                            uint32_t *__restrict__ cidx) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t D = ctl[0];
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        const uint32_t v = base + threadIdx.x;
+        const bool in = v < n && D != GV_NIL && deg[v] > D;
+        const uint32_t bal = __ballot_sync(GV_FULL_MASK, in);
+        uint32_t b0 = 0;
+        if (lane == 0 && bal) b0 = atomicAdd(&ctl[1], __popc(bal));
+        b0 = __shfl_sync(GV_FULL_MASK, b0, 0);
+        if (v < n) cidx[v] = in ? b0 + __popc(bal & ((1u << lane) - 1u)) : GV_NIL;
+    }
+}
+
+// Per oriented edge u -> w with w in the core: one more core entry of u and
+// one more in-neighbour of w.
+__global__ void k_tcc_count(const uint32_t *__restrict__ snap, const uint32_t *__restrict__ esrc, uint64_t m_plus,
+                            const uint32_t *__restrict__ cidx, uint32_t *__restrict__ ccnt,
+                            uint32_t *__restrict__ icnt) {
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < m_plus; base += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t e = base + threadIdx.x;
+        uint32_t c = GV_NIL, u = GV_NIL;
+        if (e < m_plus) {
+            c = cidx[snap[e]];
+            if (c != GV_NIL) u = esrc[e];
+        }
+        const uint32_t pc = __match_any_sync(GV_FULL_MASK, c);
+        if (c != GV_NIL && lane == (uint32_t)(__ffs(pc) - 1)) atomicAdd(&icnt[c], __popc(pc));
+        const uint32_t pu = __match_any_sync(GV_FULL_MASK, u);
+        if (u != GV_NIL && lane == (uint32_t)(__ffs(pu) - 1)) atomicAdd(&ccnt[u], __popc(pu));
+    }
+}
+
+// Fills the core lists, the in-neighbour lists and the bitmap rows.
+__global__ void k_tcc_fill(const uint32_t *__restrict__ snap, const uint32_t *__restrict__ esrc, uint64_t m_plus,
+                           TcCore k) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t below = (1u << lane) - 1u;
+    for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < m_plus; base += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t e = base + threadIdx.x;
+        uint32_t c = GV_NIL, u = GV_NIL;
+        if (e < m_plus) {
+            c = k.cidx[snap[e]];
+            if (c != GV_NIL) u = esrc[e];
+        }
+        const uint32_t pc = __match_any_sync(GV_FULL_MASK, c);
+        const uint32_t pu = __match_any_sync(GV_FULL_MASK, u);
+        const uint32_t lc = (uint32_t)(__ffs(pc) - 1), lu = (uint32_t)(__ffs(pu) - 1);
+        uint32_t bc = 0, bu = 0;
+        if (c != GV_NIL && lane == lc) bc = atomicAdd(&k.icnt[c], __popc(pc));
+        if (u != GV_NIL && lane == lu) bu = atomicAdd(&k.ccnt[u], __popc(pu));
+        bc = __shfl_sync(GV_FULL_MASK, bc, lc);
+        bu = __shfl_sync(GV_FULL_MASK, bu, lu);
+        if (c == GV_NIL) continue;
+        k.inl[k.ioff[c] + bc + __popc(pc & below)] = u;
+        k.clist[k.coff[u] + bu + __popc(pu & below)] = (uint16_t)c;
+        const uint32_t cu = k.cidx[u];
+        if (cu != GV_NIL) atomicOr(&k.rows[(size_t)cu * k.wmax + (c >> 5)], 1u << (c & 31));
+    }
+}
+
+// Core list lengths rounded up to a multiple of 8 entries.
+__global__ void k_tcc_pad(uint32_t *__restrict__ ccnt, uint32_t n) {
+    for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x)
+        ccnt[u] = (ccnt[u] + 7u) & ~7u;
+}
+
+__global__ void k_tcc_items(const unsigned long long *__restrict__ ioff, uint32_t cmax, uint32_t *__restrict__ itcnt) {
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < cmax; c += gridDim.x * blockDim.x)
+        itcnt[c] = (uint32_t)((ioff[c + 1] - ioff[c] + TCC_CHUNK - 1) / TCC_CHUNK);
+}
+
+// itc[i] = the core vertex of work item i (a warp per core vertex).
+__global__ void k_tcc_item_owner(const uint32_t *__restrict__ itoff, uint32_t cmax, uint32_t *__restrict__ itc) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < cmax; c += nw)
+        for (uint32_t i = itoff[c] + lane; i < itoff[c + 1]; i += 32) itc[i] = c;
+}
+
+// Bit tests of eight core entries (one 16-byte load) against the staged row.
+__device__ __forceinline__ uint32_t tcc_probe8(const uint32_t *srow, uint4 q) {
+    uint32_t h = 0;
+    const uint32_t w[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const uint32_t lo = w[i] & 0xFFFFu, hi = w[i] >> 16;
+        h += (srow[lo >> 5] >> (lo & 31)) & 1u;
+        h += (srow[hi >> 5] >> (hi & 31)) & 1u;
+    }
+    return h;
+}
+
+// Work item = up to TCC_CHUNK in-neighbours u of one core vertex v: the CTA
+// stages v's row, each warp fetches the list heads of its 32 u's at once (one
+// per lane) and walks their lists as one run of 16-byte chunks (eight
+// entries each), several loads per lane in flight.  Every triangle u < v < w
+// (orientation order) with v in the core is counted here once.
+static_assert(TCC_CHUNK == 32 * (TCC_THREADS / 32), "a warp takes one in-neighbour per lane");
+__global__ void __launch_bounds__(TCC_THREADS) k_tcc_probe(TcCore k, unsigned long long *__restrict__ total,
+                                                           unsigned long long *__restrict__ work) {
+    __shared__ uint32_t srow[TCC_SROW];
+    __shared__ unsigned long long wred[TCC_THREADS / 32][2];
+    constexpr uint32_t NWARP = TCC_THREADS / 32;
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t nitems = k.itoff[k.cmax];
+    const uint32_t W = (k.ctl[1] + 31) >> 5;  // < TCC_SROW: the padding bit's word stays 0
+    for (uint32_t i = W + threadIdx.x; i < TCC_SROW; i += TCC_THREADS) srow[i] = 0;
+    unsigned long long cnt = 0, probes = 0;
+    for (uint32_t item = blockIdx.x; item < nitems; item += gridDim.x) {
+        const uint32_t c = k.itc[item];
+        const unsigned long long j0 = k.ioff[c] + (unsigned long long)(item - k.itoff[c]) * TCC_CHUNK;
+        const unsigned long long j1 = min(k.ioff[c + 1], j0 + TCC_CHUNK);
+        // list heads of this warp's in-neighbours j0 + warp + NWARP t, t = lane
+        const unsigned long long jj = j0 + warp + (unsigned long long)NWARP * lane;
+        unsigned long long head = 0;
+        uint32_t len = 0;
+        if (jj < j1) {
+            const uint32_t u = k.inl[jj];
+            head = k.coff[u];
+            len = (uint32_t)(k.coff[u + 1] - head);
+        }
+        __syncthreads();
+        const uint32_t *row = k.rows + (size_t)c * k.wmax;
+        for (uint32_t i = threadIdx.x; i < W; i += TCC_THREADS) srow[i] = row[i];
+        __syncthreads();
+        // the warp's 32 lists as one run of 16-byte chunks: chunk q belongs to
+        // the lane t with pre_t <= q < pre_t + len_t / 8, so TCC_UNROLL loads
+        // per lane stay in flight across list boundaries
+        const uint32_t nq = len >> 3;
+        uint32_t incl = nq;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(GV_FULL_MASK, incl, o);
+            if (lane >= (uint32_t)o) incl += y;
+        }
+        const uint32_t pre = incl - nq, Q = __shfl_sync(GV_FULL_MASK, incl, 31);
+        uint32_t hits = 0;
+        for (uint32_t q0 = 0; q0 < Q; q0 += 32 * TCC_UNROLL) {
+            uint4 v[TCC_UNROLL];
+#pragma unroll
+            for (int r = 0; r < TCC_UNROLL; ++r) {
+                const uint32_t q = q0 + 32u * r + lane;
+                uint32_t t = 0;  // owner lane: the last with pre_t <= q
+#pragma unroll
+                for (uint32_t step = 16; step; step >>= 1) {
+                    const uint32_t pc = __shfl_sync(GV_FULL_MASK, pre, t + step);
+                    if (pc <= q) t += step;
+                }
+                const unsigned long long h = __shfl_sync(GV_FULL_MASK, head, t);
+                const uint32_t pt = __shfl_sync(GV_FULL_MASK, pre, t);
+                v[r] = make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu);  // eight TCC_DEAD entries
+                if (q < Q) v[r] = __ldg(reinterpret_cast<const uint4 *>(k.clist + h) + (q - pt));
+            }
+#pragma unroll
+            for (int r = 0; r < TCC_UNROLL; ++r) hits += tcc_probe8(srow, v[r]);
+        }
+        const uint32_t seen = Q * 8;
+        cnt += hits;
+        probes += seen;  // the same in every lane of the warp
+    }
+    cnt = warp_sum(cnt);
+    if (lane == 0) {
+        wred[warp][0] = cnt;
+        wred[warp][1] = probes;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long t = 0, p = 0;
+        for (uint32_t i = 0; i < NWARP; ++i) {
+            t += wred[i][0];
+            p += wred[i][1];
+        }
+        if (t) atomicAdd(total, t);
+        if (p) atomicAdd(work, p);
+    }
 }
 
 // ------------------------------------------------ hash-probe intersection
@@ -1264,6 +1534,84 @@ struct TcBufs {
     unsigned long long *hcur;  // per-hub write cursors
 };
 
+// Core size bound of the total-only count: GV_TC_CORE=<vertices> (0: merge
+// every edge), rounded down to a multiple of 32, at most TCC_MAX (core
+// indices are 16-bit and leave TCC_DEAD free).
+uint32_t tc_core_max() {
+    const char *env = std::getenv("GV_TC_CORE");
+    long v = env ? std::strtol(env, nullptr, 10) : (long)TCC_DEFAULT;
+    v = std::max<long>(0, std::min<long>(v, (long)TCC_MAX));
+    return (uint32_t)v & ~31u;
+}
+
+// Dense-core probes of a total-only count: picks the core, builds its rows,
+// core lists and in-neighbour lists in auxiliary slot 10 and adds the core
+// edges' triangles into tcount[0].  *core_of receives the core index array
+// the merge kernel skips by.  No host synchronisation.
+gv_status tc_core(gv_graph *g, const TcBufs &b, uint64_t mplus, uint32_t cmax, unsigned long long *work,
+                  const uint32_t **core_of, cudaStream_t s) {
+    const uint32_t n = g->d.n;
+    const uint32_t wmax = (cmax + 31) / 32;
+    auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+    const size_t o_hist = 0, o_ctl = o_hist + al((size_t)TCC_BINS * 4), o_cidx = o_ctl + 256;
+    const size_t o_ccnt = o_cidx + al((size_t)n * 4), o_coff = o_ccnt + al((size_t)n * 4);
+    const size_t o_icnt = o_coff + al(((size_t)n + 1) * 8), o_ioff = o_icnt + al(((size_t)cmax + 1) * 4);
+    const size_t o_itcnt = o_ioff + al(((size_t)cmax + 1) * 8), o_itoff = o_itcnt + al(((size_t)cmax + 1) * 4);
+    const size_t o_rows = o_itoff + al(((size_t)cmax + 1) * 4), o_clist = o_rows + al((size_t)cmax * wmax * 4);
+    const size_t o_inl = o_clist + al(((size_t)mplus + 8 * (size_t)n) * 2), o_itc = o_inl + al((size_t)mplus * 4);
+    const size_t max_items = (size_t)mplus / TCC_CHUNK + cmax + 1;  // sum of ceil(in-degree / chunk)
+    const size_t bytes = o_itc + al(max_items * 4);
+    char *p = (char *)aux_scratch(g, 10, bytes);
+    if (!p) return GV_ERR_NOMEM;
+    TcCore k;
+    k.hist = (uint32_t *)(p + o_hist);
+    k.ctl = (uint32_t *)(p + o_ctl);
+    k.cidx = (uint32_t *)(p + o_cidx);
+    k.ccnt = (uint32_t *)(p + o_ccnt);
+    k.coff = (unsigned long long *)(p + o_coff);
+    k.icnt = (uint32_t *)(p + o_icnt);
+    k.ioff = (unsigned long long *)(p + o_ioff);
+    k.itcnt = (uint32_t *)(p + o_itcnt);
+    k.itoff = (uint32_t *)(p + o_itoff);
+    k.rows = (uint32_t *)(p + o_rows);
+    k.clist = (uint16_t *)(p + o_clist);
+    k.inl = (uint32_t *)(p + o_inl);
+    k.itc = (uint32_t *)(p + o_itc);
+    k.cmax = cmax;
+    k.wmax = wmax;
+    const uint32_t *deg = b.hubs;  // live degrees, as the orientation used them
+    {
+        ProfScope ps(PROF_TC_CORE, s);
+        cudaMemsetAsync(k.hist, 0, (size_t)TCC_BINS * 4, s);
+        cudaMemsetAsync(k.ccnt, 0, (size_t)n * 4, s);
+        cudaMemsetAsync(k.icnt, 0, ((size_t)cmax + 1) * 4, s);
+        cudaMemsetAsync(k.rows, 0, (size_t)cmax * wmax * 4, s);
+        GV_LAUNCH(k_tcc_hist, grid_for(n, 256), 256, 0, s, deg, n, k.hist);
+        GV_LAUNCH(k_tcc_pick, 1, 1024, 0, s, (const uint32_t *)k.hist, cmax, k.ctl);
+        GV_LAUNCH(k_tcc_index, grid_for(n, 256), 256, 0, s, deg, n, k.ctl, k.cidx);
+        const unsigned egrid = grid_for(mplus, 256, 148 * 16);
+        GV_LAUNCH(k_tcc_count, egrid, 256, 0, s, (const uint32_t *)b.snap, (const uint32_t *)b.esrc, mplus,
+                  (const uint32_t *)k.cidx, k.ccnt, k.icnt);
+        GV_LAUNCH(k_tcc_pad, grid_for(n, 256), 256, 0, s, k.ccnt, n);
+        scan_exclusive_u32_to_u64(k.ccnt, k.coff, n, k.coff + n, g->bs.scan_tmp, s);
+        cudaMemsetAsync(k.clist, 0xFF, ((size_t)mplus + 8 * (size_t)n) * 2, s);  // padding = TCC_DEAD
+        scan_exclusive_u32_to_u64(k.icnt, k.ioff, cmax, k.ioff + cmax, g->bs.scan_tmp, s);
+        cudaMemsetAsync(k.ccnt, 0, (size_t)n * 4, s);
+        cudaMemsetAsync(k.icnt, 0, ((size_t)cmax + 1) * 4, s);
+        GV_LAUNCH(k_tcc_fill, egrid, 256, 0, s, (const uint32_t *)b.snap, (const uint32_t *)b.esrc, mplus, k);
+        GV_LAUNCH(k_tcc_items, grid_for(cmax, 256), 256, 0, s, (const unsigned long long *)k.ioff, cmax, k.itcnt);
+        scan_exclusive_u32(k.itcnt, k.itoff, cmax, k.itoff + cmax, g->bs.scan_tmp, s);
+        GV_LAUNCH(k_tcc_item_owner, grid_for(cmax, 8), 256, 0, s, (const uint32_t *)k.itoff, cmax, k.itc);
+    }
+    {
+        ProfScope ps(PROF_TC_PROBE, s);
+        GV_LAUNCH(k_tcc_probe, 148 * 8, TCC_THREADS, 0, s, k, b.tcount, work + 1);
+    }
+    cudaMemcpyAsync(work + 2, k.ctl + 1, 4, cudaMemcpyDeviceToDevice, s);  // core size (low word)
+    *core_of = k.cidx;
+    return cuda_status(cudaGetLastError(), "tc core");
+}
+
 // Builds the oriented sorted snapshot and counts.  tcount[n] receives the
 // per-vertex counts (owner or incident).  Returns m_plus via *mplus.
 gv_status tc_run(gv_graph *g, cudaStream_t s, int mode, unsigned long long **tcount_out) {
@@ -1338,7 +1686,7 @@ gv_status tc_run(gv_graph *g, cudaStream_t s, int mode, unsigned long long **tco
     }
     // per-graph word (views own theirs), so concurrent counts on views do not share it
     unsigned long long *work = (unsigned long long *)g->bs.tile_cnt + 1;
-    cudaMemsetAsync(work, 0, 8, s);
+    cudaMemsetAsync(work, 0, 24, s);  // merged entries, core probes, core vertices
     const char *packed_env = std::getenv("GV_TC_PACKED");
     if (packed_env && packed_env[0] == '1') {
         // packed hash probe: lists unsorted, u with d+ > TCP_LIGHT to one CTA each
@@ -1381,42 +1729,52 @@ gv_status tc_run(gv_graph *g, cudaStream_t s, int mode, unsigned long long **tco
         *tcount_out = b.tcount;
         return cuda_status(cudaGetLastError(), "tc launch");
     }
-    // merge path (default): sorted lists, merge-path intersection per oriented edge
-    GV_LAUNCH(k_tc_classify, grid_for(n, 256), 256, 0, s, (const unsigned long long *)b.off, n, b.snap, b.mid, b.big,
-              b.cnts);
-    GV_LAUNCH(k_tc_sort_mid, 148 * 4, AN_THREADS, 0, s, (const unsigned long long *)b.off, b.snap,
-              (const uint32_t *)b.mid, (const unsigned long long *)b.cnts);
-    // longest list bounds the CTA sort's shared memory
-    unsigned long long h[2] = {0, 0};
-    cudaMemcpyAsync(h, b.cnts, 16, cudaMemcpyDeviceToHost, s);
-    cudaError_t e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) return cuda_status(e, "tc");
-    if (h[1]) {  // lists above 1024 entries: one CTA sort each
-        std::vector<uint32_t> bl(h[1]);
-        std::vector<unsigned long long> hoff(n + 1);
-        cudaMemcpy(hoff.data(), b.off, ((size_t)n + 1) * 8, cudaMemcpyDeviceToHost);
-        cudaMemcpy(bl.data(), b.big, h[1] * 4, cudaMemcpyDeviceToHost);
-        uint64_t mx = 0;
-        for (uint32_t u : bl) mx = std::max<uint64_t>(mx, hoff[u + 1] - hoff[u]);
-        uint32_t P = 1024;
-        while (P < mx) P <<= 1;
-        const size_t smem = (size_t)P * 4;
-        if (smem > 227 * 1024) { set_error("oriented out-degree exceeds the shared-memory sort"); return GV_ERR_UNSUPPORTED; }
-        cudaFuncSetAttribute(k_tc_sort_big, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        GV_LAUNCH(k_tc_sort_big, 148, 1024, smem, s, (const unsigned long long *)b.off, b.snap,
-                  (const uint32_t *)b.big, (const unsigned long long *)b.cnts, P);
+    // merge path (default): sorted lists, merge-path intersection per oriented
+    // edge; for total-only counts the edges into the dense core go to bit
+    // probes first, and the core's own lists (read by no merge) stay unsorted
+    GV_LAUNCH(k_tc_esrc, grid_for(n, 256), 256, 0, s, (const unsigned long long *)b.off, n, b.esrc);
+    const uint32_t *core_of = nullptr;
+    if (mode == TC_TOTAL && mplus) {
+        const uint32_t cmax = std::min<uint32_t>(tc_core_max(), n);
+        if (cmax) {
+            gv_status st = tc_core(g, b, mplus, cmax, work, &core_of, s);
+            if (st != GV_OK) return st;
+        }
     }
     {
-        GV_LAUNCH(k_tc_esrc, grid_for(n, 256), 256, 0, s, (const unsigned long long *)b.off, n, b.esrc);
+        ProfScope ps(PROF_TC_SORT, s);
+        GV_LAUNCH(k_tc_classify, grid_for(n, 256), 256, 0, s, (const unsigned long long *)b.off, n, b.snap, b.mid,
+                  b.big, b.cnts, core_of);
+        GV_LAUNCH(k_tc_sort_mid, 148 * 4, AN_THREADS, 0, s, (const unsigned long long *)b.off, b.snap,
+                  (const uint32_t *)b.mid, (const unsigned long long *)b.cnts);
+        // the longest list bounds the CTA sort's shared memory
+        unsigned long long h[3] = {0, 0, 0};
+        cudaMemcpyAsync(h, b.cnts, 24, cudaMemcpyDeviceToHost, s);
+        cudaError_t e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return cuda_status(e, "tc");
+        if (h[1]) {  // lists above 1024 entries: one CTA sort each
+            uint32_t P = 1024;
+            while (P < h[2]) P <<= 1;
+            const size_t smem = (size_t)P * 4;
+            if (smem > 227 * 1024) { set_error("oriented out-degree exceeds the shared-memory sort"); return GV_ERR_UNSUPPORTED; }
+            cudaFuncSetAttribute(k_tc_sort_big, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            GV_LAUNCH(k_tc_sort_big, 148, 1024, smem, s, (const unsigned long long *)b.off, b.snap,
+                      (const uint32_t *)b.big, (const unsigned long long *)b.cnts, P);
+        }
+    }
+    {
         const unsigned cgrid = grid_for(mplus, AN_THREADS / 8, 148 * 16);
         ProfScope ps(PROF_TC_COUNT, s);
         const unsigned long long *off_c = b.off;
         if (mode == TC_INCIDENT)
-            GV_LAUNCH((k_tc_count<8, TC_INCIDENT>), cgrid, AN_THREADS, 0, s, off_c, b.snap, b.esrc, mplus, b.tcount, work);
+            GV_LAUNCH((k_tc_count<8, TC_INCIDENT>), cgrid, AN_THREADS, 0, s, off_c, b.snap, b.esrc, mplus, b.tcount, work,
+                      (const uint32_t *)nullptr);
         else if (mode == TC_TOTAL)
-            GV_LAUNCH((k_tc_count<8, TC_TOTAL>), cgrid, AN_THREADS, 0, s, off_c, b.snap, b.esrc, mplus, b.tcount, work);
+            GV_LAUNCH((k_tc_count<8, TC_TOTAL>), cgrid, AN_THREADS, 0, s, off_c, b.snap, b.esrc, mplus, b.tcount, work,
+                      core_of);
         else
-            GV_LAUNCH((k_tc_count<8, TC_OWNER>), cgrid, AN_THREADS, 0, s, off_c, b.snap, b.esrc, mplus, b.tcount, work);
+            GV_LAUNCH((k_tc_count<8, TC_OWNER>), cgrid, AN_THREADS, 0, s, off_c, b.snap, b.esrc, mplus, b.tcount, work,
+                      (const uint32_t *)nullptr);
     }
     g->last_tc_oriented = mplus;
     *tcount_out = b.tcount;

@@ -127,7 +127,7 @@ gv_status ensure_batch_scratch(gv_graph *g, uint64_t entries, uint64_t pairs) {
         }
         if ((st = dmalloc(&bs.rs_counts, radix_counts_elems(E) * 4 + 16, "rs_counts")) != GV_OK) goto fail;
         if ((st = dmalloc((char **)&bs.scan_tmp, scan_scratch_bytes(scan_elems), "scan")) != GV_OK) goto fail;
-        if ((st = dmalloc(&bs.tile_cnt, nseg_tiles * 8, "tile_cnt")) != GV_OK) goto fail;
+        if ((st = dmalloc(&bs.tile_cnt, std::max<uint64_t>(nseg_tiles, 8) * 8, "tile_cnt")) != GV_OK) goto fail;
         if ((st = dmalloc(&bs.bdst, E * 4, "bdst")) != GV_OK) goto fail;
         if ((st = dmalloc(&bs.found, E, "found")) != GV_OK) goto fail;
         if ((st = dmalloc(&bs.seg_vertex, E * 4, "seg_vertex")) != GV_OK) goto fail;
@@ -201,7 +201,8 @@ gv_status read_ctl(gv_graph *g, Ctl *out, cudaStream_t s) {
 namespace {
 const char *const kProfNames[PROF_NSLOTS] = {"radix", "segment", "member", "apply", "compact",
                                              "pull", "tc_snapshot", "tc_count", "bfs_level", "bc_dep",
-                                             "wpr_build", "wpr_sweep", "wpr_grad"};
+                                             "wpr_build", "wpr_sweep", "wpr_grad", "tc_core",
+                                             "tc_probe", "tc_sort"};
 struct ProfRec {
     int slot;
     cudaEvent_t a, b;
@@ -756,15 +757,19 @@ gv_status gv_clear_affected(gv_graph *g, void *stream) {
 gv_status gv_last_stat(gv_graph *g, const char *key, double *value) {
     if (!g || !key || !value) return GV_ERR_INVALID;
     DeviceGuard dg(g->cfg.device);
-    if (std::strcmp(key, "tc_work") == 0 || std::strcmp(key, "tc_oriented_edges") == 0) {
+    if (std::strcmp(key, "tc_work") == 0 || std::strcmp(key, "tc_oriented_edges") == 0 ||
+        std::strcmp(key, "tc_probes") == 0 || std::strcmp(key, "tc_core") == 0) {
         if (key[3] == 'o') {
             *value = (double)g->last_tc_oriented;
             return GV_OK;
         }
-        unsigned long long w = 0;  // work counter of the last count (per-graph scratch word)
-        cudaError_t e = cudaMemcpy(&w, (unsigned long long *)g->bs.tile_cnt + 1, 8, cudaMemcpyDeviceToHost);
+        // work counters of the last count (per-graph scratch words): [1] merged
+        // entries, [2] core bit probes, [3] core vertices
+        const int word = key[3] == 'w' ? 1 : key[4] == 'r' ? 2 : 3;
+        unsigned long long w = 0;
+        cudaError_t e = cudaMemcpy(&w, (unsigned long long *)g->bs.tile_cnt + word, 8, cudaMemcpyDeviceToHost);
         if (e == cudaSuccess) *value = (double)w;
-        return cuda_status(e, "tc_work");
+        return cuda_status(e, key);
     }
     if (std::strcmp(key, "tc_subset_local") == 0) {
         *value = (double)g->last_tc_local;

@@ -21,6 +21,9 @@ enum ProfSlot {
     PROF_WPR_BUILD,
     PROF_WPR_SWEEP,
     PROF_WPR_GRAD,
+    PROF_TC_CORE,
+    PROF_TC_PROBE,
+    PROF_TC_SORT,
     PROF_NSLOTS
 };
 

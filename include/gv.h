@@ -180,9 +180,10 @@ gv_status gv_check(gv_graph *g, uint64_t *violations, uint32_t *first_code,
 /* Facts about the last analytics call on this graph: "tc_work" = list
  * entries the last whole-graph triangle count read (|N+(u)| + |N+(v)| merged
  * per oriented edge; with GV_TC_PACKED=1 probes of N+(v) plus inserts of
- * N+(u)), "tc_oriented_edges", "tc_subset_local" (1 if the last
- * subset count took the neighbour-hash path), "sweeps" (last PageRank).
- * Synchronous. */
+ * N+(u)), "tc_probes" / "tc_core" (bit probes against the dense-core rows
+ * and core vertices of the last total-only count; 0 when it merged every
+ * edge), "tc_oriented_edges", "tc_subset_local" (1 if the last subset count
+ * took the neighbour-hash path), "sweeps" (last PageRank).  Synchronous. */
 gv_status gv_last_stat(gv_graph *g, const char *key, double *value);
 
 /* ---- analytics ---------------------------------------------------------- */

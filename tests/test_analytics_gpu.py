@@ -305,6 +305,56 @@ def test_triangle_paths_total_only_and_incident(packed, monkeypatch, graph12):
     assert np.array_equal(g.tc_subset(sub), o.tc_incident(sub))
 
 
+@pytest.mark.parametrize("core", ["0", "64", "1000", "32768"])
+def test_total_triangles_dense_core(core, monkeypatch, graph12):
+    """Total-only counts with the dense-core bit probes: no core (every edge
+    merged), a core of 64 or 1000 vertices (edges split between probes and
+    merges) and the default bound (every vertex with an edge in the core)."""
+    n, g, o = graph12
+    monkeypatch.setenv("GV_TC_CORE", core)
+    _, otot = o.tc()
+    _, tot = g.static_tc(per_vertex=False)
+    assert tot == otot
+    probes, csize = g.last_stat("tc_probes"), g.last_stat("tc_core")
+    if core == "0":
+        assert probes == 0 and csize == 0
+    else:
+        assert probes > 0 and 0 < csize <= int(core)
+    # after tombstones and compaction
+    off, dst, _ = o.export()
+    es, ed = sample_existing(off, dst, 3000, np.random.default_rng(int(core) + 1))
+    g2 = make_graph(n)
+    s0, d0 = rmat_graph(12, 16, seed=21)  # the pairs of graph12
+    g2.batch_insert(s0, d0)
+    g2.batch_delete(es, ed)
+    o2 = oracle.OracleGraph(n)
+    o2.insert(s0, d0)
+    o2.delete(es, ed)
+    assert g2.static_tc(per_vertex=False)[1] == o2.tc()[1]
+    g2.compaction()
+    assert g2.static_tc(per_vertex=False)[1] == o2.tc()[1]
+    g2.close()
+
+
+def test_total_triangles_core_with_hub_clique(monkeypatch):
+    """A 1100-clique inside an R-MAT graph: the clique members form the core
+    and their rows hold 1099-entry lists."""
+    monkeypatch.setenv("GV_TC_CORE", "2048")
+    n = 1 << 13
+    K = 1100
+    iu, ju = np.triu_indices(K, 1)
+    perm = np.random.default_rng(6).permutation(n)[:K].astype(np.uint32)
+    rs, rd = rmat_graph(13, 4, seed=9)
+    s = np.concatenate([perm[iu], rs])
+    d = np.concatenate([perm[ju], rd])
+    g = make_graph(n)
+    g.batch_insert(s, d)
+    o = oracle.OracleGraph(n)
+    o.insert(s, d)
+    assert g.static_tc(per_vertex=False)[1] == o.tc()[1]
+    assert g.last_stat("tc_core") > 0
+
+
 def test_wpr_forward_hub_in_edges_and_repeatable():
     """A vertex with 3000 in-edges takes the CTA-per-vertex sweep; the sorted
     in-edge transpose makes two calls bit-for-bit equal."""
