@@ -751,7 +751,8 @@ __global__ void __launch_bounds__(AN_THREADS) k_tc_count(const unsigned long lon
                                                          const uint32_t *__restrict__ esrc, uint64_t m_plus,
                                                          unsigned long long *__restrict__ tcount,
                                                          unsigned long long *__restrict__ work,
-                                                         const uint32_t *__restrict__ core_of) {
+                                                         const uint32_t *__restrict__ elist,
+                                                         const uint32_t *__restrict__ ecount) {
     constexpr int GPC = AN_THREADS / TPV;
     constexpr uint32_t HT = 2048;  // per-CTA credit table: hubs collect many credits
     __shared__ unsigned long long wred[AN_THREADS / 32];
@@ -778,9 +779,12 @@ __global__ void __launch_bounds__(AN_THREADS) k_tc_count(const unsigned long lon
     Group<TPV> G;
     const uint64_t ngroups = (uint64_t)gridDim.x * GPC;
     unsigned long long my_work = 0;  // list entries this group touched
-    for (uint64_t ei = (uint64_t)blockIdx.x * GPC + threadIdx.x / TPV; ei < m_plus; ei += ngroups) {
+    // every oriented edge, or only those listed in elist[0, *ecount) (the
+    // edges the core probes leave)
+    const uint64_t nedges = elist ? (uint64_t)*ecount : m_plus;
+    for (uint64_t i = (uint64_t)blockIdx.x * GPC + threadIdx.x / TPV; i < nedges; i += ngroups) {
+        const uint64_t ei = elist ? (uint64_t)elist[i] : i;
         const uint32_t u = esrc[ei], v = snap[ei];
-        if (core_of && core_of[v] != GV_NIL) continue;  // counted by the core probes (group-uniform)
         const uint32_t *A = snap + off[u];
         const uint32_t la = (uint32_t)(off[u + 1] - off[u]);
         const uint32_t *Bv = snap + off[v];
@@ -917,7 +921,8 @@ struct TcCore {
     uint16_t *clist;                // core entries of every N+(u) as core indices, each list padded
                                     // with TCC_DEAD to a multiple of 8 (16-byte aligned starts)
     uint32_t *inl;                  // [m+] in-neighbours of every core vertex
-    uint32_t *ctl;                  // [0] D (GV_NIL: no core), [1] core size
+    uint32_t *ctl;                  // [0] D (GV_NIL: no core), [1] core size, [2] rest edges
+    uint32_t *rest;                 // [m+] oriented edges outside the core, for the merge
     uint32_t cmax, wmax;
 };
 
@@ -959,6 +964,7 @@ __global__ void __launch_bounds__(1024) k_tcc_pick(const uint32_t *__restrict__ 
         const bool ok = best != ~0ull && (uint32_t)best != 0;
         ctl[0] = ok ? (uint32_t)(best >> 32) : GV_NIL;
         ctl[1] = 0;
+        ctl[2] = 0;
     }
 }
 
@@ -979,10 +985,10 @@ __global__ void k_tcc_index(const uint32_t *__restrict__ deg, uint32_t n, uint32
 }
 
 // Per oriented edge u -> w with w in the core: one more core entry of u and
-// one more in-neighbour of w.
+// one more in-neighbour of w; every other edge goes to the merge list.
 __global__ void k_tcc_count(const uint32_t *__restrict__ snap, const uint32_t *__restrict__ esrc, uint64_t m_plus,
                             const uint32_t *__restrict__ cidx, uint32_t *__restrict__ ccnt,
-                            uint32_t *__restrict__ icnt) {
+                            uint32_t *__restrict__ icnt, uint32_t *__restrict__ rest, uint32_t *__restrict__ nrest) {
     const uint32_t lane = threadIdx.x & 31u;
     for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < m_plus; base += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t e = base + threadIdx.x;
@@ -991,6 +997,11 @@ __global__ void k_tcc_count(const uint32_t *__restrict__ snap, const uint32_t *_
             c = cidx[snap[e]];
             if (c != GV_NIL) u = esrc[e];
         }
+        const uint32_t br = __ballot_sync(GV_FULL_MASK, e < m_plus && c == GV_NIL);
+        uint32_t r0 = 0;
+        if (lane == 0 && br) r0 = atomicAdd(nrest, __popc(br));
+        r0 = __shfl_sync(GV_FULL_MASK, r0, 0);
+        if (e < m_plus && c == GV_NIL) rest[r0 + __popc(br & ((1u << lane) - 1u))] = (uint32_t)e;
         const uint32_t pc = __match_any_sync(GV_FULL_MASK, c);
         if (c != GV_NIL && lane == (uint32_t)(__ffs(pc) - 1)) atomicAdd(&icnt[c], __popc(pc));
         const uint32_t pu = __match_any_sync(GV_FULL_MASK, u);
@@ -1102,6 +1113,10 @@ __global__ void __launch_bounds__(TCC_THREADS) k_tcc_probe(TcCore k, unsigned lo
             if (lane >= (uint32_t)o) incl += y;
         }
         const uint32_t pre = incl - nq, Q = __shfl_sync(GV_FULL_MASK, incl, 31);
+        // chunk q of the run is chunk base_t + q of the list array (mod 2^32:
+        // the list array holds fewer than 2^32 chunks)
+        const uint32_t base = (uint32_t)(head >> 3) - pre;
+        const uint4 *clist4 = reinterpret_cast<const uint4 *>(k.clist);
         uint32_t hits = 0;
         for (uint32_t q0 = 0; q0 < Q; q0 += 32 * TCC_UNROLL) {
             uint4 v[TCC_UNROLL];
@@ -1114,10 +1129,9 @@ __global__ void __launch_bounds__(TCC_THREADS) k_tcc_probe(TcCore k, unsigned lo
                     const uint32_t pc = __shfl_sync(GV_FULL_MASK, pre, t + step);
                     if (pc <= q) t += step;
                 }
-                const unsigned long long h = __shfl_sync(GV_FULL_MASK, head, t);
-                const uint32_t pt = __shfl_sync(GV_FULL_MASK, pre, t);
+                const uint32_t bt = __shfl_sync(GV_FULL_MASK, base, t);
                 v[r] = make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu);  // eight TCC_DEAD entries
-                if (q < Q) v[r] = __ldg(reinterpret_cast<const uint4 *>(k.clist + h) + (q - pt));
+                if (q < Q) v[r] = __ldg(clist4 + (bt + q));
             }
 #pragma unroll
             for (int r = 0; r < TCC_UNROLL; ++r) hits += tcc_probe8(srow, v[r]);
@@ -1544,12 +1558,9 @@ uint32_t tc_core_max() {
     return (uint32_t)v & ~31u;
 }
 
-// Dense-core probes of a total-only count: picks the core, builds its rows,
-// core lists and in-neighbour lists in auxiliary slot 10 and adds the core
-// edges' triangles into tcount[0].  *core_of receives the core index array
-// the merge kernel skips by.  No host synchronisation.
-gv_status tc_core(gv_graph *g, const TcBufs &b, uint64_t mplus, uint32_t cmax, unsigned long long *work,
-                  const uint32_t **core_of, cudaStream_t s) {
+// Dense core of a total-only count, first half: carves the core buffers from
+// auxiliary slot 10 and picks the core (k.cidx).  No host synchronisation.
+gv_status tc_core_select(gv_graph *g, const TcBufs &b, uint64_t mplus, uint32_t cmax, TcCore &k, cudaStream_t s) {
     const uint32_t n = g->d.n;
     const uint32_t wmax = (cmax + 31) / 32;
     auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
@@ -1560,10 +1571,9 @@ gv_status tc_core(gv_graph *g, const TcBufs &b, uint64_t mplus, uint32_t cmax, u
     const size_t o_rows = o_itoff + al(((size_t)cmax + 1) * 4), o_clist = o_rows + al((size_t)cmax * wmax * 4);
     const size_t o_inl = o_clist + al(((size_t)mplus + 8 * (size_t)n) * 2), o_itc = o_inl + al((size_t)mplus * 4);
     const size_t max_items = (size_t)mplus / TCC_CHUNK + cmax + 1;  // sum of ceil(in-degree / chunk)
-    const size_t bytes = o_itc + al(max_items * 4);
+    const size_t o_rest = o_itc + al(max_items * 4), bytes = o_rest + al((size_t)mplus * 4);
     char *p = (char *)aux_scratch(g, 10, bytes);
     if (!p) return GV_ERR_NOMEM;
-    TcCore k;
     k.hist = (uint32_t *)(p + o_hist);
     k.ctl = (uint32_t *)(p + o_ctl);
     k.cidx = (uint32_t *)(p + o_cidx);
@@ -1577,6 +1587,7 @@ gv_status tc_core(gv_graph *g, const TcBufs &b, uint64_t mplus, uint32_t cmax, u
     k.clist = (uint16_t *)(p + o_clist);
     k.inl = (uint32_t *)(p + o_inl);
     k.itc = (uint32_t *)(p + o_itc);
+    k.rest = (uint32_t *)(p + o_rest);
     k.cmax = cmax;
     k.wmax = wmax;
     const uint32_t *deg = b.hubs;  // live degrees, as the orientation used them
@@ -1589,9 +1600,22 @@ gv_status tc_core(gv_graph *g, const TcBufs &b, uint64_t mplus, uint32_t cmax, u
         GV_LAUNCH(k_tcc_hist, grid_for(n, 256), 256, 0, s, deg, n, k.hist);
         GV_LAUNCH(k_tcc_pick, 1, 1024, 0, s, (const uint32_t *)k.hist, cmax, k.ctl);
         GV_LAUNCH(k_tcc_index, grid_for(n, 256), 256, 0, s, deg, n, k.ctl, k.cidx);
+    }
+    return cuda_status(cudaGetLastError(), "tc core");
+}
+
+// Second half, once the lists outside the core are sorted: builds the rows,
+// core lists, in-neighbour lists and the list of edges left to the merge
+// (k.rest, count k.ctl[2]), then adds the core edges' triangles into
+// tcount[0].  No host synchronisation.
+gv_status tc_core_count(gv_graph *g, const TcBufs &b, uint64_t mplus, TcCore &k, unsigned long long *work,
+                        cudaStream_t s) {
+    const uint32_t n = g->d.n, cmax = k.cmax;
+    {
+        ProfScope ps(PROF_TC_CORE, s);
         const unsigned egrid = grid_for(mplus, 256, 148 * 16);
         GV_LAUNCH(k_tcc_count, egrid, 256, 0, s, (const uint32_t *)b.snap, (const uint32_t *)b.esrc, mplus,
-                  (const uint32_t *)k.cidx, k.ccnt, k.icnt);
+                  (const uint32_t *)k.cidx, k.ccnt, k.icnt, k.rest, k.ctl + 2);
         GV_LAUNCH(k_tcc_pad, grid_for(n, 256), 256, 0, s, k.ccnt, n);
         scan_exclusive_u32_to_u64(k.ccnt, k.coff, n, k.coff + n, g->bs.scan_tmp, s);
         cudaMemsetAsync(k.clist, 0xFF, ((size_t)mplus + 8 * (size_t)n) * 2, s);  // padding = TCC_DEAD
@@ -1608,7 +1632,6 @@ gv_status tc_core(gv_graph *g, const TcBufs &b, uint64_t mplus, uint32_t cmax, u
         GV_LAUNCH(k_tcc_probe, 148 * 8, TCC_THREADS, 0, s, k, b.tcount, work + 1);
     }
     cudaMemcpyAsync(work + 2, k.ctl + 1, 4, cudaMemcpyDeviceToDevice, s);  // core size (low word)
-    *core_of = k.cidx;
     return cuda_status(cudaGetLastError(), "tc core");
 }
 
@@ -1733,14 +1756,15 @@ gv_status tc_run(gv_graph *g, cudaStream_t s, int mode, unsigned long long **tco
     // edge; for total-only counts the edges into the dense core go to bit
     // probes first, and the core's own lists (read by no merge) stay unsorted
     GV_LAUNCH(k_tc_esrc, grid_for(n, 256), 256, 0, s, (const unsigned long long *)b.off, n, b.esrc);
-    const uint32_t *core_of = nullptr;
-    if (mode == TC_TOTAL && mplus) {
-        const uint32_t cmax = std::min<uint32_t>(tc_core_max(), n);
-        if (cmax) {
-            gv_status st = tc_core(g, b, mplus, cmax, work, &core_of, s);
-            if (st != GV_OK) return st;
-        }
+    // the core is picked first: its lists are read by no merge and stay unsorted
+    TcCore core{};
+    const bool use_core = mode == TC_TOTAL && mplus && mplus < (1ull << 32) &&  // merge-list edge ids are 32-bit
+                          std::min<uint32_t>(tc_core_max(), n) > 0;
+    if (use_core) {
+        gv_status st = tc_core_select(g, b, mplus, std::min<uint32_t>(tc_core_max(), n), core, s);
+        if (st != GV_OK) return st;
     }
+    const uint32_t *core_of = use_core ? core.cidx : nullptr;
     {
         ProfScope ps(PROF_TC_SORT, s);
         GV_LAUNCH(k_tc_classify, grid_for(n, 256), 256, 0, s, (const unsigned long long *)b.off, n, b.snap, b.mid,
@@ -1762,19 +1786,26 @@ gv_status tc_run(gv_graph *g, cudaStream_t s, int mode, unsigned long long **tco
                       (const uint32_t *)b.big, (const unsigned long long *)b.cnts, P);
         }
     }
+    const uint32_t *rest = nullptr, *nrest = nullptr;
+    if (use_core) {
+        gv_status st = tc_core_count(g, b, mplus, core, work, s);
+        if (st != GV_OK) return st;
+        rest = core.rest;
+        nrest = core.ctl + 2;
+    }
     {
         const unsigned cgrid = grid_for(mplus, AN_THREADS / 8, 148 * 16);
         ProfScope ps(PROF_TC_COUNT, s);
         const unsigned long long *off_c = b.off;
         if (mode == TC_INCIDENT)
             GV_LAUNCH((k_tc_count<8, TC_INCIDENT>), cgrid, AN_THREADS, 0, s, off_c, b.snap, b.esrc, mplus, b.tcount, work,
-                      (const uint32_t *)nullptr);
+                      (const uint32_t *)nullptr, (const uint32_t *)nullptr);
         else if (mode == TC_TOTAL)
             GV_LAUNCH((k_tc_count<8, TC_TOTAL>), cgrid, AN_THREADS, 0, s, off_c, b.snap, b.esrc, mplus, b.tcount, work,
-                      core_of);
+                      rest, nrest);
         else
             GV_LAUNCH((k_tc_count<8, TC_OWNER>), cgrid, AN_THREADS, 0, s, off_c, b.snap, b.esrc, mplus, b.tcount, work,
-                      (const uint32_t *)nullptr);
+                      (const uint32_t *)nullptr, (const uint32_t *)nullptr);
     }
     g->last_tc_oriented = mplus;
     *tcount_out = b.tcount;

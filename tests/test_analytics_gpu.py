@@ -325,7 +325,9 @@ def test_total_triangles_dense_core(core, monkeypatch, graph12):
     es, ed = sample_existing(off, dst, 3000, np.random.default_rng(int(core) + 1))
     g2 = make_graph(n)
     s0, d0 = rmat_graph(12, 16, seed=21)  # the pairs of graph12
-    g2.batch_insert(s0, d0)
+    perm = np.random.default_rng(int(core) + 2).permutation(len(s0))
+    for part in np.array_split(perm, 4):  # batches in shuffled order leave the lists unsorted
+        g2.batch_insert(s0[part], d0[part])
     g2.batch_delete(es, ed)
     o2 = oracle.OracleGraph(n)
     o2.insert(s0, d0)
