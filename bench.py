@@ -718,8 +718,10 @@ def run_gv(args, rank, world, local_rank):
     m_now = g.num_edges()
     try:
         tc_work = g.last_stat("tc_work")
+        tc_probes = g.last_stat("tc_probes")
+        tc_core = g.last_stat("tc_core")
     except Exception:
-        tc_work = None
+        tc_work = tc_probes = tc_core = None
     prof = {s: gv_b200.profile_query(s) for s in gv_b200.PROFILE_SLOTS}
 
     # e2e: same steps through the C-ABI with pinned host buffers
@@ -794,7 +796,10 @@ def run_gv(args, rank, world, local_rank):
         unit_note = "4*m + 12*n bytes per sweep"
     elif dom == "tc_count" and tc_work:
         alg = 4 * tc_work  # merged list entries, 4 B each
-        unit_note = "4 * sum over oriented edges of (|N+(u)| + |N+(v)|) bytes per launch"
+        unit_note = "4 * sum over merged oriented edges of (|N+(u)| + |N+(v)|) bytes per launch"
+    elif dom == "tc_probe" and tc_probes:
+        alg = 2 * tc_probes  # 16-bit core-list entries, each tested against a staged row
+        unit_note = "2 bytes per core-list entry tested per launch"
     roof = None
     if alg and dom_n:
         per_launch_s = dom_ms / dom_n / 1e3
@@ -804,7 +809,7 @@ def run_gv(args, rank, world, local_rank):
         if tfile.exists():
             tj = json.loads(tfile.read_text())
             if dom in tj and tj[dom].get("bytes_per_unit"):
-                units = m_now if dom == "pull" else tc_work
+                units = {"pull": m_now, "tc_count": tc_work, "tc_probe": tc_probes}[dom]
                 traffic = tj[dom]["bytes_per_unit"] * units
         roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                 "frac": achieved / hbm_peak, "traffic": traffic, "algorithmic_bytes": alg,
@@ -819,6 +824,7 @@ def run_gv(args, rank, world, local_rank):
             "data": "synthetic (seeded R-MAT graph, uniform-random inserts, deletes sampled from existing edges)",
             "config": workload_config(args, n, m0),
             "pagerank_gteps": pr_gteps, "pagerank_sweeps_avg": avg_sweeps, "m_entries": m_now,
+            "triangles": {"merged_entries": tc_work, "core_probes": tc_probes, "core_vertices": tc_core},
             "kernel_ms": phases, "roofline": roof, "gpu_launches": launches, "clocks": clocks}
     if incr:
         line["incremental_tc"] = {

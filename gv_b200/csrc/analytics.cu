@@ -98,9 +98,9 @@ __device__ __forceinline__ void pull_tiny_body(const DevGraph &g, const PullArgs
 #pragma unroll
             for (uint32_t e = 0; e < TINY_FILL; e += 4) {
                 if (e < fill) {
-                    const uint4 q = *reinterpret_cast<const uint4 *>(g.pool + base + e);
+                    const uint4 q = __ldcs(reinterpret_cast<const uint4 *>(g.pool + base + e));
                     float4 wq = make_float4(1.f, 1.f, 1.f, 1.f);
-                    if (W) wq = *reinterpret_cast<const float4 *>(g.wpool + base + e);
+                    if (W) wq = __ldcs(reinterpret_cast<const float4 *>(g.wpool + base + e));
                     const uint32_t ev[4] = {q.x, q.y, q.z, q.w};
                     const float wv[4] = {wq.x, wq.y, wq.z, wq.w};
 #pragma unroll
@@ -140,9 +140,9 @@ __device__ __forceinline__ void pull_body(const DevGraph &g, const PullArgs &a, 
         if (nb == 1) {
             const size_t base = (size_t)rec.x << g.logB;
             for (uint32_t e = G.gl * 4; e < fill; e += TPV * 4) {
-                const uint4 q = *reinterpret_cast<const uint4 *>(g.pool + base + e);
+                const uint4 q = __ldcs(reinterpret_cast<const uint4 *>(g.pool + base + e));
                 float4 wq = make_float4(1.f, 1.f, 1.f, 1.f);
-                if (W) wq = *reinterpret_cast<const float4 *>(g.wpool + base + e);
+                if (W) wq = __ldcs(reinterpret_cast<const float4 *>(g.wpool + base + e));
                 const uint32_t ev[4] = {q.x, q.y, q.z, q.w};
                 const float wv[4] = {wq.x, wq.y, wq.z, wq.w};
 #pragma unroll
@@ -156,9 +156,9 @@ __device__ __forceinline__ void pull_body(const DevGraph &g, const PullArgs &a, 
             for (uint32_t qi = G.gl; qi < nq; qi += TPV) {
                 const uint32_t e = qi << 2;
                 const size_t at = ((size_t)tab[e >> g.logB] << g.logB) + (e & (g.B - 1));
-                const uint4 q = *reinterpret_cast<const uint4 *>(g.pool + at);
+                const uint4 q = __ldcs(reinterpret_cast<const uint4 *>(g.pool + at));
                 float4 wq = make_float4(1.f, 1.f, 1.f, 1.f);
-                if (W) wq = *reinterpret_cast<const float4 *>(g.wpool + at);
+                if (W) wq = __ldcs(reinterpret_cast<const float4 *>(g.wpool + at));
                 const uint32_t ev[4] = {q.x, q.y, q.z, q.w};
                 const float wv[4] = {wq.x, wq.y, wq.z, wq.w};
 #pragma unroll
@@ -242,9 +242,9 @@ __device__ __forceinline__ void pull_items_body(const DevGraph &g, const PullArg
             const uint32_t pb = __shfl_sync(GV_FULL_MASK, my_blk, (el >> g.logB) & 31u);
             if (q >= nq) continue;
             const size_t at = ((size_t)pb << g.logB) + (el & (g.B - 1));
-            const uint4 qv = *reinterpret_cast<const uint4 *>(g.pool + at);
+            const uint4 qv = __ldcs(reinterpret_cast<const uint4 *>(g.pool + at));
             float4 wq = make_float4(1.f, 1.f, 1.f, 1.f);
-            if (W) wq = *reinterpret_cast<const float4 *>(g.wpool + at);
+            if (W) wq = __ldcs(reinterpret_cast<const float4 *>(g.wpool + at));
             const uint32_t ev[4] = {qv.x, qv.y, qv.z, qv.w};
             const float wv[4] = {wq.x, wq.y, wq.z, wq.w};
 #pragma unroll
@@ -1056,6 +1056,73 @@ __global__ void k_tcc_item_owner(const uint32_t *__restrict__ itoff, uint32_t cm
         for (uint32_t i = itoff[c] + lane; i < itoff[c + 1]; i += 32) itc[i] = c;
 }
 
+// Reorders each core list so the probe's shared-memory loads meet distinct
+// banks.  The probe's lanes read consecutive 8-entry rows of a list, and the
+// t-th load of every lane reads column t; so the entries are put in
+// round-robin order over their banks ((x >> 5) mod 32: first entry of each
+// bank, then second, ...) and that sequence fills the list column by column.
+// Consecutive rows of a column then hold entries of consecutive banks.
+// Lists of one row, or longer than TCC_COLOR_MAX, keep their order (the
+// counts never depend on it).
+constexpr uint32_t TCC_COLOR_MAX = 2048;
+constexpr uint32_t TCC_COLOR_J = 128;  // deepest bank rank handled; deeper lists keep their order
+__global__ void __launch_bounds__(256) k_tcc_color(TcCore k, uint32_t n) {
+    extern __shared__ uint16_t cbuf[];  // [8 warps][TCC_COLOR_MAX]
+    __shared__ uint32_t hist[8][32], cur[8][32], tabM[8][TCC_COLOR_J], tabS[8][TCC_COLOR_J];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    uint16_t *out = cbuf + warp * TCC_COLOR_MAX;
+    // the warp looks at 32 vertices at a time and reorders those with more than one row
+    for (uint32_t u0 = (blockIdx.x * 8 + warp) * 32; u0 < n; u0 += gridDim.x * 8 * 32) {
+        const uint32_t um = u0 + lane;
+        uint32_t Lm = 0;
+        unsigned long long am = 0;
+        if (um < n) {
+            am = k.coff[um];
+            Lm = (uint32_t)(k.coff[um + 1] - am);
+        }
+        uint32_t todo = __ballot_sync(GV_FULL_MASK, Lm > 8 && Lm <= TCC_COLOR_MAX);
+        while (todo) {
+            const uint32_t t = __ffs(todo) - 1;
+            todo &= todo - 1;
+            const uint32_t L = __shfl_sync(GV_FULL_MASK, Lm, t);  // a multiple of 8
+            const unsigned long long a = __shfl_sync(GV_FULL_MASK, am, t);
+            uint16_t *cl = k.clist + a;
+            hist[warp][lane] = 0;
+            cur[warp][lane] = 0;
+            __syncwarp();
+            for (uint32_t i = lane; i < L; i += 32) atomicAdd(&hist[warp][(cl[i] >> 5) & 31u], 1u);
+            __syncwarp();
+            // lane = bank: M_j = banks with more than j entries, S_j = entries of ranks below j
+            const uint32_t c = hist[warp][lane];
+            uint32_t jmax = c;
+#pragma unroll
+            for (int o = 16; o; o >>= 1) jmax = max(jmax, __shfl_xor_sync(GV_FULL_MASK, jmax, o));
+            if (jmax > TCC_COLOR_J) continue;  // warp-uniform
+            uint32_t S = 0;
+            for (uint32_t j = 0; j < jmax; ++j) {
+                const uint32_t M = __ballot_sync(GV_FULL_MASK, c > j);
+                if (lane == 0) {
+                    tabM[warp][j] = M;
+                    tabS[warp][j] = S;
+                }
+                S += __popc(M);
+            }
+            __syncwarp();
+            const uint32_t R = L >> 3;
+            for (uint32_t i = lane; i < L; i += 32) {
+                const uint16_t x = cl[i];
+                const uint32_t b = (x >> 5) & 31u;
+                const uint32_t j = atomicAdd(&cur[warp][b], 1u);  // rank within its bank
+                const uint32_t o = tabS[warp][j] + __popc(tabM[warp][j] & ((1u << b) - 1u));
+                out[(o % R) * 8 + o / R] = x;
+            }
+            __syncwarp();
+            for (uint32_t i = lane; i < L; i += 32) cl[i] = out[i];
+            __syncwarp();
+        }
+    }
+}
+
 // Bit tests of eight core entries (one 16-byte load) against the staged row.
 __device__ __forceinline__ uint32_t tcc_probe8(const uint32_t *srow, uint4 q) {
     uint32_t h = 0;
@@ -1558,6 +1625,12 @@ uint32_t tc_core_max() {
     return (uint32_t)v & ~31u;
 }
 
+// GV_TC_COLOR=0 leaves the core lists in fill order (for comparison).
+bool tc_color() {
+    const char *env = std::getenv("GV_TC_COLOR");
+    return !(env && env[0] == '0');
+}
+
 // Dense core of a total-only count, first half: carves the core buffers from
 // auxiliary slot 10 and picks the core (k.cidx).  No host synchronisation.
 gv_status tc_core_select(gv_graph *g, const TcBufs &b, uint64_t mplus, uint32_t cmax, TcCore &k, cudaStream_t s) {
@@ -1623,6 +1696,8 @@ gv_status tc_core_count(gv_graph *g, const TcBufs &b, uint64_t mplus, TcCore &k,
         cudaMemsetAsync(k.ccnt, 0, (size_t)n * 4, s);
         cudaMemsetAsync(k.icnt, 0, ((size_t)cmax + 1) * 4, s);
         GV_LAUNCH(k_tcc_fill, egrid, 256, 0, s, (const uint32_t *)b.snap, (const uint32_t *)b.esrc, mplus, k);
+        if (tc_color())
+            GV_LAUNCH(k_tcc_color, grid_for(n, 8 * 32, 148 * 8), 256, (size_t)8 * TCC_COLOR_MAX * 2, s, k, n);
         GV_LAUNCH(k_tcc_items, grid_for(cmax, 256), 256, 0, s, (const unsigned long long *)k.ioff, cmax, k.itcnt);
         scan_exclusive_u32(k.itcnt, k.itoff, cmax, k.itoff + cmax, g->bs.scan_tmp, s);
         GV_LAUNCH(k_tcc_item_owner, grid_for(cmax, 8), 256, 0, s, (const uint32_t *)k.itoff, cmax, k.itc);
