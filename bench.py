@@ -654,7 +654,7 @@ def run_gv(args, rank, world, local_rank):
     half = args.batch // 2
     total_steps = args.warmup + args.steps + (0 if args.no_e2e else args.steps)
     n_incr = 0 if (args.no_incremental or world > 1) else 4
-    batches = make_batches(n, off, dst, total_steps + n_incr, half, seed)
+    batches = make_batches(n, off, dst, total_steps + 2 * n_incr, half, seed)
     srcs = bc_sources(n, args.bc_sources, seed)
     dev_batches = [tuple(torch.from_numpy(a.astype(np.int32)).to(dev) for a in b) for b in batches]
     x_dev = torch.empty(n, dtype=torch.float32, device=dev)
@@ -748,29 +748,35 @@ def run_gv(args, rank, world, local_rank):
         e2e = {"ms": e2e_ms, "h2d": h2d, "d2h": d2h}
 
     # incremental triangle counts (single GPU): batches alternate between
-    # gv_update_tc (exact delta) and update + whole-graph count
+    # gv_update_tc (exact delta) and update + whole-graph count, at the step's
+    # batch size and at 1/16 of it (the first inserts and deletes of a batch)
     incr = None
     if n_incr:
-        incr = {"batch_updates": args.batch, "update_tc_ms": [], "update_then_static_tc_ms": [], "exact": True}
+        incr = {"exact": True, "sizes": {}}
         _, t_ref = g.static_tc(per_vertex=False)
-        for j in range(n_incr):
-            ins_s, ins_d, del_s, del_d = dev_batches[total_steps + j]
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            if j % 2 == 0:
-                dt, _ = g.update_tc(ins_s, ins_d, del_s, del_d, compact=True)
+        for fi, frac in enumerate((1, 16)):
+            k = args.batch // 2 // frac
+            rec = {"updates": 2 * k, "update_tc_ms": [], "update_then_static_tc_ms": []}
+            for j in range(n_incr):
+                ins_s, ins_d, del_s, del_d = (a[:k] for a in dev_batches[total_steps + fi * n_incr + j])
                 torch.cuda.synchronize()
-                incr["update_tc_ms"].append((time.perf_counter() - t0) * 1e3)
-                _, t_chk = g.static_tc(per_vertex=False)
-                incr["exact"] = incr["exact"] and (t_chk == t_ref + dt)
-                t_ref = t_chk
-            else:
-                g.batch_insert(ins_s, ins_d)
-                g.batch_delete(del_s, del_d)
-                g.compaction()
-                _, t_ref = g.static_tc(per_vertex=False)
-                torch.cuda.synchronize()
-                incr["update_then_static_tc_ms"].append((time.perf_counter() - t0) * 1e3)
+                t0 = time.perf_counter()
+                if j % 2 == 0:
+                    dt, _ = g.update_tc(ins_s, ins_d, del_s, del_d, compact=True)
+                    torch.cuda.synchronize()
+                    rec["update_tc_ms"].append((time.perf_counter() - t0) * 1e3)
+                    _, t_chk = g.static_tc(per_vertex=False)
+                    incr["exact"] = incr["exact"] and (t_chk == t_ref + dt)
+                    t_ref = t_chk
+                else:
+                    g.batch_insert(ins_s, ins_d)
+                    g.batch_delete(del_s, del_d)
+                    g.compaction()
+                    _, t_ref = g.static_tc(per_vertex=False)
+                    torch.cuda.synchronize()
+                    rec["update_then_static_tc_ms"].append((time.perf_counter() - t0) * 1e3)
+            incr["sizes"][str(2 * k)] = {"update_tc_ms": statistics.mean(rec["update_tc_ms"]),
+                                         "update_then_static_tc_ms": statistics.mean(rec["update_then_static_tc_ms"])}
         incr["triangles_after"] = int(t_ref)
     # max over ranks
     t = torch.tensor([elapsed_ms, e2e["ms"] if e2e else 0.0], dtype=torch.float64, device=dev)
@@ -828,11 +834,10 @@ def run_gv(args, rank, world, local_rank):
             "kernel_ms": phases, "roofline": roof, "gpu_launches": launches, "clocks": clocks}
     if incr:
         line["incremental_tc"] = {
-            "workload": ("same graph and batch size as the steps; gv_update_tc (inserts, deletes, compaction and "
-                         "the exact triangle delta) against insert + delete + compaction + whole-graph count"),
-            "update_tc_ms": statistics.mean(incr["update_tc_ms"]),
-            "update_then_static_tc_ms": statistics.mean(incr["update_then_static_tc_ms"]),
-            "exact": incr["exact"], "triangles_after": incr["triangles_after"]}
+            "workload": ("same graph as the steps, batches of the step's size and of 1/16 of it; gv_update_tc "
+                         "(inserts, deletes, compaction and the exact triangle delta) against insert + delete + "
+                         "compaction + whole-graph count"),
+            "by_batch_updates": incr["sizes"], "exact": incr["exact"], "triangles_after": incr["triangles_after"]}
     if e2e:
         line["e2e"] = {"value": updates / (e2e_ms / 1e3), "unit": "edge updates/s",
                        "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"]}

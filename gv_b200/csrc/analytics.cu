@@ -78,6 +78,19 @@ __device__ __forceinline__ float pull_finish(const PullArgs &a, uint32_t v, floa
     return xv;
 }
 
+// Adds the gathered values of the live entries among four (entries at or past
+// `limit` and tombstones skipped).
+template <bool W>
+__device__ __forceinline__ float pull_gather4(const PullArgs &a, uint4 q, float4 wq, uint32_t e, uint32_t limit) {
+    const uint32_t ev[4] = {q.x, q.y, q.z, q.w};
+    const float wv[4] = {wq.x, wq.y, wq.z, wq.w};
+    float s = 0.f;
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+        if (e + j < limit && ev[j] != GV_TOMB) s += W ? wv[j] * __ldg(a.gather + ev[j]) : __ldg(a.gather + ev[j]);
+    return s;
+}
+
 // Vertices with at most TINY_FILL entries: one thread per vertex issues all
 // of its (at most 8) 16-byte loads and gathers at once, so the dependent
 // chain vertex -> block -> neighbours is paid once per thread instead of
@@ -138,32 +151,42 @@ __device__ __forceinline__ void pull_body(const DevGraph &g, const PullArgs &a, 
         if (fill > LIGHT_FILL || fill <= TINY_FILL) continue;  // k_pull_items / k_pull_tiny
         float sum = 0.f;
         if (nb == 1) {
+            // two 16-byte loads per lane before their gathers: eight gathers in flight
             const size_t base = (size_t)rec.x << g.logB;
-            for (uint32_t e = G.gl * 4; e < fill; e += TPV * 4) {
+            for (uint32_t e = G.gl * 4; e < fill; e += TPV * 8) {
+                const uint32_t e2 = e + TPV * 4;
                 const uint4 q = __ldcs(reinterpret_cast<const uint4 *>(g.pool + base + e));
-                float4 wq = make_float4(1.f, 1.f, 1.f, 1.f);
-                if (W) wq = __ldcs(reinterpret_cast<const float4 *>(g.wpool + base + e));
-                const uint32_t ev[4] = {q.x, q.y, q.z, q.w};
-                const float wv[4] = {wq.x, wq.y, wq.z, wq.w};
-#pragma unroll
-                for (int j = 0; j < 4; ++j)
-                    if (e + j < fill && ev[j] != GV_TOMB) sum += W ? wv[j] * __ldg(a.gather + ev[j]) : __ldg(a.gather + ev[j]);
+                uint4 q2 = make_uint4(GV_TOMB, GV_TOMB, GV_TOMB, GV_TOMB);
+                if (e2 < fill) q2 = __ldcs(reinterpret_cast<const uint4 *>(g.pool + base + e2));
+                float4 wq = make_float4(1.f, 1.f, 1.f, 1.f), wq2 = wq;
+                if (W) {
+                    wq = __ldcs(reinterpret_cast<const float4 *>(g.wpool + base + e));
+                    if (e2 < fill) wq2 = __ldcs(reinterpret_cast<const float4 *>(g.wpool + base + e2));
+                }
+                sum += pull_gather4<W>(a, q, wq, e, fill);
+                sum += pull_gather4<W>(a, q2, wq2, e2, fill);
             }
         } else if (nb > 1) {
             fill_block_table(g, rec.x, 0, nb, tab, G.gl, TPV);
             G.sync();
             const uint32_t nq = (fill + 3) >> 2;
-            for (uint32_t qi = G.gl; qi < nq; qi += TPV) {
-                const uint32_t e = qi << 2;
+            for (uint32_t qi = G.gl; qi < nq; qi += 2 * TPV) {
+                const uint32_t e = qi << 2, e2 = (qi + TPV) << 2;
                 const size_t at = ((size_t)tab[e >> g.logB] << g.logB) + (e & (g.B - 1));
                 const uint4 q = __ldcs(reinterpret_cast<const uint4 *>(g.pool + at));
-                float4 wq = make_float4(1.f, 1.f, 1.f, 1.f);
-                if (W) wq = __ldcs(reinterpret_cast<const float4 *>(g.wpool + at));
-                const uint32_t ev[4] = {q.x, q.y, q.z, q.w};
-                const float wv[4] = {wq.x, wq.y, wq.z, wq.w};
-#pragma unroll
-                for (int j = 0; j < 4; ++j)
-                    if (e + j < fill && ev[j] != GV_TOMB) sum += W ? wv[j] * __ldg(a.gather + ev[j]) : __ldg(a.gather + ev[j]);
+                uint4 q2 = make_uint4(GV_TOMB, GV_TOMB, GV_TOMB, GV_TOMB);
+                size_t at2 = 0;
+                if (qi + TPV < nq) {
+                    at2 = ((size_t)tab[e2 >> g.logB] << g.logB) + (e2 & (g.B - 1));
+                    q2 = __ldcs(reinterpret_cast<const uint4 *>(g.pool + at2));
+                }
+                float4 wq = make_float4(1.f, 1.f, 1.f, 1.f), wq2 = wq;
+                if (W) {
+                    wq = __ldcs(reinterpret_cast<const float4 *>(g.wpool + at));
+                    if (qi + TPV < nq) wq2 = __ldcs(reinterpret_cast<const float4 *>(g.wpool + at2));
+                }
+                sum += pull_gather4<W>(a, q, wq, e, fill);
+                sum += pull_gather4<W>(a, q2, wq2, e2, fill);
             }
             G.sync();
         }
@@ -235,21 +258,25 @@ __device__ __forceinline__ void pull_items_body(const DevGraph &g, const PullArg
         const uint32_t e1 = min(fill, (kb0 + 32) << g.logB);
         const uint32_t nq = (e1 - e0 + 3) >> 2;
         float sum = 0.f;
-#pragma unroll 4
-        for (uint32_t q0 = 0; q0 < nq; q0 += 32) {  // warp-uniform trip count
-            const uint32_t q = q0 + lane;
-            const uint32_t el = q << 2;  // entry offset within the item
+        for (uint32_t q0 = 0; q0 < nq; q0 += 64) {  // warp-uniform trip count; two loads per lane in flight
+            const uint32_t q = q0 + lane, q2 = q + 32;
+            const uint32_t el = q << 2, el2 = q2 << 2;  // entry offsets within the item
             const uint32_t pb = __shfl_sync(GV_FULL_MASK, my_blk, (el >> g.logB) & 31u);
-            if (q >= nq) continue;
+            const uint32_t pb2 = __shfl_sync(GV_FULL_MASK, my_blk, (el2 >> g.logB) & 31u);
+            uint4 qv = make_uint4(GV_TOMB, GV_TOMB, GV_TOMB, GV_TOMB), qv2 = qv;
+            float4 wq = make_float4(1.f, 1.f, 1.f, 1.f), wq2 = wq;
             const size_t at = ((size_t)pb << g.logB) + (el & (g.B - 1));
-            const uint4 qv = __ldcs(reinterpret_cast<const uint4 *>(g.pool + at));
-            float4 wq = make_float4(1.f, 1.f, 1.f, 1.f);
-            if (W) wq = __ldcs(reinterpret_cast<const float4 *>(g.wpool + at));
-            const uint32_t ev[4] = {qv.x, qv.y, qv.z, qv.w};
-            const float wv[4] = {wq.x, wq.y, wq.z, wq.w};
-#pragma unroll
-            for (int j = 0; j < 4; ++j)
-                if (e0 + el + j < e1 && ev[j] != GV_TOMB) sum += W ? wv[j] * __ldg(a.gather + ev[j]) : __ldg(a.gather + ev[j]);
+            const size_t at2 = ((size_t)pb2 << g.logB) + (el2 & (g.B - 1));
+            if (q < nq) {
+                qv = __ldcs(reinterpret_cast<const uint4 *>(g.pool + at));
+                if (W) wq = __ldcs(reinterpret_cast<const float4 *>(g.wpool + at));
+            }
+            if (q2 < nq) {
+                qv2 = __ldcs(reinterpret_cast<const uint4 *>(g.pool + at2));
+                if (W) wq2 = __ldcs(reinterpret_cast<const float4 *>(g.wpool + at2));
+            }
+            sum += pull_gather4<W>(a, qv, wq, e0 + el, e1);
+            sum += pull_gather4<W>(a, qv2, wq2, e0 + el2, e1);
         }
         sum = warp_sum(sum);
         if (lane == 0) ipart[i] = sum;
