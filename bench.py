@@ -84,6 +84,8 @@ class ClockSampler:
         self.thread = None
 
     def start(self):
+        """Starts nvidia-smi and waits for its first sample, so its start-up
+        (NVML initialisation) is over before the timed region begins."""
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
@@ -93,12 +95,17 @@ class ClockSampler:
             return
         self.thread = threading.Thread(target=self._read, daemon=True)
         self.thread.start()
+        t_wait = time.monotonic() + 10.0
+        while not self.lines and time.monotonic() < t_wait:
+            time.sleep(0.01)
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.monotonic(), line.strip()))
 
-    def stop(self) -> dict | None:
+    def stop(self, t0: float | None = None, t1: float | None = None) -> dict | None:
+        """Summary of the samples taken in [t0, t1] (host monotonic time; all
+        samples when no window is given or none falls inside it)."""
         if not self.proc:
             return None
         self.proc.terminate()
@@ -110,7 +117,8 @@ class ClockSampler:
             self.thread.join(timeout=2)
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        inside = [ln for t, ln in self.lines if t0 is not None and t0 <= t <= t1 + 0.2]
+        for ln in inside or [ln for _, ln in self.lines]:
             p = [x.strip() for x in ln.split(",")]
             if len(p) < 7:
                 continue
@@ -688,21 +696,25 @@ def run_gv(args, rank, world, local_rank):
             dist.barrier()
         torch.cuda.synchronize()
 
-    # warm-up
-    for b in range(args.warmup):
-        step(b, dev_batches[b])
-    barrier()
-    for k in stats:
-        stats[k].clear()
     sampler = ClockSampler(local_rank)
     if not args.no_clocks:
         sampler.start()
+    # warm-up; a BC call as well when no warm-up step ran one, so the BC
+    # scratch is sized before the timed region like everything else
+    for b in range(args.warmup):
+        step(b, dev_batches[b])
+    if args.warmup < args.bc_every:
+        g.bc(srcs)
+    barrier()
+    for k in stats:
+        stats[k].clear()
     gv_b200.profile_reset()
     gv_b200.profile_enable(True)
     launches0 = gv_b200.kernel_launches()
     t_start = torch.cuda.Event(enable_timing=True)
     t_end = torch.cuda.Event(enable_timing=True)
     barrier()
+    h_start = time.monotonic()
     t_start.record()
     for i in range(args.steps):
         b = args.warmup + i
@@ -712,7 +724,7 @@ def run_gv(args, rank, world, local_rank):
     barrier()
     gv_b200.profile_enable(False)
     launches = gv_b200.kernel_launches() - launches0
-    clocks = sampler.stop()
+    clocks = sampler.stop(h_start, time.monotonic())
     elapsed_ms = t_start.elapsed_time(t_end)
     timed_sweeps = list(stats["pr_sweeps"])  # the e2e leg below appends its own
     m_now = g.num_edges()
