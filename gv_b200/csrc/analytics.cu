@@ -12,6 +12,7 @@
 //              intersection (packed hash probe behind GV_TC_PACKED=1),
 //              uint64 counts;
 #include <algorithm>
+#include <cstdio>
 #include <cmath>
 #include <cstring>
 #include <type_traits>
@@ -35,6 +36,16 @@ constexpr int BIG_TAB_A = 1024;
 // one CTA per vertex up to HUB_FILL, the whole grid above.
 constexpr uint32_t LIGHT_FILL = 256;
 constexpr uint32_t TINY_FILL = 32;  // thread-per-vertex tier of the pull sweeps
+constexpr unsigned FIN_GRID = 148;
+// The fused sweep runs SWEEP_WAVES rounds of SWEEP_PERIOD CTAs; of each
+// round, the tiers get CTAs in proportion to their estimated work, so no
+// tier's CTAs carry the tail.  Residual slots: lane-group tier [0,
+// SWEEP_GRID), item finish [SWEEP_GRID, + FIN_GRID), thread-per-vertex tier
+// [SWEEP_GRID + FIN_GRID, + SWEEP_GRID).
+constexpr unsigned SWEEP_PERIOD = 16;
+constexpr unsigned SWEEP_WAVES = 148 * 24 / SWEEP_PERIOD;
+constexpr unsigned SWEEP_GRID = SWEEP_PERIOD * SWEEP_WAVES;
+constexpr unsigned SWEEP_PARTS = SWEEP_GRID + FIN_GRID + SWEEP_GRID;
 constexpr uint32_t HUB_FILL = 16384;
 
 // Lanes per block and blocks per warp step for the grid-cooperative paths.
@@ -96,15 +107,15 @@ __device__ __forceinline__ float pull_gather4(const PullArgs &a, uint4 q, float4
 // chain vertex -> block -> neighbours is paid once per thread instead of
 // once per vertex by a whole lane group.
 template <bool W>
-__device__ __forceinline__ void pull_tiny_body(const DevGraph &g, const PullArgs &a, uint32_t part_base, uint32_t vb,
-                                               uint32_t vg) {
+__device__ __forceinline__ void pull_tiny_body(const DevGraph &g, const PullArgs &a, const uint32_t *__restrict__ list,
+                                               uint32_t cnt, uint32_t part_base, uint32_t vb, uint32_t vg) {
     __shared__ double red[AN_THREADS / 32];
     if (a.state[0]) return;
     double res = 0.0;
-    for (uint32_t v = vb * blockDim.x + threadIdx.x; v < g.n; v += vg * blockDim.x) {
+    for (uint32_t i = vb * blockDim.x + threadIdx.x; i < cnt; i += vg * blockDim.x) {
+        const uint32_t v = list[i];  // the vertices with at most TINY_FILL entries, in id order
         const uint4 rec = g.vtx[v];
         const uint32_t fill = rec.y;
-        if (fill > TINY_FILL) continue;  // k_pull / k_pull_items
         float sum = 0.f;
         if (fill) {
             const size_t base = (size_t)rec.x << g.logB;  // fill <= 32 <= B: one block
@@ -136,7 +147,8 @@ __device__ __forceinline__ void pull_tiny_body(const DevGraph &g, const PullArgs
 }
 
 template <int TPV, bool W>
-__device__ __forceinline__ void pull_body(const DevGraph &g, const PullArgs &a, uint32_t vb, uint32_t vg) {
+__device__ __forceinline__ void pull_body(const DevGraph &g, const PullArgs &a, const uint32_t *__restrict__ list,
+                                          uint32_t cnt, uint32_t vb, uint32_t vg) {
     __shared__ double red[AN_THREADS / 32];
     if (a.state[0]) return;
     constexpr int GPC = AN_THREADS / TPV;
@@ -145,10 +157,10 @@ __device__ __forceinline__ void pull_body(const DevGraph &g, const PullArgs &a, 
     uint32_t *tab = tabs[threadIdx.x / TPV];
     const uint32_t ngroups = vg * GPC;
     double res = 0.0;
-    for (uint32_t v = vb * GPC + threadIdx.x / TPV; v < g.n; v += ngroups) {
+    for (uint32_t i = vb * GPC + threadIdx.x / TPV; i < cnt; i += ngroups) {
+        const uint32_t v = list[i];  // the vertices with TINY_FILL < fill <= LIGHT_FILL, in id order
         const uint4 rec = g.vtx[v];
         const uint32_t fill = rec.y, nb = blocks_for(fill, g.logB);
-        if (fill > LIGHT_FILL || fill <= TINY_FILL) continue;  // k_pull_items / k_pull_tiny
         float sum = 0.f;
         if (nb == 1) {
             // two 16-byte loads per lane before their gathers: eight gathers in flight
@@ -212,20 +224,61 @@ struct Items {
     const uint32_t *item_vertex;  // item -> vertex
     const uint32_t *item_first;   // vertex -> its first item (n + 1)
     const uint32_t *multi;        // vertices that have items
-    uint32_t nitems, nmulti;
+    const uint32_t *light;        // vertices with TINY_FILL < fill <= LIGHT_FILL (lane-group tier), id order
+    const uint32_t *tiny;         // vertices with fill <= TINY_FILL (thread-per-vertex tier), id order
+    uint32_t nitems, nmulti, nlight, ntiny;
+    uint32_t split;               // CTAs of the fused sweep per SWEEP_PERIOD: lane-group | tiny << 8 | items << 16
 };
 
+// Items per vertex; tier[0..4] (nullable) gets the entries and vertices of
+// the thread-per-vertex tier, those of the lane-group tier and the entries
+// of the item tier, which size the tiers' shares of the fused sweep.
 __global__ void k_item_count(DevGraph g, uint32_t *__restrict__ cnt, uint32_t *__restrict__ multi,
-                             unsigned long long *nmulti) {
+                             unsigned long long *nmulti, unsigned long long *__restrict__ tier) {
     const uint32_t chunk_log = g.logB + 5;  // 32 blocks per item
-    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < g.n; v += gridDim.x * blockDim.x) {
+    unsigned long long t[5] = {0, 0, 0, 0, 0};
+    for (uint32_t base = blockIdx.x * blockDim.x; base < g.n; base += gridDim.x * blockDim.x) {
+        const uint32_t v = base + threadIdx.x;
+        if (v >= g.n) continue;
         const uint32_t fill = g.vtx[v].y;
         uint32_t c = 0;
         if (fill > LIGHT_FILL) {
             c = (fill + (1u << chunk_log) - 1) >> chunk_log;
             multi[atomicAdd(nmulti, 1ull)] = v;
+            t[4] += fill;
+        } else if (fill > TINY_FILL) {
+            t[2] += fill;
+            t[3] += 1;
+        } else if (fill) {
+            t[0] += fill;
+            t[1] += 1;
         }
         cnt[v] = c;
+    }
+    if (!tier) return;
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+        const unsigned long long s = warp_sum(t[i]);
+        if ((threadIdx.x & 31) == 0 && s) atomicAdd(&tier[i], s);
+    }
+}
+
+// Tier flags of every vertex: tl[v] = 1 for the lane-group tier, tt[v] = 1
+// for the thread-per-vertex tier (scanned into list positions next).
+__global__ void k_tier_flags(DevGraph g, uint32_t *__restrict__ tl, uint32_t *__restrict__ tt) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < g.n; v += gridDim.x * blockDim.x) {
+        const uint32_t fill = g.vtx[v].y;
+        tl[v] = (fill > TINY_FILL && fill <= LIGHT_FILL) ? 1u : 0u;
+        tt[v] = fill <= TINY_FILL ? 1u : 0u;
+    }
+}
+
+// Scatters the tier members into their lists at the scanned positions (id order).
+__global__ void k_tier_lists(DevGraph g, const uint32_t *__restrict__ pl, const uint32_t *__restrict__ pt,
+                             uint32_t *__restrict__ light, uint32_t *__restrict__ tiny) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < g.n; v += gridDim.x * blockDim.x) {
+        if (pl[v + 1] != pl[v]) light[pl[v]] = v;
+        if (pt[v + 1] != pt[v]) tiny[pt[v]] = v;
     }
 }
 
@@ -283,16 +336,18 @@ __device__ __forceinline__ void pull_items_body(const DevGraph &g, const PullArg
     }
 }
 
-// One launch for the three tiers of a sweep, CTAs interleaved (CTA i runs
-// tier i % 3) so the thread-per-vertex, lane-group and hub-item work share
-// every wave instead of running one after another.
+// One launch for the three tiers of a sweep, CTAs interleaved (each round of
+// SWEEP_PERIOD CTAs holds the tiers' shares, it.split) so the lane-group,
+// thread-per-vertex and hub-item work share every wave instead of running one
+// after another.
 template <int TPV, bool W>
 __global__ void __launch_bounds__(AN_THREADS) k_pull_fused(DevGraph g, PullArgs a, Items it, float *__restrict__ ipart,
                                                            uint32_t tiny_base) {
-    const uint32_t part = blockIdx.x % 3u, vb = blockIdx.x / 3u, vg = gridDim.x / 3u;
-    if (part == 0) pull_body<TPV, W>(g, a, vb, vg);
-    else if (part == 1) pull_tiny_body<W>(g, a, tiny_base, vb, vg);
-    else pull_items_body<W>(g, a, it, ipart, vb, vg);
+    const uint32_t t0 = it.split & 0xFFu, t1 = (it.split >> 8) & 0xFFu, t2 = (it.split >> 16) & 0xFFu;
+    const uint32_t r = blockIdx.x % SWEEP_PERIOD, w = blockIdx.x / SWEEP_PERIOD, waves = gridDim.x / SWEEP_PERIOD;
+    if (r < t0) pull_body<TPV, W>(g, a, it.light, it.nlight, w * t0 + r, waves * t0);
+    else if (r < t0 + t1) pull_tiny_body<W>(g, a, it.tiny, it.ntiny, tiny_base, w * t1 + (r - t0), waves * t1);
+    else pull_items_body<W>(g, a, it, ipart, w * t2 + (r - t0 - t1), waves * t2);
 }
 
 __global__ void __launch_bounds__(AN_THREADS) k_pull_items_fin(DevGraph g, PullArgs a, Items it,
@@ -385,25 +440,64 @@ IterBufs carve_iter(void *base, uint32_t n, uint32_t parts) {
 
 constexpr unsigned PULL_GRID = 148 * 8;
 constexpr unsigned HUB_GRID = 148 * 2;
-constexpr unsigned FIN_GRID = 148;
-constexpr unsigned TINY_GRID = 148 * 8;
-constexpr unsigned SWEEP_PARTS = PULL_GRID + FIN_GRID + TINY_GRID;
+
+// Tier shares of a round from tier[] of k_item_count: the work of a tier is
+// its entries plus a per-vertex cost (the record load, the dependent first
+// block load and the finish) of 16 entries.  On R-MAT scale 22 this gives
+// 3, 4 and 9 CTAs of 16 to the lane-group, thread-per-vertex and item tiers,
+// the best of the splits measured (0.58 ms per sweep; equal thirds 0.69).  A
+// tier with work gets at least one CTA per round; GV_SWEEP_SPLIT="a,b,c"
+// overrides the split.
+uint32_t sweep_split(const unsigned long long *tier) {
+    if (const char *env = std::getenv("GV_SWEEP_SPLIT")) {  // "lane-group,tiny,items" CTAs per round
+        unsigned x = 0, y = 0, z = 0;
+        if (std::sscanf(env, "%u,%u,%u", &x, &y, &z) == 3 && x + y + z == SWEEP_PERIOD && x && y && z)
+            return x | (y << 8) | (z << 16);
+    }
+    const double w[3] = {(double)tier[2] + 16.0 * tier[3], (double)tier[0] + 16.0 * tier[1], (double)tier[4]};
+    const double tot = w[0] + w[1] + w[2];
+    uint32_t t[3] = {0, 0, 0};
+    if (tot <= 0) return 1u | (1u << 8) | (1u << 16);
+    uint32_t sum = 0;
+    for (int i = 0; i < 3; ++i) {
+        t[i] = w[i] > 0 ? std::max<uint32_t>(1, (uint32_t)(SWEEP_PERIOD * w[i] / tot + 0.5)) : 0;
+        sum += t[i];
+    }
+    // settle the rounding on the tier with the most CTAs
+    int big = 0;
+    for (int i = 1; i < 3; ++i)
+        if (t[i] > t[big]) big = i;
+    while (sum > SWEEP_PERIOD) { --t[big]; --sum; }
+    while (sum < SWEEP_PERIOD) { ++t[big]; ++sum; }
+    return t[0] | (t[1] << 8) | (t[2] << 16);
+}
 
 // Builds the chunked item list of the current graph (aux scratch slots 1, 2);
 // *ipart gets one 4-byte slot per item.
 gv_status build_items(gv_graph *g, cudaStream_t s, unsigned long long *nmulti, Items *it, float **ipart) {
     DevGraph d = g->d;
     const uint32_t n = d.n;
-    uint32_t *first = (uint32_t *)aux_scratch(g, 1, ((size_t)n + 1) * 4 * 2 + 64);
+    // first, multi, the two tier position arrays (n + 1 each), the two tier lists (n each), counters
+    uint32_t *first = (uint32_t *)aux_scratch(g, 1, ((size_t)n + 1) * 4 * 4 + (size_t)n * 4 * 2 + 128);
     if (!first) return GV_ERR_NOMEM;
     uint32_t *multi = first + (n + 1);
+    uint32_t *pl = multi + (n + 1), *pt = pl + (n + 1), *light = pt + (n + 1), *tiny = light + n;
+    unsigned long long *tier = (unsigned long long *)(((uintptr_t)(tiny + n) + 7) & ~(uintptr_t)7);
+    GV_LAUNCH(k_tier_flags, grid_for(n, 256), 256, 0, s, d, pl, pt);
+    scan_exclusive_u32(pl, pl, n, pl + n, g->bs.scan_tmp, s);
+    scan_exclusive_u32(pt, pt, n, pt + n, g->bs.scan_tmp, s);
+    GV_LAUNCH(k_tier_lists, grid_for(n, 256), 256, 0, s, d, (const uint32_t *)pl, (const uint32_t *)pt, light, tiny);
     cudaMemsetAsync(nmulti, 0, 8, s);
-    GV_LAUNCH(k_item_count, grid_for(n, 256), 256, 0, s, d, first, multi, nmulti);
+    cudaMemsetAsync(tier, 0, 5 * 8, s);
+    GV_LAUNCH(k_item_count, grid_for(n, 256), 256, 0, s, d, first, multi, nmulti, tier);
     scan_exclusive_u32(first, first, n, first + n, g->bs.scan_tmp, s);
-    uint32_t nitems = 0;
-    unsigned long long nm = 0;
+    uint32_t nitems = 0, nl = 0, nt = 0;
+    unsigned long long nm = 0, ht[5] = {0, 0, 0, 0, 0};
     cudaMemcpyAsync(&nitems, first + n, 4, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(&nl, pl + n, 4, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(&nt, pt + n, 4, cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(&nm, nmulti, 8, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(ht, tier, 5 * 8, cudaMemcpyDeviceToHost, s);
     cudaError_t e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_status(e, "items");
     uint32_t *item_vertex = nullptr;
@@ -419,6 +513,11 @@ gv_status build_items(gv_graph *g, cudaStream_t s, unsigned long long *nmulti, I
     it->multi = multi;
     it->nitems = nitems;
     it->nmulti = (uint32_t)nm;
+    it->light = light;
+    it->tiny = tiny;
+    it->nlight = nl;
+    it->ntiny = nt;
+    it->split = sweep_split(ht);
     *ipart = ip;
     return GV_OK;
 }
@@ -452,16 +551,15 @@ gv_status run_sweeps(gv_graph *g, cudaStream_t s, IterBufs &b, PullArgs proto, b
             a.state = b.state;
             if (!contrib_pr && !weighted) a.gather = ca;
             ProfScope ps(PROF_PULL, s);
-            static_assert(TINY_GRID == PULL_GRID, "the fused sweep gives each tier the same CTA count");
             dispatch_tpv(g->cfg.threads_per_vertex, [&](auto t) {
                 constexpr int T = decltype(t)::value;
                 if (weighted)
-                    GV_LAUNCH((k_pull_fused<T, true>), 3 * PULL_GRID, AN_THREADS, 0, s, d, a, it, ipart, PULL_GRID + FIN_GRID);
+                    GV_LAUNCH((k_pull_fused<T, true>), SWEEP_GRID, AN_THREADS, 0, s, d, a, it, ipart, SWEEP_GRID + FIN_GRID);
                 else
-                    GV_LAUNCH((k_pull_fused<T, false>), 3 * PULL_GRID, AN_THREADS, 0, s, d, a, it, ipart, PULL_GRID + FIN_GRID);
+                    GV_LAUNCH((k_pull_fused<T, false>), SWEEP_GRID, AN_THREADS, 0, s, d, a, it, ipart, SWEEP_GRID + FIN_GRID);
             });
             if (it.nitems)
-                GV_LAUNCH(k_pull_items_fin, FIN_GRID, AN_THREADS, 0, s, d, a, it, (const float *)ipart, PULL_GRID);
+                GV_LAUNCH(k_pull_items_fin, FIN_GRID, AN_THREADS, 0, s, d, a, it, (const float *)ipart, SWEEP_GRID);
             GV_LAUNCH(k_iter_done, 1, 256, 0, s, b.partial, nparts, eps, b.state, b.res);
             std::swap(xa, xb);
             std::swap(ca, cb);

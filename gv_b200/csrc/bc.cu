@@ -318,8 +318,8 @@ __global__ void k_ms_close(MsBufs<NW> b, typename MaskOf<NW>::type *__restrict__
 
 // Backward sum over one block's entries for the sources in A: the entries one
 // level deeper for some of them are packed, then every lane gathers coef of
-// its sources for eight entries at a time (predicated and unrolled, so a
-// warp keeps several gathers in flight) and adds them in entry order.
+// its sources for eight (one word) or four (two words) entries at a time,
+// eight predicated gathers in flight per lane, and adds them in entry order.
 template <int NW>
 __device__ __forceinline__ void ms_bwd_block(const DevGraph &g, const MsBufs<NW> &b,
                                              const typename MaskOf<NW>::type *__restrict__ deeper, uint32_t blk,
@@ -344,19 +344,21 @@ __device__ __forceinline__ void ms_bwd_block(const DevGraph &g, const MsBufs<NW>
         if (mw) pack[__popc(bal & ((1u << lane) - 1u))] = Packed<NW>{w, mw};
         __syncwarp();
         const uint32_t c = __popc(bal);
-        for (uint32_t j0 = 0; j0 < c; j0 += 8) {
-            Packed<NW> x[8];
+        constexpr int GB = NW == 1 ? 8 : 4;  // entries per batch: 8 gathers in flight per lane either way
+        for (uint32_t j0 = 0; j0 < c; j0 += GB) {
+            Packed<NW> x[GB];
 #pragma unroll
-            for (int t = 0; t < 8; ++t) x[t] = (j0 + t < c) ? pack[j0 + t] : Packed<NW>{0u, (M)0};
+            for (int t = 0; t < GB; ++t) x[t] = (j0 + t < c) ? pack[j0 + t] : Packed<NW>{0u, (M)0};
+            unsigned long long v[NW][GB];
 #pragma unroll
-            for (int k = 0; k < NW; ++k) {
-                unsigned long long v[8];
+            for (int k = 0; k < NW; ++k)
 #pragma unroll
-                for (int t = 0; t < 8; ++t)
-                    v[t] = has_src(x[t].m, lane, k) ? __ldg(row + (size_t)x[t].w * 32 * NW + lane + 32 * k) : 0ull;
+                for (int t = 0; t < GB; ++t)
+                    v[k][t] = has_src(x[t].m, lane, k) ? __ldg(row + (size_t)x[t].w * 32 * NW + lane + 32 * k) : 0ull;
 #pragma unroll
-                for (int t = 0; t < 8; ++t) acc[k] += as_f64(v[t]);
-            }
+            for (int k = 0; k < NW; ++k)
+#pragma unroll
+                for (int t = 0; t < GB; ++t) acc[k] += as_f64(v[k][t]);
         }
         __syncwarp();
     }
@@ -461,7 +463,7 @@ __device__ __forceinline__ void ms_bwd_heavy(const DevGraph &g, const MsBufs<NW>
 }
 
 template <int NW>
-__global__ void __launch_bounds__(MS_THREADS, NW == 1 ? 4 : 3) k_ms_bwd(DevGraph g, MsBufs<NW> b,
+__global__ void __launch_bounds__(MS_THREADS, 4) k_ms_bwd(DevGraph g, MsBufs<NW> b,
                                                        const typename MaskOf<NW>::type *__restrict__ mask,
                                                        const typename MaskOf<NW>::type *__restrict__ deeper) {
     uint32_t vb, vgl, vgh;
