@@ -2205,16 +2205,19 @@ __device__ __forceinline__ void ppr_finish(const DevGraph &g, const PprBatch &a,
     res += (double)fabsf(xv - a.xold[at]);
 }
 
-__global__ void __launch_bounds__(AN_THREADS) k_ppr_light(DevGraph g, PprBatch a) {
+// Warp per vertex of the thread-per-vertex and lane-group tiers (it.tiny,
+// then it.light), lane = query; CTA vb of vg, residual slot vb.
+__device__ __forceinline__ void ppr_light_body(const DevGraph &g, const PprBatch &a, const Items &it, uint32_t vb,
+                                               uint32_t vg) {
     __shared__ double red[AN_THREADS / 32][32];
     if (a.state[0]) return;
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     double res = 0.0;
-    const uint32_t nw = gridDim.x * (AN_THREADS / 32);
-    for (uint32_t v = blockIdx.x * (AN_THREADS / 32) + warp; v < g.n; v += nw) {
+    const uint32_t nw = vg * (AN_THREADS / 32), nv = it.ntiny + it.nlight;
+    for (uint32_t i = vb * (AN_THREADS / 32) + warp; i < nv; i += nw) {
+        const uint32_t v = i < it.ntiny ? it.tiny[i] : it.light[i - it.ntiny];
         const uint4 rec = g.vtx[v];
         const uint32_t fill = rec.y;
-        if (fill > LIGHT_FILL) continue;  // items path
         const uint32_t nb = blocks_for(fill, g.logB);
         const uint32_t my_blk = item_block(g, rec, 0, nb);  // lane k holds block k (nb <= 8)
         float acc = 0.f;
@@ -2236,15 +2239,16 @@ __global__ void __launch_bounds__(AN_THREADS) k_ppr_light(DevGraph g, PprBatch a
     if (warp == 0) {
         double t = 0.0;
         for (int w = 0; w < AN_THREADS / 32; ++w) t += red[w][lane];
-        a.partial[(size_t)blockIdx.x * 32 + lane] = t;
+        a.partial[(size_t)vb * 32 + lane] = t;
     }
 }
 
-__global__ void __launch_bounds__(AN_THREADS) k_ppr_items(DevGraph g, PprBatch a, Items it, float *__restrict__ ipart) {
+__device__ __forceinline__ void ppr_items_body(const DevGraph &g, const PprBatch &a, const Items &it,
+                                               float *__restrict__ ipart, uint32_t vb, uint32_t vg) {
     if (a.state[0]) return;
     const uint32_t lane = threadIdx.x & 31;
-    const uint32_t nw = gridDim.x * (AN_THREADS / 32);
-    for (uint32_t i = blockIdx.x * (AN_THREADS / 32) + (threadIdx.x >> 5); i < it.nitems; i += nw) {
+    const uint32_t nw = vg * (AN_THREADS / 32);
+    for (uint32_t i = vb * (AN_THREADS / 32) + (threadIdx.x >> 5); i < it.nitems; i += nw) {
         const uint32_t v = it.item_vertex[i];
         const uint32_t c = i - it.item_first[v];
         const uint4 rec = g.vtx[v];
@@ -2266,6 +2270,14 @@ __global__ void __launch_bounds__(AN_THREADS) k_ppr_items(DevGraph g, PprBatch a
         }
         ipart[(size_t)i * 32 + lane] = acc;
     }
+}
+
+// One launch for both parts of a batched sweep: CTA i takes the warp-per-
+// vertex part when i is even (residual slot i / 2), the hub items when odd.
+__global__ void __launch_bounds__(AN_THREADS) k_ppr_fused(DevGraph g, PprBatch a, Items it, float *__restrict__ ipart) {
+    const uint32_t vb = blockIdx.x >> 1, vg = gridDim.x >> 1;
+    if ((blockIdx.x & 1u) == 0) ppr_light_body(g, a, it, vb, vg);
+    else ppr_items_body(g, a, it, ipart, vb, vg);
 }
 
 __global__ void __launch_bounds__(AN_THREADS) k_ppr_items_fin(DevGraph g, PprBatch a, Items it,
@@ -2356,11 +2368,9 @@ gv_status ppr_batch_impl(gv_graph *g, const uint32_t *sources, uint32_t k, float
         for (int i = 0; i < chunk; ++i) {
             PprBatch a{k, dsrc, alpha, c[cur], x[cur], x[cur ^ 1], c[cur ^ 1], partial, state};
             ProfScope ps(PROF_PULL, s);
-            GV_LAUNCH(k_ppr_light, PULL_GRID, AN_THREADS, 0, s, d, a);
-            if (it.nitems) {
-                GV_LAUNCH(k_ppr_items, PULL_GRID, AN_THREADS, 0, s, d, a, it, ipart);
+            GV_LAUNCH(k_ppr_fused, 2 * PULL_GRID, AN_THREADS, 0, s, d, a, it, ipart);
+            if (it.nitems)
                 GV_LAUNCH(k_ppr_items_fin, FIN_GRID, AN_THREADS, 0, s, d, a, it, (const float *)ipart, PULL_GRID);
-            }
             GV_LAUNCH(k_ppr_done, 1, 32, 0, s, (const double *)partial, nparts, k, eps, state);
             cur ^= 1;
         }
