@@ -829,12 +829,25 @@ def run_gv(args, rank, world, local_rank):
             if dom in tj and tj[dom].get("bytes_per_unit"):
                 units = {"pull": m_now, "tc_count": tc_work, "tc_probe": tc_probes}[dom]
                 traffic = tj[dom]["bytes_per_unit"] * units
+        if dom == "pull":  # the variant that counts the gathered ranks as well
+            roof_extra = {"achieved_8m_12n": (8 * m_now + 12 * n) / per_launch_s / 1e9}
+        else:
+            roof_extra = {}
         roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                 "frac": achieved / hbm_peak, "traffic": traffic, "algorithmic_bytes": alg,
                 "avg_launch_ms": dom_ms / dom_n, "launches": dom_n, "peak_source": peak_src,
-                "note": unit_note + f"; fraction of {peak_src} HBM copy bandwidth"}
+                "note": unit_note + f"; fraction of {peak_src} HBM copy bandwidth", **roof_extra}
     pr_ms = prof["pull"][0]
     pr_gteps = (m_now * sum(timed_sweeps)) / (pr_ms / 1e3) / 1e9 if pr_ms else None
+    # betweenness calls in the timed region: TEPS = m * sources / device time
+    bc_calls = sum(1 for i in range(args.steps) if ((args.warmup + i) % args.bc_every) == args.bc_every - 1)
+    bc_ms = prof["bfs_level"][0] + prof["bc_dep"][0]
+    bc_info = None
+    if bc_calls and bc_ms:
+        bc_info = {"sources": args.bc_sources, "calls": bc_calls, "ms_per_call": bc_ms / bc_calls,
+                   "forward_ms_per_call": prof["bfs_level"][0] / bc_calls,
+                   "dependency_ms_per_call": prof["bc_dep"][0] / bc_calls,
+                   "gteps": m_now * args.bc_sources * bc_calls / (bc_ms / 1e3) / 1e9}
     phases = {k: {"ms_total": v[0], "launches": v[1]} for k, v in prof.items() if v[1]}
     line = {"metric": METRIC, "value": value, "unit": "edge updates/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
@@ -842,6 +855,7 @@ def run_gv(args, rank, world, local_rank):
             "data": "synthetic (seeded R-MAT graph, uniform-random inserts, deletes sampled from existing edges)",
             "config": workload_config(args, n, m0),
             "pagerank_gteps": pr_gteps, "pagerank_sweeps_avg": avg_sweeps, "m_entries": m_now,
+            "betweenness": bc_info,
             "triangles": {"merged_entries": tc_work, "core_probes": tc_probes, "core_vertices": tc_core},
             "kernel_ms": phases, "roofline": roof, "gpu_launches": launches, "clocks": clocks}
     if incr:
