@@ -338,6 +338,28 @@ def test_total_triangles_dense_core(core, monkeypatch, graph12):
     g2.close()
 
 
+def test_core_list_order_does_not_change_counts(monkeypatch, graph12):
+    """The bank-spreading reorder of the core lists (GV_TC_COLOR) changes
+    only the order in which entries are tested."""
+    n, g, o = graph12
+    monkeypatch.setenv("GV_TC_CORE", "1000")
+    _, otot = o.tc()
+    for color in ("0", "1"):
+        monkeypatch.setenv("GV_TC_COLOR", color)
+        assert g.static_tc(per_vertex=False)[1] == otot
+
+
+def test_sweep_split_does_not_change_pagerank(monkeypatch, graph12):
+    """The fused sweep's CTA shares per tier (GV_SWEEP_SPLIT) move work
+    between CTAs, never between lanes: the ranks are bit-for-bit the same."""
+    n, g, o = graph12
+    ref, sw = g.static_pagerank(0.85, 1e-6, 100)
+    for split in ("1,1,14", "8,4,4", "5,5,6"):
+        monkeypatch.setenv("GV_SWEEP_SPLIT", split)
+        x, sw2 = g.static_pagerank(0.85, 1e-6, 100)
+        assert sw2 == sw and np.array_equal(x, ref), split
+
+
 def test_total_triangles_core_with_hub_clique(monkeypatch):
     """A 1100-clique inside an R-MAT graph: the clique members form the core
     and their rows hold 1099-entry lists."""
