@@ -250,6 +250,16 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def max_over_ranks(values, device, dist=None):
+    """Element-wise maximum of each rank's timings (every rank gets it): the
+    job is as slow as its slowest replica."""
+    import torch
+    t = torch.tensor(values, dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t]
+
+
 def workload_config(args, n, m0):
     return {"workload": (f"plain method at scale: undirected R-MAT scale {args.scale} ef {args.edge_factor}; "
                          f"per step {args.batch} updates ({args.batch // 2} inserts + {args.batch // 2} deletes) "
@@ -790,11 +800,7 @@ def run_gv(args, rank, world, local_rank):
             incr["sizes"][str(2 * k)] = {"update_tc_ms": statistics.mean(rec["update_tc_ms"]),
                                          "update_then_static_tc_ms": statistics.mean(rec["update_then_static_tc_ms"])}
         incr["triangles_after"] = int(t_ref)
-    # max over ranks
-    t = torch.tensor([elapsed_ms, e2e["ms"] if e2e else 0.0], dtype=torch.float64, device=dev)
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    elapsed_ms, e2e_ms = float(t[0]), float(t[1])
+    elapsed_ms, e2e_ms = max_over_ranks([elapsed_ms, e2e["ms"] if e2e else 0.0], dev, dist)
     g.close()
     if rank != 0:
         return
