@@ -338,6 +338,25 @@ def test_total_triangles_dense_core(core, monkeypatch, graph12):
     g2.close()
 
 
+def test_total_triangles_without_a_core():
+    """30000 disjoint triangles: every vertex has degree 2, so no degree
+    threshold leaves at most 65504 vertices above it and every edge takes
+    the merge path; and an empty graph counts 0."""
+    k = 30000
+    n = 3 * k
+    a = np.arange(k, dtype=np.uint32) * 3
+    s = np.concatenate([a, a + 1, a + 2])
+    d = np.concatenate([a + 1, a + 2, a])
+    g = make_graph(n)
+    g.batch_insert(s, d)
+    assert g.static_tc(per_vertex=False)[1] == k
+    assert g.last_stat("tc_core") == 0 and g.last_stat("tc_probes") == 0
+    e = make_graph(64)
+    assert e.static_tc(per_vertex=False)[1] == 0
+    g.close()
+    e.close()
+
+
 def test_core_list_order_does_not_change_counts(monkeypatch, graph12):
     """The bank-spreading reorder of the core lists (GV_TC_COLOR) changes
     only the order in which entries are tested."""
