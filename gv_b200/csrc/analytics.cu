@@ -474,7 +474,8 @@ uint32_t sweep_split(const unsigned long long *tier) {
 
 // Builds the chunked item list of the current graph (aux scratch slots 1, 2);
 // *ipart gets one 4-byte slot per item.
-gv_status build_items(gv_graph *g, cudaStream_t s, unsigned long long *nmulti, Items *it, float **ipart) {
+gv_status build_items(gv_graph *g, cudaStream_t s, unsigned long long *nmulti, Items *it, float **ipart,
+                      bool tiers = true) {
     DevGraph d = g->d;
     const uint32_t n = d.n;
     // first, multi, the two tier position arrays (n + 1 each), the two tier lists (n each), counters
@@ -483,10 +484,15 @@ gv_status build_items(gv_graph *g, cudaStream_t s, unsigned long long *nmulti, I
     uint32_t *multi = first + (n + 1);
     uint32_t *pl = multi + (n + 1), *pt = pl + (n + 1), *light = pt + (n + 1), *tiny = light + n;
     unsigned long long *tier = (unsigned long long *)(((uintptr_t)(tiny + n) + 7) & ~(uintptr_t)7);
-    GV_LAUNCH(k_tier_flags, grid_for(n, 256), 256, 0, s, d, pl, pt);
-    scan_exclusive_u32(pl, pl, n, pl + n, g->bs.scan_tmp, s);
-    scan_exclusive_u32(pt, pt, n, pt + n, g->bs.scan_tmp, s);
-    GV_LAUNCH(k_tier_lists, grid_for(n, 256), 256, 0, s, d, (const uint32_t *)pl, (const uint32_t *)pt, light, tiny);
+    if (tiers) {  // the sweeps' tier lists (the triangle snapshot needs only the items)
+        GV_LAUNCH(k_tier_flags, grid_for(n, 256), 256, 0, s, d, pl, pt);
+        scan_exclusive_u32(pl, pl, n, pl + n, g->bs.scan_tmp, s);
+        scan_exclusive_u32(pt, pt, n, pt + n, g->bs.scan_tmp, s);
+        GV_LAUNCH(k_tier_lists, grid_for(n, 256), 256, 0, s, d, (const uint32_t *)pl, (const uint32_t *)pt, light, tiny);
+    } else {
+        cudaMemsetAsync(pl + n, 0, 4, s);
+        cudaMemsetAsync(pt + n, 0, 4, s);
+    }
     cudaMemsetAsync(nmulti, 0, 8, s);
     cudaMemsetAsync(tier, 0, 5 * 8, s);
     GV_LAUNCH(k_item_count, grid_for(n, 256), 256, 0, s, d, first, multi, nmulti, tier);
@@ -1875,7 +1881,7 @@ gv_status tc_run(gv_graph *g, cudaStream_t s, int mode, unsigned long long **tco
         cudaMemsetAsync(b.cnts, 0, 64, s);
         Items it{};
         float *ip = nullptr;
-        gv_status st = build_items(g, s, b.cnts + 3, &it, &ip);
+        gv_status st = build_items(g, s, b.cnts + 3, &it, &ip, false);
         if (st != GV_OK) return st;
         uint32_t *icnt = (uint32_t *)ip;
         uint32_t *ioff = nullptr;
