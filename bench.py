@@ -464,11 +464,16 @@ def run_ingest(args):
     host = torch.frombuffer(bytearray(text), dtype=torch.uint8).pin_memory()
     dev = host.cuda()
     gv_b200.mtx_parse(dev)  # warm-up
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    meta, src, dst, _ = gv_b200.mtx_parse(dev)
-    torch.cuda.synchronize()
-    dev_s = time.perf_counter() - t0
+    # each call sizes and parses the text and allocates its own scratch and
+    # outputs, whose allocation time varies from call to call: best of five
+    times = []
+    for _ in range(5):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        meta, src, dst, _ = gv_b200.mtx_parse(dev)
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t0)
+    dev_s = min(times)
     ok = bool(np.array_equal(src[:1000].cpu().numpy().view(np.uint32), s[:1000]))
     t0 = time.perf_counter()
     gv_b200.mtx_parse(host.numpy().tobytes())
@@ -476,6 +481,7 @@ def run_ingest(args):
     out = {"workload": f"R-MAT scale {scale} ef {args.edge_factor} as Matrix-Market text",
            "text_bytes": len(text), "entries": int(meta["entries"]), "first_entries_match": ok,
            "device_text_gb_s": len(text) / dev_s / 1e9, "device_text_entries_per_s": meta["entries"] / dev_s,
+           "device_calls_s": times,
            "host_text_gb_s": len(text) / host_s / 1e9,
            "host_note": "host text: pageable copy, host header read, device parse and copy back of the ids"}
     with tempfile.TemporaryDirectory() as td:
