@@ -756,6 +756,10 @@ extern "C" gv_status gv_bc(gv_graph *g, const uint32_t *sources, uint64_t ns, fl
 extern "C" gv_status gv_bc_multi(gv_graph *g, const uint32_t *sources, const uint64_t *offsets, uint32_t nreq,
                                  float *bc_out, int mem, void *stream) {
     if (!g || !bc_out || !offsets || nreq == 0) return GV_ERR_INVALID;
+    if ((uint64_t)nreq * std::max<uint32_t>(g->d.n, 1) > (1ull << 40)) {  // fp64 score rows in device scratch
+        set_error("too many BC requests for one call");
+        return GV_ERR_INVALID;
+    }
     for (uint32_t r = 0; r < nreq; ++r)
         if (offsets[r + 1] < offsets[r]) { set_error("request offsets must not decrease"); return GV_ERR_INVALID; }
     if (offsets[0] != 0) { set_error("request offsets start at 0"); return GV_ERR_INVALID; }
