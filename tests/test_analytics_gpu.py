@@ -173,6 +173,21 @@ def test_bc_pass_widths(graph12, count):
     assert np.all(b[ob == 0] == 0)
 
 
+def test_bc_pull_levels_give_the_same_scores(monkeypatch, graph12):
+    """Forward levels by pull (GV_BC_PULL, from rarely to nearly always) or by
+    push give the same path counts, so the scores are bit-for-bit equal."""
+    n, g, o = graph12
+    src = np.random.default_rng(12).choice(n, 64, replace=False).astype(np.uint32)
+    monkeypatch.setenv("GV_BC_PULL", "0")
+    ref = g.bc(src)
+    for alpha in ("1", "2", "1000"):
+        monkeypatch.setenv("GV_BC_PULL", alpha)
+        assert np.array_equal(g.bc(src), ref), alpha
+    ob = o.bc(src)
+    rel = np.max(np.abs(ref - ob) / np.maximum(np.abs(ob), 1e-300) * (ob != 0))
+    assert rel < BC_REL
+
+
 def test_bc_multi_matches_single(graph12):
     """Requests paired into shared passes score as they do alone."""
     n, g, o = graph12
