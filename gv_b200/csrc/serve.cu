@@ -58,7 +58,7 @@ struct Server {
         switch (kind) {
             case GV_REQ_PPR: return 20ull * n * k + 16ull * n;  // 4 iterate blocks + the result block
             case GV_REQ_TC: return 64ull * n + 8ull * g->d.P * g->d.B / 2;
-            default: return 512ull * n + 8ull * 32 * n + 32ull * n + 12ull * n * k;  // BC: sigma rows, 32 level masks, lists, scores
+            default: return 512ull * n + 8ull * 32 * n + 48ull * n + 12ull * n * k;  // BC: sigma rows, 32 level masks, lists, scores
         }
     }
 
