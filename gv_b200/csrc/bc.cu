@@ -74,7 +74,8 @@ struct MsBufs {
     double *bc;               // [outputs][n]; half k of the pass adds into row out[k]
     uint32_t *clight;         // pull levels: vertices some source has not reached, fill <= MS_HEAVY_FILL
     uint32_t *cheavy;         // the rest of them
-    unsigned long long *esum; // [0] entries of the level's vertices, [1] entries of the candidates
+    unsigned long long *esum; // [0] entries of the level's vertices; [1] entries of the vertices some
+                              // source has not reached (counted down by k_ms_close as vertices fill up)
     M full;                   // the pass's sources
     uint32_t alpha;           // pull when alpha * esum[0] > esum[1] (0: always push)
     uint32_t n;
@@ -250,10 +251,11 @@ __device__ __forceinline__ bool ms_pull_level(const MsBufs<NW> &b) {
 }
 
 // Candidates of a pull level: vertices with entries that some source of the
-// pass has not reached (warp-aggregated appends), and their entry count.
+// pass has not reached (warp-aggregated appends); nothing on push levels.
 template <int NW>
 __global__ void k_ms_cand(DevGraph g, MsBufs<NW> b) {
     using M = typename MaskOf<NW>::type;
+    if (!ms_pull_level(b)) return;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t n = b.n;
     for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
@@ -268,14 +270,11 @@ __global__ void k_ms_cand(DevGraph g, MsBufs<NW> b) {
                 heavy = fill > MS_HEAVY_FILL;
             }
         }
-        if (!on) fill = 0;
         const uint32_t bl = __ballot_sync(GV_FULL_MASK, on && !heavy), bh = __ballot_sync(GV_FULL_MASK, on && heavy);
-        const unsigned long long es = warp_sum((unsigned long long)fill);
         uint32_t ol = 0, oh = 0;
         if (lane == 0) {
             if (bl) ol = atomicAdd(&b.cnt[2], __popc(bl));
             if (bh) oh = atomicAdd(&b.cnt[3], __popc(bh));
-            if (es) atomicAdd(&b.esum[1], es);
         }
         ol = __shfl_sync(GV_FULL_MASK, ol, 0);
         oh = __shfl_sync(GV_FULL_MASK, oh, 0);
@@ -283,6 +282,15 @@ __global__ void k_ms_cand(DevGraph g, MsBufs<NW> b) {
         if (on && !heavy) b.clight[ol + __popc(bl & below)] = v;
         if (on && heavy) b.cheavy[oh + __popc(bh & below)] = v;
     }
+}
+
+// Entries of every vertex, the pull levels' starting count of entries of
+// vertices some source has not reached.
+__global__ void k_ms_total_fill(DevGraph g, unsigned long long *__restrict__ out) {
+    unsigned long long t = 0;
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < g.n; v += gridDim.x * blockDim.x) t += g.vtx[v].y;
+    t = warp_sum(t);
+    if ((threadIdx.x & 31u) == 0 && t) atomicAdd(out, t);
 }
 
 template <typename M>
@@ -517,7 +525,8 @@ __global__ void __launch_bounds__(MS_THREADS, 4) k_ms_pull(DevGraph g, MsBufs<NW
 
 // Closes level L: masks[L+1] = nxt, vis |= nxt, flags[L+1] = any.
 template <int NW>
-__global__ void k_ms_close(MsBufs<NW> b, typename MaskOf<NW>::type *__restrict__ next_mask, uint32_t *flag) {
+__global__ void k_ms_close(DevGraph g, MsBufs<NW> b, typename MaskOf<NW>::type *__restrict__ next_mask,
+                           uint32_t *flag) {
     using M = typename MaskOf<NW>::type;
     __shared__ int any;
     if (threadIdx.x == 0) any = 0;
@@ -527,9 +536,13 @@ __global__ void k_ms_close(MsBufs<NW> b, typename MaskOf<NW>::type *__restrict__
         const M x = b.nxt[v];
         next_mask[v] = x;
         if (x) {
-            b.vis[v] |= x;
+            const M old = b.vis[v];
+            b.vis[v] = old | x;
             b.nxt[v] = 0;
             mine = true;
+            // every source has reached v: its entries leave the pull levels' count
+            if (b.alpha && (old | x) == b.full && old != b.full)
+                atomicAdd(&b.esum[1], 0ull - (unsigned long long)g.vtx[v].y);
         }
     }
     if (mine) any = 1;
@@ -763,6 +776,10 @@ gv_status ms_forward(gv_graph *g, MsBufs<NW> &b, const uint32_t *dsrc, uint32_t 
     cudaMemsetAsync(b.nxt, 0, (size_t)n * sizeof(M), s);
     cudaMemsetAsync(b.masks, 0, (size_t)n * sizeof(M), s);
     GV_LAUNCH(k_ms_init<NW>, 1, 32 * NW, 0, s, b, dsrc);
+    if (b.alpha) {
+        cudaMemsetAsync(b.esum + 1, 0, 8, s);
+        GV_LAUNCH(k_ms_total_fill, grid_for(n, 256), 256, 0, s, d, b.esum + 1);
+    }
     const uint32_t chunk = 4;
     uint32_t L = 0;
     for (;;) {
@@ -773,7 +790,7 @@ gv_status ms_forward(gv_graph *g, MsBufs<NW> &b, const uint32_t *dsrc, uint32_t 
             const M *mask = b.masks + (size_t)L * n;
             ProfScope ps(PROF_BFS_LEVEL, s);
             cudaMemsetAsync(b.cnt, 0, 16, s);
-            cudaMemsetAsync(b.esum, 0, 16, s);
+            cudaMemsetAsync(b.esum, 0, 8, s);
             GV_LAUNCH(k_ms_split<NW>, grid_for(n, 256), 256, 0, s, d, b, mask);
             static_assert(MS_LIGHT_GRID == 4 * MS_HEAVY_GRID, "the fused launch interleaves 4 light CTAs per heavy one");
             if (b.alpha) {
@@ -781,7 +798,7 @@ gv_status ms_forward(gv_graph *g, MsBufs<NW> &b, const uint32_t *dsrc, uint32_t 
                 GV_LAUNCH(k_ms_pull<NW>, MS_LIGHT_GRID + MS_HEAVY_GRID, MS_THREADS, 0, s, d, b, mask);
             }
             GV_LAUNCH(k_ms_fwd<NW>, MS_LIGHT_GRID + MS_HEAVY_GRID, MS_THREADS, 0, s, d, b, mask);
-            GV_LAUNCH(k_ms_close<NW>, grid_for(n, 256), 256, 0, s, b, b.masks + (size_t)(L + 1) * n, b.flags + L + 1);
+            GV_LAUNCH(k_ms_close<NW>, grid_for(n, 256), 256, 0, s, d, b, b.masks + (size_t)(L + 1) * n, b.flags + L + 1);
         }
         cudaError_t e = cudaMemcpyAsync(h_flags, b.flags + L - chunk + 1, chunk * 4, cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -852,7 +869,7 @@ gv_status ms_setup(gv_graph *g, uint32_t nw, uint32_t outputs, MsArena &a) {
 // Pull levels: a forward level of a 64-source pass pulls when MS_PULL_ALPHA
 // times its own entries exceed the entries of the vertices some source has
 // not reached; GV_BC_PULL=<alpha> overrides it (0: push every level).  On
-// R-MAT scale 22 this takes the forward of 64 sources from 21.1 to 17.4 ms;
+// R-MAT scale 22 this takes the forward of 64 sources from 21.1 to 15.2 ms;
 // 32-source passes push every level (pull levels made them slower: their
 // push adds touch half the row bytes).
 constexpr uint32_t MS_PULL_ALPHA = 2;
