@@ -48,7 +48,7 @@ def parse():
     ap.add_argument("--bc-every", type=int, default=5)
     ap.add_argument("--bc-sources", type=int, default=64)
     ap.add_argument("--block", type=int, default=128)
-    ap.add_argument("--tpv", type=int, default=8)
+    ap.add_argument("--tpv", type=int, default=16)
     ap.add_argument("--seed", type=int, default=2026)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
