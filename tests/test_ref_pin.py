@@ -92,9 +92,14 @@ def test_reference_matches_oracle_and_libgv(tmp_path):
     if not HARNESS.exists():
         pytest.skip("reference harness not built (oracle/ref_build.py)")
     import torch
+    import gc
+    gc.collect()
+    torch.cuda.empty_cache()
     free, total = torch.cuda.mem_get_info()
-    if free < 0.55 * total:
-        pytest.skip("the reference needs half of the GPU's memory free")
+    # the reference takes half of the GPU's total memory for its pool, unchecked,
+    # and then allocates its batch buffers beside it
+    if free < 0.65 * total:
+        pytest.skip("the reference needs well over half of the GPU's memory free")
     n = 2048
     rng = np.random.default_rng(20261203)
     base, ins, dele = _workload(n, rng)
