@@ -49,7 +49,7 @@ struct gv_graph {
     int32_t last_tc_local = 0;  // 1: the last subset count took the local path
     int32_t last_sweeps = 0;
     // independent auxiliary device buffers, grown on demand
-    static constexpr int AUX_SLOTS = 11;
+    static constexpr int AUX_SLOTS = 12;
     void *aux[AUX_SLOTS] = {};
     size_t aux_bytes[AUX_SLOTS] = {};
     // a view shares the parent's store and owns only analytics scratch

@@ -688,18 +688,18 @@ static gv_status td_pairs(gv_graph *g, const uint32_t *dsrc, const uint32_t *dds
     return GV_OK;
 }
 
-// Counts the triangles of the current graph through the `cnt` changed pairs.
-static gv_status td_count(gv_graph *g, const unsigned long long *pairs, uint32_t cnt, unsigned long long *total,
-                          long long *owner, long long sign, uint32_t *err, cudaStream_t s) {
-    if (cnt == 0) return GV_OK;
+// Neighbour tables of the heavy endpoints of the changed pairs (slots 8 and
+// 9), built once for both halves of a batch: the created pairs are counted
+// after the inserts and the destroyed ones before the deletes, on the same
+// graph.
+struct TdTables {
+    const uint32_t *hidx = nullptr, *hlog = nullptr, *gtab = nullptr;
+    const unsigned long long *hoff = nullptr;
+};
+
+static gv_status td_tables(gv_graph *g, const unsigned long long *const *lists, const uint32_t *counts, int nlists,
+                           uint32_t *err, TdTables *out, cudaStream_t s) {
     const uint32_t n = g->d.n;
-    uint32_t log = 10;
-    while ((1ull << log) < 2ull * cnt) ++log;
-    unsigned long long *set = (unsigned long long *)aux_scratch(g, 5, (8ull << log) + 256);
-    if (!set) return GV_ERR_NOMEM;
-    cudaMemsetAsync(set, 0xFF, 8ull << log, s);
-    GV_LAUNCH(k_td_set_build, grid_for(cnt, 256), 256, 0, s, pairs, cnt, set, log, err);
-    // heavy endpoints: flag, list, table sizes and offsets (slot 8), tables (slot 9)
     auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
     const size_t o_flag = 0, o_list = al((size_t)n * 4), o_hidx = o_list + al((size_t)n * 4);
     const size_t o_log = o_hidx + al((size_t)n * 4), o_cap = o_log + al((size_t)n * 4);
@@ -713,7 +713,9 @@ static gv_status td_count(gv_graph *g, const unsigned long long *pairs, uint32_t
     uint32_t *nh = reinterpret_cast<uint32_t *>(hoff + n);  // scratch word until the scan writes the offsets
     cudaMemsetAsync(flag, 0, (size_t)n * 4, s);
     cudaMemsetAsync(nh, 0, 4, s);
-    GV_LAUNCH(k_td_mark, grid_for(cnt, 256), 256, 0, s, g->d, pairs, cnt, g->bitsn, flag, hlist, nh);
+    for (int l = 0; l < nlists; ++l)
+        if (counts[l])
+            GV_LAUNCH(k_td_mark, grid_for(counts[l], 256), 256, 0, s, g->d, lists[l], counts[l], g->bitsn, flag, hlist, nh);
     uint32_t hn = 0;
     cudaError_t e = cudaMemcpyAsync(&hn, nh, 4, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -735,9 +737,26 @@ static gv_status td_count(gv_graph *g, const unsigned long long *pairs, uint32_t
         GV_LAUNCH(k_td_build, std::min<uint32_t>(hn, 148 * 8), TD_THREADS, 0, s, g->d, (const uint32_t *)hlist,
                   (const uint32_t *)dn, (const unsigned long long *)hoff, (const uint32_t *)hlog, gtab, err);
     }
+    out->hidx = hidx;
+    out->hlog = hlog;
+    out->hoff = hoff;
+    out->gtab = gtab;
+    return cuda_status(cudaGetLastError(), "tc delta tables");
+}
+
+// Counts the triangles of the current graph through the `cnt` changed pairs
+// (the set of those pairs decides at which changed edge a triangle counts).
+static gv_status td_count(gv_graph *g, const unsigned long long *pairs, uint32_t cnt, const TdTables &t,
+                          unsigned long long *total, long long *owner, long long sign, uint32_t *err, cudaStream_t s) {
+    if (cnt == 0) return GV_OK;
+    uint32_t log = 10;
+    while ((1ull << log) < 2ull * cnt) ++log;
+    unsigned long long *set = (unsigned long long *)aux_scratch(g, 5, (8ull << log) + 256);
+    if (!set) return GV_ERR_NOMEM;
+    cudaMemsetAsync(set, 0xFF, 8ull << log, s);
+    GV_LAUNCH(k_td_set_build, grid_for(cnt, 256), 256, 0, s, pairs, cnt, set, log, err);
     GV_LAUNCH(k_td_count, grid_for(cnt, TD_WARPS, 148 * 8), TD_THREADS, 0, s, g->d, pairs, cnt, g->bitsn,
-              (const unsigned long long *)set, log, (const uint32_t *)hidx, (const unsigned long long *)hoff,
-              (const uint32_t *)hlog, (const uint32_t *)gtab, total, owner, sign, err);
+              (const unsigned long long *)set, log, t.hidx, t.hoff, t.hlog, t.gtab, total, owner, sign, err);
     return cuda_status(cudaGetLastError(), "tc delta count");
 }
 
@@ -794,7 +813,8 @@ extern "C" gv_status gv_update_tc(gv_graph *g, const uint32_t *ins_src, const ui
         if (!owner) return GV_ERR_NOMEM;
         cudaMemsetAsync(owner, 0, (size_t)n * 8, s);
     }
-    // inserts: the new pairs A (absent now), applied, then the triangles through A
+    // inserts: the new pairs A (absent now), then applied; the triangles through
+    // A are counted on the graph after the inserts
     unsigned long long *pairs = nullptr;
     uint32_t cnt = 0;
     gv_status st = GV_OK;
@@ -807,19 +827,38 @@ extern "C" gv_status gv_update_tc(gv_graph *g, const uint32_t *ins_src, const ui
     }
     st = td_pairs(g, is, id, n_ins, 0u, &pairs, &cnt, s);
     if (st != GV_OK) return st;
+    // A moves out of the pair scratch (slot 11), which the deletes' pairs reuse
+    unsigned long long *apairs = nullptr;
+    const uint32_t acnt = cnt;
+    if (acnt) {
+        apairs = (unsigned long long *)aux_scratch(g, 11, (size_t)acnt * 8 + 256);
+        if (!apairs) return GV_ERR_NOMEM;
+        cudaError_t e = cudaMemcpyAsync(apairs, pairs, (size_t)acnt * 8, cudaMemcpyDeviceToDevice, s);
+        if (e != cudaSuccess) return cuda_status(e, "tc delta pairs");
+    }
     if (n_ins) {
         st = gv_insert_edges(g, is, id, iw, n_ins, GV_MEM_DEVICE, stream);
         if (st == GV_OK) st = gv_synchronize(g, stream);
         if (st != GV_OK) return st;
     }
-    st = td_count(g, pairs, cnt, words + 0, owner, 1, err, s);
-    if (st != GV_OK) return st;
-    // deletes: the pairs present now R, the triangles through R, then applied
+    // deletes: the pairs present now R; A and R are counted on this graph with
+    // one set of neighbour tables, then the deletes are applied
+    uint32_t rcnt = 0;
+    unsigned long long *rpairs = nullptr;
     if (n_del) {
-        st = td_pairs(g, ds, dd, n_del, 1u, &pairs, &cnt, s);
+        st = td_pairs(g, ds, dd, n_del, 1u, &rpairs, &rcnt, s);
         if (st != GV_OK) return st;
-        st = td_count(g, pairs, cnt, words + 1, owner, -1, err, s);
+    }
+    if (acnt || rcnt) {
+        const unsigned long long *lists[2] = {apairs, rpairs};
+        const uint32_t counts[2] = {acnt, rcnt};
+        TdTables tabs;
+        st = td_tables(g, lists, counts, 2, err, &tabs, s);
+        if (st == GV_OK) st = td_count(g, apairs, acnt, tabs, words + 0, owner, 1, err, s);
+        if (st == GV_OK) st = td_count(g, rpairs, rcnt, tabs, words + 1, owner, -1, err, s);
         if (st != GV_OK) return st;
+    }
+    if (n_del) {
         st = gv_delete_edges(g, ds, dd, n_del, GV_MEM_DEVICE, stream);
         if (st == GV_OK) st = gv_synchronize(g, stream);
         if (st != GV_OK) return st;
