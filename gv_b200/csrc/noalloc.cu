@@ -1,23 +1,29 @@
 // PageRank that allocates nothing: gv_pagerank_noalloc.
 //
 // Some callers cannot call cudaMalloc at the moment they need a result:
-// code running while a CUDA graph is being captured (allocation calls are
-// not allowed during capture), serving threads on a latency budget (a
-// device allocation may synchronise the device and stall other streams),
-// and hosts that hand all device memory to their own arena up front.  This
-// entry point serves them: its scratch is a file-scope __device__ array of
-// fixed size, so the call itself never allocates; the caller passes the
-// graph and a device output buffer.
+// serving threads on a latency budget (a device allocation may synchronise
+// the device and stall the other streams' work), and hosts that hand all
+// device memory to their own arena up front, so that a later cudaMalloc
+// fails or takes memory the arena counts on.  This entry point serves them:
+// its scratch is a file-scope __device__ array of fixed size, so the call
+// itself never allocates; the caller passes the graph and a device output
+// buffer.
 //
 // Limits and rules:
+//   * undirected (symmetric) stores only (a directed store -> GV_ERR_STATE);
 //   * graphs of at most GV_NOALLOC_MAX_VERTICES vertices (larger -> GV_ERR_CAPACITY);
 //   * every GPU that loads libgv holds the array (about 16 MiB) until exit;
-//   * all calls on a device share the one array: calls that overlap on the
-//     GPU (different streams, or different graphs at the same time) race
-//     and must be serialised by the caller;
+//   * all calls on a device share the one array, which keeps the last call's
+//     contents: calls that overlap on the GPU (different streams, or
+//     different graphs at the same time) race and must be serialised by the
+//     caller;
 //   * the first call on a device looks up the array's device address
-//     (cudaGetSymbolAddress) with that device current; make that first call
-//     before any stream capture.
+//     (cudaGetSymbolAddress) with that device current and keeps it for the
+//     life of the process; make that first call before any stream capture.
+//     The kept address does not survive cudaDeviceReset: a process that
+//     resets the device must not call this entry point afterwards.
+//   * the call synchronises on `stream`: every 8 sweeps it reads the
+//     convergence flag back to the host.
 #include <mutex>
 #include "store.cuh"
 #include "group.cuh"
@@ -168,7 +174,7 @@ extern "C" gv_status gv_pagerank_noalloc(gv_graph *g, float alpha, float epsilon
     // the array keeps the previous call's contents: clear what must start at zero
     cudaError_t e = cudaMemsetAsync(state, 0, 4 * sizeof(int), s);
     if (e == cudaSuccess) e = cudaMemsetAsync(partial, 0, NA_GRID * sizeof(double), s);
-    GV_LAUNCH(k_na_init, grid_for(n, 256), 256, 0, s, d, x[0], c[0]);
+    if (e == cudaSuccess) GV_LAUNCH(k_na_init, grid_for(n, 256), 256, 0, s, d, x[0], c[0]);
     const float b = (1.0f - alpha) / (float)n;
     int h_state[2] = {0, 0};
     int launched = 0, cur = 0;

@@ -202,18 +202,23 @@ gv_status gv_pagerank(gv_graph *g, float alpha, float epsilon, int32_t max_iter,
 gv_status gv_pagerank_dynamic(gv_graph *g, float alpha, float epsilon, int32_t max_iter,
                               float *x_inout, int32_t *sweeps, int mem, void *stream);
 
-/* PageRank (same definition as gv_pagerank) that allocates nothing.  No
- * counterpart in the reference.  For callers that cannot allocate device
- * memory when they need the result: code running during CUDA graph stream
- * capture, serving threads that must not stall on an allocation, hosts that
- * hand all device memory to their own arena.  Its scratch is one fixed
- * file-scope device array (about 16 MiB, held by every GPU that loads the
- * library until exit), so graphs are limited to 1048576 vertices (larger:
- * GV_ERR_CAPACITY).  x_out is a caller-owned DEVICE buffer of n floats.
- * All calls on a device share the array: calls that overlap on the GPU race
- * and must be serialised by the caller.  The first call on a device looks
- * up the array's address with that device current; make it before any
- * stream capture.  Synchronous (reads the sweep count). */
+/* PageRank (same definition as gv_pagerank on an undirected store) that
+ * allocates nothing.  No counterpart in the reference.  For callers that
+ * cannot allocate device memory when they need the result: serving threads
+ * that must not stall on an allocation (cudaMalloc may synchronise the
+ * device), and hosts that hand all device memory to their own arena up
+ * front.  Its scratch is one fixed file-scope device array (about 16 MiB,
+ * held by every GPU that loads the library until exit), so graphs are
+ * limited to 1048576 vertices (larger: GV_ERR_CAPACITY).  Undirected
+ * (symmetric) stores only: a directed store gives GV_ERR_STATE (gv_pagerank
+ * handles those through its transposed pull, which needs scratch).  x_out is
+ * a caller-owned DEVICE buffer of n floats.  All calls on a device share the
+ * array, which keeps the last call's contents: calls that overlap on the GPU
+ * race and must be serialised by the caller.  The first call on a device
+ * looks up the array's address with that device current and keeps it for
+ * the process (not valid after cudaDeviceReset); make that first call before
+ * any stream capture.  Synchronous: it reads the convergence flag back every
+ * 8 sweeps and the sweep count at the end. */
 gv_status gv_pagerank_noalloc(gv_graph *g, float alpha, float epsilon, int32_t max_iter,
                               float *x_out, int32_t *sweeps, void *stream);
 

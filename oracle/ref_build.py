@@ -8,9 +8,14 @@ build list (CMakeLists.txt:20-37) minus src/main.cu, whose role the harness
 takes.  Needs nvcc only; the reference's CMake build is not used.
 
     python -m oracle.ref_build [/path/to/reference]
+
+The reference's location comes from the argument, else from the
+GV_REFERENCE_DIR environment variable, else DEFAULT_REFERENCE_DIR (where the
+build container mounts it); when none holds the sources nothing is built.
 """
 from __future__ import annotations
 
+import os
 import subprocess
 import sys
 from pathlib import Path
@@ -30,8 +35,16 @@ INCLUDES = ["include", "include/algorithm/pagerank", "include/algorithm/tc", "in
             "include/dynamicStructure", "include/dynamicStructure/kernels", "include/reader", "include/util", "src"]
 
 
-def build(ref: Path = Path("/root/reference"), force: bool = False) -> Path | None:
-    ref = Path(ref)
+DEFAULT_REFERENCE_DIR = "/root/reference"
+
+
+def reference_dir() -> Path:
+    """The reference checkout: GV_REFERENCE_DIR, else DEFAULT_REFERENCE_DIR."""
+    return Path(os.environ.get("GV_REFERENCE_DIR") or DEFAULT_REFERENCE_DIR)
+
+
+def build(ref: Path | None = None, force: bool = False) -> Path | None:
+    ref = Path(ref) if ref is not None else reference_dir()
     if not (ref / "src").exists():
         return None
     harness = HERE / "ref_harness.cu"
@@ -63,4 +76,4 @@ def build(ref: Path = Path("/root/reference"), force: bool = False) -> Path | No
 
 
 if __name__ == "__main__":
-    print(build(Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference"), force=True))
+    print(build(Path(sys.argv[1]) if len(sys.argv) > 1 else None, force=True))
