@@ -558,71 +558,120 @@ double or_wpr_objective(const or_graph *g, double alpha, double tol, int max_ite
     return j;
 }
 
+// Central differences (J(w + h e_uv) - J(w - h e_uv)) / 2h of J = sum c_i x_i
+// for k raw-weight entries at once.  Changing the raw weight of (u, v) by d
+// changes only row u of the normalised matrix, by r(d) q_u with r = d/(s_u+d)
+// and q_u[j] = ([j == v] s_u - w_uj) / s_u over u's out-entries.  With
+// y = a (I - a T)^-1 q_u (one forward-direction solve per entry, shared by
+// both signs) the perturbed solve is exactly
+//     x(d) - x0 = r x0[u] y / (1 - r y[u])          (rank-one update),
+// so J(d) - J(0) = r x0[u] (c . y) / (1 - r y[u]) is evaluated without
+// subtracting two nearly equal objectives and without stopping a perturbed
+// solve early.  The k solves share each sweep over the transposed matrix
+// (vertex-major rows of k values) and run until every right-hand side's L1
+// step is below rel_tol of its norm.  `tol` bounds the base solve's L1 step.
 int or_wpr_fd(const or_graph *g, double alpha, double tol, int max_iter, const double *c, const uint32_t *eu,
               const uint32_t *ev, uint32_t k, double h, double *fd) {
     const uint32_t n = g->n;
-    // transpose once; pos[u][i] = slot of out-entry i of u in the transpose
+    if (k == 0) return 0;
     std::vector<uint64_t> toff(n + 1, 0);
     for (uint32_t u = 0; u < n; ++u)
         for (uint32_t v : g->adj[u]) toff[v + 1]++;
     for (uint32_t v = 0; v < n; ++v) toff[v + 1] += toff[v];
     std::vector<uint32_t> tsrc(toff[n]);
     std::vector<double> tw(toff[n]);
-    std::vector<std::vector<uint64_t>> pos(n);
     std::vector<uint64_t> cur(toff.begin(), toff.end() - 1);
     const std::vector<double> rinv = row_inverse(g);
-    for (uint32_t u = 0; u < n; ++u) {
-        pos[u].resize(g->adj[u].size());
+    auto raw = [&](uint32_t u, size_t i) { return g->weighted ? (double)g->w[u][i] : 1.0; };
+    for (uint32_t u = 0; u < n; ++u)
         for (size_t i = 0; i < g->adj[u].size(); ++i) {
             const uint64_t p = cur[g->adj[u][i]]++;
             tsrc[p] = u;
-            tw[p] = (g->weighted ? (double)g->w[u][i] : 1.0) * rinv[u];
-            pos[u][i] = p;
+            tw[p] = raw(u, i) * rinv[u];
         }
-    }
+    // base solve x0 = (1-a)/n + a T x0
     const double base = (1.0 - alpha) / n;
-    auto solve = [&](std::vector<double> &x) {
-        std::vector<double> xn(n);
-        int sweeps = 0;
-        for (int it = 0; it < max_iter; ++it) {
-            double diff = 0.0;
+    std::vector<double> x0(n, 1.0 / n), xn(n);
+    int sweeps = 0;
+    for (int it = 0; it < max_iter; ++it) {
+        double diff = 0.0;
 #pragma omp parallel for schedule(dynamic, 1024) reduction(+ : diff)
-            for (long v = 0; v < (long)n; ++v) {
-                double acc = 0.0;
-                for (uint64_t i = toff[v]; i < toff[v + 1]; ++i) acc += tw[i] * x[tsrc[i]];
-                xn[v] = base + alpha * acc;
-                diff += std::fabs(xn[v] - x[v]);
-            }
-            x.swap(xn);
-            ++sweeps;
-            if (diff < tol) break;
+        for (long v = 0; v < (long)n; ++v) {
+            double acc = 0.0;
+            for (uint64_t i = toff[v]; i < toff[v + 1]; ++i) acc += tw[i] * x0[tsrc[i]];
+            xn[v] = base + alpha * acc;
+            diff += std::fabs(xn[v] - x0[v]);
         }
-        return sweeps;
-    };
-    auto objective = [&](const std::vector<double> &x) {
-        double j = 0.0;
-        for (uint32_t i = 0; i < n; ++i) j += c[i] * x[i];
-        return j;
-    };
-    std::vector<double> x0(n, 1.0 / n);
-    const int sweeps = solve(x0);
+        x0.swap(xn);
+        ++sweeps;
+        if (diff < tol) break;
+    }
+    // forcing a q_e, sparse over the out-entries of u_e
+    std::vector<double> s_of(k);
+    std::vector<std::vector<std::pair<uint32_t, double>>> force(n);
     for (uint32_t e = 0; e < k; ++e) {
         const uint32_t u = eu[e];
-        double jj[2] = {0.0, 0.0};
-        for (int side = 0; side < 2; ++side) {
-            const double delta = side == 0 ? h : -h;
-            double sum = 0.0;
-            for (size_t i = 0; i < g->adj[u].size(); ++i)
-                sum += (g->weighted ? (double)g->w[u][i] : 1.0) + (g->adj[u][i] == ev[e] ? delta : 0.0);
-            for (size_t i = 0; i < g->adj[u].size(); ++i)
-                tw[pos[u][i]] = ((g->weighted ? (double)g->w[u][i] : 1.0) + (g->adj[u][i] == ev[e] ? delta : 0.0)) / sum;
-            std::vector<double> x = x0;
-            solve(x);
-            jj[side] = objective(x);
+        double s = 0.0;
+        for (size_t i = 0; i < g->adj[u].size(); ++i) s += raw(u, i);
+        s_of[e] = s;
+        for (size_t i = 0; i < g->adj[u].size(); ++i) {
+            const double q = ((g->adj[u][i] == ev[e] ? s : 0.0) - raw(u, i)) / s;
+            force[g->adj[u][i]].push_back({e, alpha * q});
         }
-        for (size_t i = 0; i < g->adj[u].size(); ++i)
-            tw[pos[u][i]] = (g->weighted ? (double)g->w[u][i] : 1.0) * rinv[u];
-        fd[e] = (jj[0] - jj[1]) / (2.0 * h);
+    }
+    const double rel_tol = 1e-11;
+    std::vector<double> Y((size_t)n * k, 0.0), Yn((size_t)n * k);
+    for (uint32_t v = 0; v < n; ++v)
+        for (auto &f : force[v]) Y[(size_t)v * k + f.first] = f.second;
+    std::vector<double> step(k), norm(k);
+    for (int it = 0; it < 4 * max_iter; ++it) {
+        std::fill(step.begin(), step.end(), 0.0);
+        std::fill(norm.begin(), norm.end(), 0.0);
+#pragma omp parallel
+        {
+            std::vector<double> acc(k), lstep(k, 0.0), lnorm(k, 0.0);
+#pragma omp for schedule(dynamic, 512) nowait
+            for (long v = 0; v < (long)n; ++v) {
+                std::fill(acc.begin(), acc.end(), 0.0);
+                for (uint64_t i = toff[v]; i < toff[v + 1]; ++i) {
+                    const double t = alpha * tw[i];
+                    const double *row = &Y[(size_t)tsrc[i] * k];
+                    for (uint32_t j = 0; j < k; ++j) acc[j] += t * row[j];
+                }
+                for (auto &f : force[v]) acc[f.first] += f.second;
+                double *out = &Yn[(size_t)v * k];
+                const double *old = &Y[(size_t)v * k];
+                for (uint32_t j = 0; j < k; ++j) {
+                    lstep[j] += std::fabs(acc[j] - old[j]);
+                    lnorm[j] += std::fabs(acc[j]);
+                    out[j] = acc[j];
+                }
+            }
+#pragma omp critical
+            for (uint32_t j = 0; j < k; ++j) {
+                step[j] += lstep[j];
+                norm[j] += lnorm[j];
+            }
+        }
+        Y.swap(Yn);
+        bool done = true;
+        for (uint32_t j = 0; j < k; ++j)
+            if (step[j] > rel_tol * norm[j]) done = false;
+        if (done) break;
+    }
+    std::vector<double> cy(k, 0.0);
+    for (uint32_t v = 0; v < n; ++v)
+        for (uint32_t j = 0; j < k; ++j) cy[j] += c[v] * Y[(size_t)v * k + j];
+    for (uint32_t e = 0; e < k; ++e) {
+        const uint32_t u = eu[e];
+        const double yu = Y[(size_t)u * k + e];
+        double dj[2];
+        for (int side = 0; side < 2; ++side) {
+            const double d = side == 0 ? h : -h;
+            const double r = d / (s_of[e] + d);
+            dj[side] = r * x0[u] * cy[e] / (1.0 - r * yu);
+        }
+        fd[e] = (dj[0] - dj[1]) / (2.0 * h);
     }
     return sweeps;
 }

@@ -75,10 +75,11 @@ double or_wpr_objective(const or_graph *g, double alpha, double tol, int max_ite
 
 /* Central finite differences (J(w + h) - J(w - h)) / 2h of J = sum c_i x_i
  * with respect to the raw weights of the k entries (eu[i], ev[i]), in fp64.
- * The transposed, normalised matrix is built once and only row eu[i] is
- * re-weighted per evaluation; each perturbed solve starts from the converged
- * unperturbed x and runs until the L1 step is below tol.  Returns the
- * unperturbed sweeps. */
+ * Each perturbed objective is evaluated exactly through the rank-one form of
+ * the perturbed fixed point (one forward-direction solve per entry, shared
+ * by +h and -h, all k solves sharing each sweep), so no perturbed solve is
+ * cut short and no two nearly equal objectives are subtracted.  tol bounds
+ * the unperturbed solve's L1 step.  Returns the unperturbed sweeps. */
 int or_wpr_fd(const or_graph *g, double alpha, double tol, int max_iter, const double *c, const uint32_t *eu,
               const uint32_t *ev, uint32_t k, double h, double *fd);
 

@@ -270,6 +270,41 @@ def test_wpr_forward_and_gradient():
         assert err < 1e-4
 
 
+def test_wpr_gradient_matches_dense_fp64_gradient_scale12():
+    """The differentiation workload's dense check: directed weighted R-MAT
+    scale 12 (weights U(0.1, 1], normalised per row), the GPU's gradient of
+    sum c_i x_i with respect to every raw weight against the gradient from
+    dense fp64 solves of the forward and transposed systems (numpy)."""
+    scale = 12
+    n = 1 << scale
+    rng = np.random.default_rng(1212)
+    s, d = rmat_graph(scale, 16, seed=1212)
+    w = (1.0 - 0.9 * rng.random(len(s))).astype(np.float32)
+    g = make_graph(n, directed=True, weighted=True)
+    g.batch_insert(s, d, w)
+    g.synchronize()
+    off, dst, wt = g.export_csr(with_weights=True)
+    src = np.repeat(np.arange(n), np.diff(off).astype(np.int64))
+    W = np.zeros((n, n))
+    W[src, dst] = wt.astype(np.float64)
+    rs = W.sum(1)
+    P = np.divide(W, rs[:, None], out=np.zeros_like(W), where=rs[:, None] > 0)
+    a = 0.85
+    x = np.linalg.solve(np.eye(n) - a * P.T, np.full(n, (1 - a) / n))
+    c = rng.standard_normal(n)
+    lam = np.linalg.solve(np.eye(n) - a * P, c)
+    # d J / d raw w_uv = a x_u (lam_v - (P lam)_u) / s_u
+    Plam = P @ lam
+    want = a * x[src] * (lam[dst] - Plam[src]) / rs[src]
+    xg, _ = g.wpr_forward(a, 1e-9, 300)
+    assert np.abs(xg.astype(np.float64) - x).sum() < PR_L1
+    grad, _, _ = g.wpr_backward(xg, c.astype(np.float32), a, 1e-9, 300, mode=0)
+    err = np.abs(grad.astype(np.float64) - want).max() / np.abs(want).max()
+    print(f"scale 12: {len(dst)} entries, max |grad - dense fp64| / max |grad| = {err:.3e}")
+    assert err < 1e-4
+    g.close()
+
+
 @pytest.mark.parametrize("mode", ["local", "global", ""])
 def test_triangle_subset_paths_agree(mode, monkeypatch):
     """Both subset paths (neighbour hash sets, whole-graph oriented count) are
