@@ -13,19 +13,9 @@ __global__ void k_rmat(uint32_t scale, uint64_t first, uint64_t count, uint64_t 
         gv_rmat_pair(seed, first + i, scale, &src[i], &dst[i]);
 }
 
-__host__ __device__ inline void uniform_pair(uint32_t n, uint64_t seed, uint64_t i, uint32_t *s, uint32_t *d) {
-    const uint64_t h1 = gv_mix64(seed * 0x9E3779B97F4A7C15ull + 2 * i);
-    const uint64_t h2 = gv_mix64(seed * 0x9E3779B97F4A7C15ull + 2 * i + 1);
-    const uint32_t u = gv_uniform_u32(h1, n);
-    uint32_t v = gv_uniform_u32(h2, n - 1);  // v in [0, n-1) then skip u
-    if (v >= u) ++v;
-    *s = u;
-    *d = v;
-}
-
 __global__ void k_uniform(uint32_t n, uint64_t count, uint64_t seed, uint32_t *src, uint32_t *dst) {
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (uint64_t)gridDim.x * blockDim.x)
-        uniform_pair(n, seed, i, &src[i], &dst[i]);
+        gv_uniform_pair(n, seed, i, &src[i], &dst[i]);
 }
 
 }  // namespace
@@ -54,7 +44,7 @@ gv_status gv_gen_uniform(uint32_t n, uint64_t count, uint64_t seed, uint32_t *sr
         return cuda_status(cudaGetLastError(), "gen uniform");
     }
 #pragma omp parallel for schedule(static)
-    for (long long i = 0; i < (long long)count; ++i) uniform_pair(n, seed, (uint64_t)i, &src[i], &dst[i]);
+    for (long long i = 0; i < (long long)count; ++i) gv_uniform_pair(n, seed, (uint64_t)i, &src[i], &dst[i]);
     return GV_OK;
 }
 

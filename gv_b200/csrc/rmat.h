@@ -47,3 +47,15 @@ GV_HD void gv_rmat_pair(uint64_t seed, uint64_t i, uint32_t scale, uint32_t *src
 GV_HD uint32_t gv_uniform_u32(uint64_t h, uint32_t range) {
     return (uint32_t)(((h >> 32) * (uint64_t)range) >> 32);
 }
+
+// Uniform pair u != v over [0, n): u uniform, v uniform over the other n-1
+// vertices; pair i depends only on (n, seed, i).
+GV_HD void gv_uniform_pair(uint32_t n, uint64_t seed, uint64_t i, uint32_t *s, uint32_t *d) {
+    const uint64_t h1 = gv_mix64(seed * 0x9E3779B97F4A7C15ull + 2 * i);
+    const uint64_t h2 = gv_mix64(seed * 0x9E3779B97F4A7C15ull + 2 * i + 1);
+    const uint32_t u = gv_uniform_u32(h1, n);
+    uint32_t v = gv_uniform_u32(h2, n - 1);  // v in [0, n-1) then skip u
+    if (v >= u) ++v;
+    *s = u;
+    *d = v;
+}

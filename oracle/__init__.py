@@ -37,6 +37,7 @@ _SIG = {
     "or_wpr_objective": (C.c_double, [_P, C.c_double, C.c_double, C.c_int, _P, C.c_uint32, C.c_uint32, C.c_double]),
     "or_wpr_fd": (C.c_int, [_P, C.c_double, C.c_double, C.c_int, _P, _P, _P, C.c_uint32, C.c_double, _P]),
     "or_rmat_pairs": (None, [C.c_uint32, C.c_uint64, C.c_uint64, _P, _P]),
+    "or_uniform_pairs": (None, [C.c_uint32, C.c_uint64, C.c_uint64, _P, _P]),
 }
 _lib = None
 
@@ -67,6 +68,14 @@ def rmat_pairs(scale: int, num_pairs: int, seed: int):
     s = np.empty(num_pairs, np.uint32)
     d = np.empty(num_pairs, np.uint32)
     lib().or_rmat_pairs(scale, num_pairs, seed, s.ctypes.data, d.ctypes.data)
+    return s, d
+
+
+def uniform_pairs(n: int, num_pairs: int, seed: int):
+    """Seeded uniform pairs u != v (the generator libgv's gen_uniform uses)."""
+    s = np.empty(num_pairs, np.uint32)
+    d = np.empty(num_pairs, np.uint32)
+    lib().or_uniform_pairs(n, num_pairs, seed, s.ctypes.data, d.ctypes.data)
     return s, d
 
 
@@ -115,9 +124,10 @@ class OracleGraph:
         sw = lib().or_ppr(self._h, source, alpha, epsilon, max_iter, fixed_sweeps, x.ctypes.data)
         return x, sw
 
-    def tc(self):
-        pv = np.empty(self.n, np.uint64)
-        tot = lib().or_tc(self._h, pv.ctypes.data)
+    def tc(self, per_vertex: bool = True):
+        """(per-vertex counts or None, total); per_vertex=False counts the total only."""
+        pv = np.empty(self.n, np.uint64) if per_vertex else None
+        tot = lib().or_tc(self._h, pv.ctypes.data if per_vertex else None)
         return pv, int(tot)
 
     def tc_incident(self, subset):

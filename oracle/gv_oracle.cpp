@@ -314,8 +314,9 @@ static uint64_t tc_symmetric(const or_graph *g, uint64_t *per_vertex) {
     for (long u = 0; u < n; ++u)
         for (uint32_t v : g->adj[u])
             if (less((uint32_t)u, v)) out[u].push_back(v);  // adj is sorted, so out[u] is sorted
-    std::vector<std::atomic<uint64_t>> cnt(n);
-    for (long u = 0; u < n; ++u) cnt[u].store(0, std::memory_order_relaxed);
+    // per-vertex credits only when asked for (the atomics cost more than the merges)
+    std::vector<std::atomic<uint64_t>> cnt(per_vertex ? n : 0);
+    for (long u = 0; u < (long)cnt.size(); ++u) cnt[u].store(0, std::memory_order_relaxed);
     uint64_t total = 0;
 #pragma omp parallel for schedule(dynamic, 64) reduction(+ : total)
     for (long u = 0; u < n; ++u) {
@@ -328,8 +329,10 @@ static uint64_t tc_symmetric(const or_graph *g, uint64_t *per_vertex) {
                 if (*a < *b) ++a;
                 else if (*b < *a) ++b;
                 else {
-                    const uint32_t o = std::min<uint32_t>(std::min<uint32_t>((uint32_t)u, v), *a);
-                    cnt[o].fetch_add(1, std::memory_order_relaxed);
+                    if (per_vertex) {
+                        const uint32_t o = std::min<uint32_t>(std::min<uint32_t>((uint32_t)u, v), *a);
+                        cnt[o].fetch_add(1, std::memory_order_relaxed);
+                    }
                     ++total;
                     ++a;
                     ++b;
@@ -674,6 +677,11 @@ int or_wpr_fd(const or_graph *g, double alpha, double tol, int max_iter, const d
         fd[e] = (dj[0] - dj[1]) / (2.0 * h);
     }
     return sweeps;
+}
+
+void or_uniform_pairs(uint32_t n, uint64_t num_pairs, uint64_t seed, uint32_t *src, uint32_t *dst) {
+#pragma omp parallel for schedule(static)
+    for (long long i = 0; i < (long long)num_pairs; ++i) gv_uniform_pair(n, seed, (uint64_t)i, &src[i], &dst[i]);
 }
 
 void or_rmat_pairs(uint32_t scale, uint64_t num_pairs, uint64_t seed, uint32_t *src, uint32_t *dst) {

@@ -85,6 +85,9 @@ int or_wpr_fd(const or_graph *g, double alpha, double tol, int max_iter, const d
 
 /* Seeded R-MAT pairs, the same generator libgv uses (gv_b200/csrc/rmat.h). */
 void or_rmat_pairs(uint32_t scale, uint64_t num_pairs, uint64_t seed, uint32_t *src, uint32_t *dst);
+/* Seeded uniform pairs u != v over [0, n), the same generator libgv uses
+ * (gv_uniform_pair in gv_b200/csrc/rmat.h). */
+void or_uniform_pairs(uint32_t n, uint64_t num_pairs, uint64_t seed, uint32_t *src, uint32_t *dst);
 
 #ifdef __cplusplus
 }

@@ -249,5 +249,10 @@ def test_generator_is_shared_with_libgv():
     s1, d1 = oracle.rmat_pairs(12, 5000, 77)
     s2, d2 = gv_b200.gen_rmat(12, 5000, 77)
     assert np.array_equal(s1, s2) and np.array_equal(d1, d2)
+    for n, seed in ((1 << 12, 3), (1000, 2026005), (2, 9)):
+        u1, v1 = oracle.uniform_pairs(n, 4000, seed)
+        u2, v2 = gv_b200.gen_uniform(n, 4000, seed=seed)
+        assert np.array_equal(u1, u2) and np.array_equal(v1, v2)
+        assert np.all(u1 != v1) and u1.max() < n and v1.max() < n
     # R-MAT skew: vertex 0 is the densest quadrant corner
     assert np.bincount(s1, minlength=1 << 12)[0] > 20

@@ -104,6 +104,64 @@ def test_hub_paths_and_block_multiples():
     assert_sound(g)
 
 
+def test_hubs_beyond_one_block_table_window():
+    """Hubs of more than 1024 blocks of 32 entries (the CTA-per-vertex
+    membership and compaction paths walk their blocks in windows of 1024
+    table entries) and of more than 2048 blocks (the BC kernels' table
+    windows): insert, BC and PageRank across windows, deletes spread over
+    every window, compaction that moves tail entries into earlier windows,
+    then inserts into the compacted hub, each step against the oracle."""
+    scale = 17
+    n = 1 << scale
+    B = 32
+    rng = np.random.default_rng(17)
+    bs, bd = rmat_graph(scale, 4, seed=17)
+    others = np.setdiff1d(np.arange(n, dtype=np.uint32), [5, 9])
+    h5 = rng.permutation(others)[:80_000]           # 2500 blocks
+    h9 = rng.permutation(others)[:40_000]           # 1250 blocks
+    s = np.concatenate([bs, np.full(len(h5), 5, np.uint32), np.full(len(h9), 9, np.uint32)])
+    d = np.concatenate([bd, h5, h9])
+    g, o = build_pair(n, s, d, block_size=B, threads_per_vertex=8)
+    assert_same_adjacency(g, o)
+    assert_sound(g)
+    assert g.degrees()[5] > 2048 * B
+    src = np.array([5, 9, 77, 1234], np.uint32)
+    b = g.bc(src)
+    ob = o.bc(src)
+    nz = ob != 0
+    assert np.max(np.abs(b[nz] - ob[nz]) / np.abs(ob[nz])) < 1e-5
+    assert np.all(b[~nz] == 0)
+    x, sweeps = g.static_pagerank(0.85, 1e-6, 100)
+    xo, _ = o.pagerank(0.85, 1e-6, 100, fixed_sweeps=sweeps)
+    assert np.abs(x - xo).sum() < 1e-6
+    # delete 60% of each hub's entries (spread over every window) plus some background
+    d5 = h5[rng.random(len(h5)) < 0.6]
+    d9 = h9[rng.random(len(h9)) < 0.6]
+    ooff, odst, _ = o.export()
+    es, ed = sample_existing(ooff, odst, 20_000, rng)
+    ds = np.concatenate([np.full(len(d5), 5, np.uint32), d9, es])
+    dd = np.concatenate([d5, np.full(len(d9), 9, np.uint32), ed])  # hub 9 deleted from the other side
+    g.batch_delete(ds, dd)
+    o.delete(ds, dd)
+    g.compaction()
+    g.synchronize()
+    assert_same_adjacency(g, o)
+    assert_sound(g)
+    # re-insert part of what was deleted plus new neighbours into the compacted hubs
+    add = np.concatenate([d5[:15_000], rng.permutation(others)[:30_000]])
+    g.batch_insert(np.full(len(add), 5, np.uint32), add)
+    o.insert(np.full(len(add), 5, np.uint32), add)
+    g.batch_insert(d9[:10_000], np.full(10_000, 9, np.uint32))
+    o.insert(d9[:10_000], np.full(10_000, 9, np.uint32))
+    g.synchronize()
+    assert_same_adjacency(g, o)
+    assert_sound(g)
+    pv, tot = g.static_tc()
+    opv, otot = o.tc()
+    assert tot == otot and np.array_equal(pv, opv)
+    g.close()
+
+
 def test_directed_store():
     n = 1 << 10
     s, d = rmat_graph(10, 8, seed=4)
