@@ -90,6 +90,7 @@ SIGNATURES = {
     "gv_pool_stats": (C.c_int, [P, pu64, pu64]),
     "gv_get_config": (C.c_int, [P, C.POINTER(gv_config)]),
     "gv_degrees": (C.c_int, [P, P, C.c_int, P]),
+    "gv_vertex_records": (C.c_int, [P, P]),
     "gv_export_csr": (C.c_int, [P, P, P, P, u64, C.c_int, P]),
     "gv_affected": (C.c_int, [P, P, C.c_int, P]),
     "gv_clear_affected": (C.c_int, [P, P]),

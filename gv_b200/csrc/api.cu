@@ -674,6 +674,12 @@ gv_status gv_pool_stats(gv_graph *g, uint64_t *capacity, uint64_t *free_blocks) 
     return GV_OK;
 }
 
+gv_status gv_vertex_records(gv_graph *g, const void **records) {
+    if (!g || !records) return GV_ERR_INVALID;
+    *records = g->d.vtx;
+    return GV_OK;
+}
+
 gv_status gv_degrees(gv_graph *g, uint32_t *deg, int mem, void *stream) {
     if (!g || !deg) return GV_ERR_INVALID;
     DeviceGuard dg(g->cfg.device);

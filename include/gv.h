@@ -138,6 +138,14 @@ gv_status gv_get_config(const gv_graph *g, gv_config *cfg);
 /* Per-vertex degree (live entries) into deg[n] (uint32). */
 gv_status gv_degrees(gv_graph *g, uint32_t *deg, int mem, void *stream);
 
+/* Device address of the vertex records: n records of four uint32 each,
+ * {first block (pool index, 0xFFFFFFFF if none), filled slots, live
+ * entries, last block}.  Read-only for the caller; valid until the next
+ * call that adds vertices or destroys the graph.  Replaces
+ * GraphVine::getVertexDictionary (graphvine.cu:493-495), whose
+ * VertexDictionary the reference's algorithm kernels walk. */
+gv_status gv_vertex_records(gv_graph *g, const void **records);
+
 /* Snapshot of the live adjacency as CSR, each vertex's entries in storage
  * order.  offsets[n+1] (uint64), dst[cap], weights[cap] (nullable).
  * Synchronous; returns GV_ERR_CAPACITY if cap < live entries. */

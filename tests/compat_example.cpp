@@ -1,11 +1,14 @@
-// Reference-style driver written against include/graphvine.hpp: the same
-// calls src/main.cu:46-119 makes (readGraph, GraphVine(CSR*), batchInsert,
-// batchDelete, compaction, static_pagerank, static_tc, bc), on libgv.
+// Reference-style driver written against include/graphvine.hpp with host
+// containers: the same calls src/main.cu:46-119 makes (readGraph,
+// GraphVine(CSR*), batchInsert, batchDelete, compaction, static_pagerank,
+// static_tc, bc), on libgv, built by a plain C++ compiler.
 // Usage: compat_example <graph.mtx> <insert.mtx> <delete.mtx> <out_prefix>
 #include <cstdio>
 #include <vector>
 
 #include "graphvine.hpp"
+
+size_t BATCH_SIZE = 1000;  // the application defines it, as src/main.cu:18 does
 
 int main(int argc, char **argv) {
     if (argc != 5) {
@@ -26,7 +29,7 @@ int main(int argc, char **argv) {
         std::vector<float> pr1, pr2, tc;
         static_pagerank(&g, 0.85f, 1e-6f, 100, pr1, pr2);
         static_tc(&g, tc);
-        std::vector<float> b = bc(&g, 0);
+        std::vector<float> b = bc_scores(&g);
         const std::string pre = argv[4];
         auto dump = [&](const char *name, const std::vector<float> &v) {
             FILE *f = std::fopen((pre + name).c_str(), "wb");
@@ -37,8 +40,8 @@ int main(int argc, char **argv) {
         dump(".tc", tc);
         dump(".bc", b);
         std::printf("ok n=%lu\n", g.getVertexSize());
-    } catch (const gv::Error &e) {
-        std::fprintf(stderr, "gv error: %s\n", e.what());
+    } catch (const std::exception &e) {
+        std::fprintf(stderr, "error: %s\n", e.what());
         return 1;
     }
     return 0;
