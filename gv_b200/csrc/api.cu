@@ -785,6 +785,7 @@ gv_status gv_last_stat(gv_graph *g, const char *key, double *value) {
         *value = (double)g->last_sweeps;
         return GV_OK;
     }
+    if (window_stat(g, key, value)) return GV_OK;
     set_error(std::string("unknown stat ") + key);
     return GV_ERR_INVALID;
 }

@@ -10,8 +10,12 @@
 // per operation type, and compaction runs once at the end.  The final graph
 // equals applying the batches one by one; tests/test_batch_gpu.py checks it.
 //
-// With GV_BATCH_GRAPH the window's device work is captured into a CUDA graph
-// and launched as one graph.
+// The window is applied by one persistent launch (launch_window_apply in
+// update.cu) when the free stack holds the window's worst case, else by the
+// two-stage exact path (one insert and one delete pass).  With
+// GV_BATCH_GRAPH the persistent path's device work is captured once per
+// capacity (window entries rounded up to a power of two) and the captured
+// graph is replayed for later windows: its sizes are read on the device.
 //
 // The reference applies one batch per host call with several host round
 // trips each (src/dynamicStructure/graphvine.cu:222-451).
@@ -25,6 +29,7 @@
 #include "group.cuh"
 #include "prims.cuh"
 #include "launch.hpp"
+#include "prof.hpp"
 
 namespace gv {
 namespace {
@@ -123,6 +128,185 @@ __global__ void k_fill_sent(unsigned long long *__restrict__ out, const uint32_t
         out[i] = sent;
 }
 
+// Net effect over both operations: keep = last of its run of equal keys and
+// not the sentinel; the kept keys (sorted, unique) and their operation go to
+// out/otype.
+__device__ __forceinline__ bool net_last(const unsigned long long *K, uint64_t i, uint64_t N, unsigned long long sent) {
+    if (i >= N) return false;
+    const unsigned long long k = K[i];
+    if (k == sent) return false;
+    return !(i + 1 < N && K[i + 1] == k);
+}
+
+__global__ void __launch_bounds__(NET_THREADS) k_net_all_count(const unsigned long long *__restrict__ K, uint64_t N,
+                                                               unsigned long long sent,
+                                                               uint32_t *__restrict__ tile_cnt) {
+    __shared__ uint32_t wt[33];
+    const uint64_t base = (uint64_t)blockIdx.x * NET_TILE + (uint64_t)threadIdx.x * NET_ITEMS;
+    uint32_t c = 0;
+#pragma unroll
+    for (int j = 0; j < NET_ITEMS; ++j) c += net_last(K, base + j, N, sent) ? 1u : 0u;
+    const uint32_t tot = cta_sum<uint32_t, NET_THREADS>(c, wt);
+    if (threadIdx.x == 0) tile_cnt[blockIdx.x] = tot;
+}
+
+__global__ void __launch_bounds__(NET_THREADS) k_net_all_write(const unsigned long long *__restrict__ K,
+                                                               const uint32_t *__restrict__ V, uint64_t N,
+                                                               unsigned long long sent,
+                                                               const uint32_t *__restrict__ tile_off,
+                                                               unsigned long long *__restrict__ out,
+                                                               uint32_t *__restrict__ otype) {
+    __shared__ uint32_t wt[33];
+    const uint64_t base = (uint64_t)blockIdx.x * NET_TILE + (uint64_t)threadIdx.x * NET_ITEMS;
+    bool keep[NET_ITEMS];
+    uint32_t c = 0;
+#pragma unroll
+    for (int j = 0; j < NET_ITEMS; ++j) {
+        keep[j] = net_last(K, base + j, N, sent);
+        c += keep[j] ? 1u : 0u;
+    }
+    uint32_t tot;
+    uint32_t p = cta_excl_scan<uint32_t, NET_THREADS>(c, wt, tot) + tile_off[blockIdx.x];
+#pragma unroll
+    for (int j = 0; j < NET_ITEMS; ++j)
+        if (keep[j]) {
+            out[p] = K[base + j];
+            otype[p] = V[base + j];
+            ++p;
+        }
+}
+
+// Segments of the net keys (one per source vertex): heads counted per tile,
+// then seg_vertex/seg_start, the destinations (bdst) and cleared found flags
+// written; ctl->nseg and seg_start[nseg] set by the first thread.
+__device__ __forceinline__ bool wseg_head(const unsigned long long *K, uint64_t i, uint32_t cnt, uint32_t bitsn) {
+    if (i >= cnt) return false;
+    return i == 0 || (K[i] >> bitsn) != (K[i - 1] >> bitsn);
+}
+
+__global__ void __launch_bounds__(NET_THREADS) k_wseg_count(const unsigned long long *__restrict__ K,
+                                                            const uint32_t *__restrict__ count, uint32_t bitsn,
+                                                            uint32_t *__restrict__ tile_cnt) {
+    __shared__ uint32_t wt[33];
+    const uint32_t cnt = *count;
+    const uint64_t base = (uint64_t)blockIdx.x * NET_TILE + (uint64_t)threadIdx.x * NET_ITEMS;
+    uint32_t c = 0;
+#pragma unroll
+    for (int j = 0; j < NET_ITEMS; ++j) c += wseg_head(K, base + j, cnt, bitsn) ? 1u : 0u;
+    const uint32_t tot = cta_sum<uint32_t, NET_THREADS>(c, wt);
+    if (threadIdx.x == 0) tile_cnt[blockIdx.x] = tot;
+}
+
+__global__ void __launch_bounds__(NET_THREADS) k_wseg_write(const unsigned long long *__restrict__ K,
+                                                            const uint32_t *__restrict__ count, uint32_t bitsn,
+                                                            const uint32_t *__restrict__ tile_off,
+                                                            const uint32_t *__restrict__ nseg_total,
+                                                            uint32_t *__restrict__ bdst, uint8_t *__restrict__ found,
+                                                            uint32_t *__restrict__ seg_vertex,
+                                                            uint32_t *__restrict__ seg_start, Ctl *ctl) {
+    __shared__ uint32_t wt[33];
+    const uint32_t cnt = *count;
+    const uint64_t base = (uint64_t)blockIdx.x * NET_TILE + (uint64_t)threadIdx.x * NET_ITEMS;
+    const unsigned long long dmask = (1ull << bitsn) - 1ull;
+    bool h[NET_ITEMS];
+    uint32_t c = 0;
+#pragma unroll
+    for (int j = 0; j < NET_ITEMS; ++j) {
+        h[j] = wseg_head(K, base + j, cnt, bitsn);
+        c += h[j] ? 1u : 0u;
+    }
+    uint32_t tot;
+    uint32_t p = cta_excl_scan<uint32_t, NET_THREADS>(c, wt, tot) + tile_off[blockIdx.x];
+#pragma unroll
+    for (int j = 0; j < NET_ITEMS; ++j) {
+        const uint64_t i = base + j;
+        if (i < cnt) {
+            bdst[i] = (uint32_t)(K[i] & dmask);
+            found[i] = 0;
+        }
+        if (h[j]) {
+            seg_vertex[p] = (uint32_t)(K[i] >> bitsn);
+            seg_start[p] = (uint32_t)i;
+            ++p;
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        const uint32_t ns = *nseg_total;
+        ctl->nseg = ns;
+        seg_start[ns] = cnt;
+    }
+}
+
+// Window header on the device: the graph of a window reads its sizes here,
+// so one captured graph serves every window that fits its capacity.
+struct WinHeader {
+    unsigned long long total;  // pairs in the window
+    unsigned int nb;           // batches
+    unsigned int pad;
+};
+
+// Window expansion with sizes from the header; keys past the window's
+// entries (up to the capacity E) become the sentinel.
+__global__ void k_window_expand_dev(const uint32_t *__restrict__ src, const uint32_t *__restrict__ dst,
+                                    const WinHeader *__restrict__ hdr, uint64_t E,
+                                    const unsigned long long *__restrict__ bstart,
+                                    const unsigned long long *__restrict__ bsplit, int sym, uint32_t n, uint32_t bitsn,
+                                    unsigned long long *__restrict__ keys, uint32_t *__restrict__ vals,
+                                    uint8_t *__restrict__ affected, Ctl *ctl) {
+    const unsigned long long sent = (bitsn >= 32) ? ~0ull : ((1ull << (2 * bitsn)) - 1ull);
+    const uint64_t total = hdr->total;
+    const uint32_t nb = hdr->nb;
+    const uint64_t per = sym ? 2 : 1;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i * per < E; i += (uint64_t)gridDim.x * blockDim.x) {
+        if (i >= total) {
+            keys[per * i] = sent;
+            vals[per * i] = 0;
+            if (sym) {
+                keys[per * i + 1] = sent;
+                vals[per * i + 1] = 0;
+            }
+            continue;
+        }
+        uint32_t lo = 0, hi = nb;  // last batch with bstart <= i
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (bstart[mid] <= i) lo = mid; else hi = mid;
+        }
+        const uint32_t type = (i < bsplit[lo]) ? 1u : 0u;
+        const uint32_t s = src[i], d = dst[i];
+        const bool bad = (s >= n) || (d >= n);
+        if (bad) {
+            atomicOr(&ctl->status, GV_DEV_ERR_RANGE);
+            ctl->batch_abort = 1;
+        }
+        const bool drop = bad || (s == d);
+        if (!drop) {
+            affected[s] = 1;
+            affected[d] = 1;
+        }
+        if (sym) {
+            keys[2 * i] = drop ? sent : (((unsigned long long)s << bitsn) | d);
+            keys[2 * i + 1] = drop ? sent : (((unsigned long long)d << bitsn) | s);
+            vals[2 * i] = type;
+            vals[2 * i + 1] = type;
+        } else {
+            keys[i] = drop ? sent : (((unsigned long long)s << bitsn) | d);
+            vals[i] = type;
+        }
+    }
+}
+
+// A captured window graph and what it was captured against: it is replayed
+// while the buffers, the store arrays and the capacity are unchanged.
+struct WinGraph {
+    uint64_t E = 0, nb_cap = 0;
+    uint32_t flags = 0;
+    std::vector<const void *> ptrs;
+    DevGraph d{};
+    cudaGraphExec_t exec = nullptr;
+    unsigned long long launches = 0;  // kernels per replay
+};
+
 struct WindowBufs {
     uint64_t cap_src = 0, cap_dst = 0, cap_vals = 0, cap_vals_alt = 0, cap_bstart = 0, cap_bsplit = 0, cap_tiles = 0;
     uint32_t *src = nullptr, *dst = nullptr;  // device copies of host windows
@@ -130,6 +314,14 @@ struct WindowBufs {
     unsigned long long *bstart = nullptr, *bsplit = nullptr;
     uint32_t *tile_cnt = nullptr;  // tiles + 1 (the last slot holds the count)
     cudaStream_t cap_stream = nullptr;
+    // persistent path: header, work queue and counts on the device
+    void *wctl = nullptr;
+    std::vector<WinGraph> graphs;
+    unsigned long long captures = 0, replays = 0, persistent = 0, exact = 0;  // window counts by path
+    WinHeader *hdr() const { return (WinHeader *)wctl; }
+    unsigned long long *queue() const { return (unsigned long long *)((char *)wctl + 16); }
+    uint32_t *net_count() const { return (uint32_t *)((char *)wctl + 48); }
+    uint32_t *nseg_total() const { return (uint32_t *)((char *)wctl + 52); }
 };
 
 std::mutex win_mu;
@@ -157,13 +349,32 @@ gv_status grow(T **p, uint64_t &cap, uint64_t want, size_t elem, const char *wha
 
 }  // namespace
 
+bool window_stat(gv_graph *g, const char *key, double *value) {
+    const char *keys[4] = {"window_captures", "window_replays", "window_persistent", "window_exact"};
+    int which = -1;
+    for (int i = 0; i < 4; ++i)
+        if (!std::strcmp(key, keys[i])) which = i;
+    if (which < 0) return false;
+    std::lock_guard<std::mutex> lk(win_mu);
+    unsigned long long v = 0;
+    for (auto &w : g_windows)
+        if (w.first == g) {
+            const WindowBufs &b = *w.second;
+            v = which == 0 ? b.captures : which == 1 ? b.replays : which == 2 ? b.persistent : b.exact;
+        }
+    *value = (double)v;
+    return true;
+}
+
 void release_window(gv_graph *g) {
     std::lock_guard<std::mutex> lk(win_mu);
     for (size_t i = 0; i < g_windows.size(); ++i)
         if (g_windows[i].first == g) {
             WindowBufs &b = *g_windows[i].second;
+            for (WinGraph &wg : b.graphs)
+                if (wg.exec) cudaGraphExecDestroy(wg.exec);
             for (void *p : {(void *)b.src, (void *)b.dst, (void *)b.vals, (void *)b.vals_alt, (void *)b.bstart,
-                            (void *)b.bsplit, (void *)b.tile_cnt})
+                            (void *)b.bsplit, (void *)b.tile_cnt, b.wctl})
                 if (p) cudaFree(p);
             if (b.cap_stream) cudaStreamDestroy(b.cap_stream);
             g_windows.erase(g_windows.begin() + i);
@@ -199,6 +410,117 @@ static void enqueue_window(gv_graph *g, WindowBufs &wb, uint32_t nb, const uint3
     if (flags & GV_BATCH_COMPACT) run_compact(g, s);
 }
 
+// Enqueues the persistent-path window over capacity E (launch only, no
+// allocation, no host sync, sizes read from the header): expand, sort, net
+// effect over both operations, segments, then one persistent launch applies
+// every segment (launch_window_apply) and compaction follows.
+static void enqueue_window_persistent(gv_graph *g, WindowBufs &wb, uint64_t E, uint32_t flags, cudaStream_t s) {
+    const bool sym = !g->cfg.directed;
+    BatchScratch &bs = g->bs;
+    const unsigned long long sent = (g->bitsn >= 32) ? ~0ull : ((1ull << (2 * g->bitsn)) - 1ull);
+    cudaMemsetAsync(wb.queue(), 0, 24, s);
+    const uint64_t per = sym ? 2 : 1;
+    GV_LAUNCH(k_window_expand_dev, grid_for(E / per, 256, 148 * 16), 256, 0, s, (const uint32_t *)wb.src,
+              (const uint32_t *)wb.dst, (const WinHeader *)wb.hdr(), E, (const unsigned long long *)wb.bstart,
+              (const unsigned long long *)wb.bsplit, sym ? 1 : 0, g->d.n, g->bitsn, bs.keys, wb.vals, g->d.affected,
+              g->d.ctl);
+    int which;
+    {
+        ProfScope ps(PROF_RADIX, s);
+        which = radix_sort_u64(bs.keys, bs.keys_alt, wb.vals, wb.vals_alt, E, 2 * (int)g->bitsn, bs.rs_counts,
+                               bs.scan_tmp, s);
+    }
+    const unsigned long long *K = which ? bs.keys_alt : bs.keys;
+    const uint32_t *V = which ? wb.vals_alt : wb.vals;
+    unsigned long long *out = which ? bs.keys : bs.keys_alt;
+    uint32_t *otype = which ? wb.vals : wb.vals_alt;
+    const unsigned ntiles = (unsigned)((E + NET_TILE - 1) / NET_TILE);
+    {
+        ProfScope ps(PROF_SEGMENT, s);
+        GV_LAUNCH(k_net_all_count, ntiles, NET_THREADS, 0, s, K, E, sent, wb.tile_cnt);
+        scan_exclusive_u32(wb.tile_cnt, wb.tile_cnt, ntiles, wb.net_count(), bs.scan_tmp, s);
+        GV_LAUNCH(k_net_all_write, ntiles, NET_THREADS, 0, s, K, V, E, sent, (const uint32_t *)wb.tile_cnt, out, otype);
+        GV_LAUNCH(k_wseg_count, ntiles, NET_THREADS, 0, s, (const unsigned long long *)out,
+                  (const uint32_t *)wb.net_count(), g->bitsn, wb.tile_cnt);
+        scan_exclusive_u32(wb.tile_cnt, wb.tile_cnt, ntiles, wb.nseg_total(), bs.scan_tmp, s);
+        GV_LAUNCH(k_wseg_write, ntiles, NET_THREADS, 0, s, (const unsigned long long *)out,
+                  (const uint32_t *)wb.net_count(), g->bitsn, (const uint32_t *)wb.tile_cnt,
+                  (const uint32_t *)wb.nseg_total(), bs.bdst, bs.found, bs.seg_vertex, bs.seg_start, g->d.ctl);
+    }
+    launch_window_apply(g, bs.seg_vertex, bs.seg_start, bs.bdst, otype, bs.found, bs.big_list, wb.queue(), s);
+    if (flags & GV_BATCH_COMPACT) run_compact(g, s);
+}
+
+// The buffers a persistent-path graph captures.
+static std::vector<const void *> window_ptrs(gv_graph *g, WindowBufs &wb) {
+    const BatchScratch &bs = g->bs;
+    return {wb.src, wb.dst, wb.vals, wb.vals_alt, wb.bstart, wb.bsplit, wb.tile_cnt, wb.wctl, bs.keys, bs.keys_alt,
+            bs.rs_counts, bs.scan_tmp, bs.bdst, bs.found, bs.seg_vertex, bs.seg_start, bs.big_list};
+}
+
+// Runs the persistent-path window of capacity E on stream s: replays the
+// graph captured for (E, batch capacity, flags) when the buffers and the
+// store are those it was captured with, else captures it first.
+static gv_status run_window_graph(gv_graph *g, WindowBufs &wb, uint64_t E, uint64_t nb_cap, uint32_t flags,
+                                  cudaStream_t s) {
+    const std::vector<const void *> ptrs = window_ptrs(g, wb);
+    WinGraph *hit = nullptr;
+    for (WinGraph &wg : wb.graphs)
+        if (wg.E == E && wg.nb_cap == nb_cap && wg.flags == flags && wg.ptrs == ptrs &&
+            std::memcmp(&wg.d, &g->d, sizeof(DevGraph)) == 0)
+            hit = &wg;
+    if (!hit) {
+        // graphs captured against buffers that have since moved are useless
+        for (size_t i = 0; i < wb.graphs.size();) {
+            if (wb.graphs[i].ptrs != ptrs || std::memcmp(&wb.graphs[i].d, &g->d, sizeof(DevGraph)) != 0) {
+                if (wb.graphs[i].exec) cudaGraphExecDestroy(wb.graphs[i].exec);
+                wb.graphs.erase(wb.graphs.begin() + i);
+            } else {
+                ++i;
+            }
+        }
+        if (!wb.cap_stream) {
+            cudaError_t e = cudaStreamCreateWithFlags(&wb.cap_stream, cudaStreamNonBlocking);
+            if (e != cudaSuccess) return cuda_status(e, "capture stream");
+        }
+        const unsigned long long l0 = g_launches.load();
+        cudaGraph_t graph = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(wb.cap_stream, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            enqueue_window_persistent(g, wb, E, flags, wb.cap_stream);
+            e = cudaStreamEndCapture(wb.cap_stream, &graph);
+        }
+        WinGraph wg;
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&wg.exec, graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+        if (e != cudaSuccess) {
+            if (wg.exec) cudaGraphExecDestroy(wg.exec);
+            return cuda_status(e, "window graph capture");
+        }
+        wg.E = E;
+        wg.nb_cap = nb_cap;
+        wg.flags = flags;
+        wg.ptrs = ptrs;
+        wg.d = g->d;
+        wg.launches = g_launches.load() - l0;
+        g_launches.fetch_sub(wg.launches);  // counted when the graph runs
+        wb.graphs.push_back(wg);
+        hit = &wb.graphs.back();
+        ++wb.captures;
+    } else {
+        ++wb.replays;
+    }
+    cudaError_t e = cudaGraphLaunch(hit->exec, s);
+    if (e == cudaSuccess) g_launches.fetch_add(hit->launches);
+    return cuda_status(e, "window graph launch");
+}
+
+static uint64_t pow2_at_least(uint64_t x, uint64_t lo) {
+    uint64_t p = lo;
+    while (p < x) p <<= 1;
+    return p;
+}
+
 }  // namespace gv
 
 using namespace gv;
@@ -223,58 +545,66 @@ extern "C" gv_status gv_batch_run(gv_graph *g, const gv_batch_desc *descs, uint3
     cudaStream_t s = (cudaStream_t)stream;
     WindowBufs &wb = window_bufs(g);
     const bool sym = !g->cfg.directed;
-    const uint64_t E = sym ? 2 * total : total;
-    gv_status st = ensure_batch_scratch(g, E, 1);
-    const uint64_t ntiles = (E + NET_TILE - 1) / NET_TILE;
-    if (st == GV_OK) st = grow(&wb.vals, wb.cap_vals, E, 4, "window vals");
-    if (st == GV_OK) st = grow(&wb.vals_alt, wb.cap_vals_alt, E, 4, "window vals");
-    if (st == GV_OK) st = grow(&wb.bstart, wb.cap_bstart, nbatches, 8, "window starts");
-    if (st == GV_OK) st = grow(&wb.bsplit, wb.cap_bsplit, nbatches, 8, "window splits");
+    const uint64_t per = sym ? 2 : 1;
+    const uint64_t E = per * total;
+    // Persistent path: capacity rounded up to a power of two so that windows
+    // of similar size share one captured graph; its sizes live on the device.
+    const uint64_t Ecap = pow2_at_least(E, 1ull << 16);
+    const uint64_t nb_cap = pow2_at_least(nbatches, 64);
+    const uint64_t pcap = Ecap / per;
+    gv_status st = ensure_batch_scratch(g, Ecap, 1);
+    const uint64_t ntiles = (Ecap + NET_TILE - 1) / NET_TILE;
+    if (st == GV_OK) st = grow(&wb.vals, wb.cap_vals, Ecap, 4, "window vals");
+    if (st == GV_OK) st = grow(&wb.vals_alt, wb.cap_vals_alt, Ecap, 4, "window vals");
+    if (st == GV_OK) st = grow(&wb.bstart, wb.cap_bstart, nb_cap, 8, "window starts");
+    if (st == GV_OK) st = grow(&wb.bsplit, wb.cap_bsplit, nb_cap, 8, "window splits");
     if (st == GV_OK) st = grow(&wb.tile_cnt, wb.cap_tiles, ntiles + 2, 4, "window tiles");
-    const uint32_t *dsrc = src, *ddst = dst;
+    if (st == GV_OK) st = grow(&wb.src, wb.cap_src, pcap, 4, "window src");
+    if (st == GV_OK) st = grow(&wb.dst, wb.cap_dst, pcap, 4, "window dst");
+    if (st == GV_OK && !wb.wctl) {
+        cudaError_t e = cudaMalloc(&wb.wctl, 64);
+        if (e != cudaSuccess) st = cuda_status(e, "window control");
+    }
     if (st == GV_OK && mem == GV_MEM_HOST) {
         const uint32_t n = g->d.n;
         for (uint64_t i = 0; i < total; ++i)
             if (src[i] >= n || dst[i] >= n) { set_error("vertex id out of range"); st = GV_ERR_INVALID; break; }
-        if (st == GV_OK) st = grow(&wb.src, wb.cap_src, total, 4, "window src");
-        if (st == GV_OK) st = grow(&wb.dst, wb.cap_dst, total, 4, "window dst");
-        if (st == GV_OK) {
-            cudaMemcpyAsync(wb.src, src, total * 4, cudaMemcpyHostToDevice, s);
-            cudaMemcpyAsync(wb.dst, dst, total * 4, cudaMemcpyHostToDevice, s);
-            dsrc = wb.src;
-            ddst = wb.dst;
-        }
     }
+    Ctl cc{};
     if (st == GV_OK) {
+        const cudaMemcpyKind k = mem == GV_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+        cudaError_t e = cudaMemcpyAsync(wb.src, src, total * 4, k, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(wb.dst, dst, total * 4, k, s);
         std::vector<unsigned long long> hs(nbatches), hp(nbatches);
         for (uint32_t i = 0; i < nbatches; ++i) {
             hs[i] = descs[i].offset;
             hp[i] = descs[i].offset + descs[i].n_insert;
         }
-        cudaMemcpyAsync(wb.bstart, hs.data(), nbatches * 8, cudaMemcpyHostToDevice, s);
-        cudaMemcpyAsync(wb.bsplit, hp.data(), nbatches * 8, cudaMemcpyHostToDevice, s);
-        // the host vectors die here: wait for the copies before returning
-        cudaError_t e = cudaStreamSynchronize(s);
-        if (e != cudaSuccess) st = cuda_status(e, "window descriptors");
+        WinHeader h{total, nbatches, 0};
+        if (e == cudaSuccess) e = cudaMemcpyAsync(wb.bstart, hs.data(), nbatches * 8, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(wb.bsplit, hp.data(), nbatches * 8, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(wb.hdr(), &h, sizeof(h), cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&cc, g->d.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s);
+        // the host vectors and the header die here: wait for the copies before returning
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) st = cuda_status(e, "window inputs");
     }
     if (st == GV_OK) {
-        if (flags & GV_BATCH_GRAPH) {
-            if (!wb.cap_stream) cudaStreamCreateWithFlags(&wb.cap_stream, cudaStreamNonBlocking);
-            cudaGraph_t graph = nullptr;
-            cudaGraphExec_t exec = nullptr;
-            cudaError_t e = cudaStreamBeginCapture(wb.cap_stream, cudaStreamCaptureModeRelaxed);
-            if (e == cudaSuccess) {
-                enqueue_window(g, wb, nbatches, dsrc, ddst, total, flags, wb.cap_stream);
-                e = cudaStreamEndCapture(wb.cap_stream, &graph);
+        // Admission for the persistent path: the free stack must hold the
+        // worst case of the window, one block per touched vertex plus one
+        // per B inserted entries; otherwise the two-stage path plans the
+        // blocks exactly and rejects the window if they do not fit.
+        const uint64_t worst = (E + g->d.B - 1) / g->d.B + std::min<uint64_t>(E, g->d.n);
+        if (worst <= cc.free_top) {
+            ++wb.persistent;
+            if (flags & GV_BATCH_GRAPH) st = run_window_graph(g, wb, Ecap, nb_cap, flags, s);
+            else {
+                enqueue_window_persistent(g, wb, Ecap, flags, s);
+                st = cuda_status(cudaGetLastError(), "window launch");
             }
-            if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
-            if (e == cudaSuccess) e = cudaGraphLaunch(exec, s);
-            if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // the exec is destroyed below
-            if (exec) cudaGraphExecDestroy(exec);
-            if (graph) cudaGraphDestroy(graph);
-            st = cuda_status(e, "window graph");
         } else {
-            enqueue_window(g, wb, nbatches, dsrc, ddst, total, flags, s);
+            ++wb.exact;
+            enqueue_window(g, wb, nbatches, wb.src, wb.dst, total, flags, s);
             st = cuda_status(cudaGetLastError(), "window launch");
         }
     }
@@ -282,9 +612,11 @@ extern "C" gv_status gv_batch_run(gv_graph *g, const gv_batch_desc *descs, uint3
     return st;
 }
 
-// Autotuner: builds the sample graph once per candidate (edge-block size x
-// threads per vertex), times one window of batches and one PageRank with
-// CUDA events, and keeps the fastest total.
+// Autotuner: for every candidate (edge-block size x threads per vertex)
+// builds the sample graph, times one window of batches and one PageRank
+// with CUDA events, and repeats that on a fresh graph; the first round
+// warms the candidate up (scratch growth) and is dropped, the median of the
+// other rounds is kept.  The candidate with the smallest median total wins.
 extern "C" gv_status gv_autotune(const gv_config *base, const uint32_t *src0, const uint32_t *dst0, uint64_t k0,
                                  const gv_batch_desc *descs, uint32_t nbatches, const uint32_t *bsrc,
                                  const uint32_t *bdst, int mem, gv_tune_result *results, uint32_t *nresults,
@@ -301,30 +633,41 @@ extern "C" gv_status gv_autotune(const gv_config *base, const uint32_t *src0, co
     cudaEventCreate(&e2);
     gv_status st = GV_OK;
     std::vector<float> x(base->num_vertices);
+    constexpr int ROUNDS = 4;  // one warm-up, three timed
     for (uint32_t B : blocks)
         for (uint32_t T : tpvs) {
             gv_config c = *base;
             c.block_size = B;
             c.threads_per_vertex = T;
-            gv_graph *g = nullptr;
-            st = gv_create(&c, &g);
-            if (st != GV_OK) break;
-            st = gv_insert_edges(g, src0, dst0, nullptr, k0, mem, nullptr);
-            if (st == GV_OK) st = gv_synchronize(g, nullptr);
-            float upd = 0.f, pr = 0.f;
-            if (st == GV_OK) {
-                cudaEventRecord(e0, 0);
-                st = gv_batch_run(g, descs, nbatches, bsrc, bdst, mem, GV_BATCH_COMPACT, nullptr);
-                cudaEventRecord(e1, 0);
-                int32_t sw = 0;
-                if (st == GV_OK) st = gv_pagerank(g, 0.85f, 1e-6f, 100, x.data(), &sw, GV_MEM_HOST, nullptr);
-                cudaEventRecord(e2, 0);
-                cudaEventSynchronize(e2);
-                cudaEventElapsedTime(&upd, e0, e1);
-                cudaEventElapsedTime(&pr, e1, e2);
+            std::vector<float> upd_ms, pr_ms;
+            for (int r = 0; r < ROUNDS && st == GV_OK; ++r) {
+                gv_graph *g = nullptr;
+                st = gv_create(&c, &g);
+                if (st != GV_OK) break;
+                st = gv_insert_edges(g, src0, dst0, nullptr, k0, mem, nullptr);
+                if (st == GV_OK) st = gv_synchronize(g, nullptr);
+                float upd = 0.f, pr = 0.f;
+                if (st == GV_OK) {
+                    cudaEventRecord(e0, 0);
+                    st = gv_batch_run(g, descs, nbatches, bsrc, bdst, mem, GV_BATCH_COMPACT, nullptr);
+                    cudaEventRecord(e1, 0);
+                    int32_t sw = 0;
+                    if (st == GV_OK) st = gv_pagerank(g, 0.85f, 1e-6f, 100, x.data(), &sw, GV_MEM_HOST, nullptr);
+                    cudaEventRecord(e2, 0);
+                    cudaEventSynchronize(e2);
+                    cudaEventElapsedTime(&upd, e0, e1);
+                    cudaEventElapsedTime(&pr, e1, e2);
+                }
+                gv_destroy(g);
+                if (r > 0) {
+                    upd_ms.push_back(upd);
+                    pr_ms.push_back(pr);
+                }
             }
-            gv_destroy(g);
             if (st != GV_OK) break;
+            std::sort(upd_ms.begin(), upd_ms.end());
+            std::sort(pr_ms.begin(), pr_ms.end());
+            const float upd = upd_ms[upd_ms.size() / 2], pr = pr_ms[pr_ms.size() / 2];
             if (results && nresults && nr < *nresults) results[nr] = {B, T, upd, pr};
             ++nr;
             if (upd + pr < best_ms) {

@@ -77,8 +77,17 @@ gv_status run_update(gv_graph *g, const uint32_t *dsrc, const uint32_t *ddst, co
 gv_status apply_sorted(gv_graph *g, const unsigned long long *K, const uint32_t *V, uint64_t E, bool symmetric,
                        const float *dw, bool is_delete, bool finish, cudaStream_t s);
 void launch_commit_keep_abort(gv_graph *g, cudaStream_t s);
+// One persistent launch applying a window's net segments (both operations;
+// btype[i] = 1 for an insert), then the commit of its block allocation.
+// queue[0..2] must be zero; big_list holds up to nseg entries.
+gv_status launch_window_apply(gv_graph *g, const uint32_t *seg_vertex, const uint32_t *seg_start,
+                              const uint32_t *bdst, const uint32_t *btype, uint8_t *found, uint32_t *big_list,
+                              unsigned long long *queue, cudaStream_t s);
 void launch_finish(gv_graph *g, cudaStream_t s);
 void release_window(gv_graph *g);
+// Window counters of gv_batch_run (keys window_captures, window_replays,
+// window_persistent, window_exact); false for other keys.
+bool window_stat(gv_graph *g, const char *key, double *value);
 gv_status run_compact(gv_graph *g, cudaStream_t s);
 // Tombstones every entry whose source or destination is flagged in del[n].
 gv_status run_vertex_delete(gv_graph *g, const uint8_t *del, cudaStream_t s);

@@ -483,6 +483,253 @@ __global__ void __launch_bounds__(BIG_THREADS) k_apply_big(DevGraph g, const uin
     }
 }
 
+// ------------------------------------------------------------ window apply
+// A window's net updates in one persistent launch.  The window has been
+// reduced to the last operation per pair, so every touched vertex u has one
+// segment: its destinations sorted, each marked insert or delete, and no
+// pair appears twice.  Units of work are segments, taken from a device
+// queue: first the big ones (more than BIG_BLOCKS blocks or BIG_SEGMENT
+// entries), one per CTA, then chunks of WIN_CHUNK small ones per warp, a
+// lane group per segment.  A unit scans u's blocks once: an entry found
+// among the segment's deletes becomes a tombstone, one found among its
+// inserts marks that insert as already present.  The remaining inserts are
+// appended after the last used slot into blocks popped from the free stack
+// (warp-aggregated atomics), the new blocks are linked into the CBT and the
+// vertex record is rewritten.  The caller has checked that the free stack
+// holds the window's worst case (one block per segment plus one per B
+// inserts), so no unit can run out; a unit that would still overrun the
+// stack records GV_DEV_ERR_NOMEM and writes nothing past it.
+constexpr uint32_t WIN_CHUNK = 64;
+
+struct WinSegs {
+    const uint32_t *seg_vertex, *seg_start, *bdst;
+    const uint32_t *btype;       // per entry: 1 insert, 0 delete
+    uint8_t *found;              // per entry: the insert is already stored
+    uint32_t *big_list;          // big segments
+    unsigned long long *queue;   // [0] next big unit, [1] next small chunk, [2] big units
+};
+
+__device__ __forceinline__ uint32_t win_new_blocks(uint32_t fill, uint32_t nb_old, uint32_t newcnt, uint32_t logB) {
+    const uint32_t room = (nb_old << logB) - fill;
+    const uint32_t extra = newcnt > room ? newcnt - room : 0u;
+    return (extra + (1u << logB) - 1u) >> logB;
+}
+
+// Rewrites u's record after a unit (one thread).
+__device__ __forceinline__ void win_record(const DevGraph &g, uint32_t u, uint4 rec, uint32_t nb_old, uint32_t newcnt,
+                                           uint32_t nnew, uint32_t ndel, unsigned long long top, uint32_t base) {
+    if (!newcnt && !ndel) return;
+    uint4 nrec = rec;
+    if (newcnt) {
+        const uint32_t newfill = rec.y + newcnt;
+        if (nb_old > 0) g.bcount[rec.w] = min(g.B, newfill - ((nb_old - 1) << g.logB));
+        nrec.x = nb_old ? rec.x : new_block(g, top, base, 0);
+        nrec.y = newfill;
+        nrec.w = nnew ? new_block(g, top, base, nnew - 1) : rec.w;
+    }
+    nrec.z = rec.z - ndel + newcnt;
+    g.vtx[u] = nrec;
+    atomicAdd(&g.ctl->live_edges, (unsigned long long)((long long)newcnt - (long long)ndel));
+    if (ndel && !g.dirty[u]) {
+        g.dirty[u] = 1;
+        g.dirty_list[atomicAdd(&g.ctl->ndirty, 1ull)] = u;
+    }
+}
+
+__global__ void k_window_classify(DevGraph g, WinSegs w) {
+    const uint32_t nseg = (uint32_t)g.ctl->nseg;
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < nseg; s += gridDim.x * blockDim.x) {
+        const uint32_t len = w.seg_start[s + 1] - w.seg_start[s];
+        const uint32_t nb = blocks_for(g.vtx[w.seg_vertex[s]].y, g.logB);
+        if (is_big(nb, len)) w.big_list[atomicAdd(&w.queue[2], 1ull)] = s;
+    }
+}
+
+template <int TPV>
+__global__ void __launch_bounds__(BIG_THREADS) k_window_apply(DevGraph g, WinSegs w) {
+    constexpr int GPC = BIG_THREADS / TPV;
+    constexpr int GPW = 32 / TPV;
+    __shared__ uint32_t tab[BIG_TAB];
+    __shared__ uint32_t tabs[GPC][BIG_BLOCKS];
+    __shared__ uint32_t wt[33];
+    __shared__ uint32_t unit_s;
+    __shared__ unsigned long long base_s;
+    if (g.ctl->batch_abort) return;
+    const unsigned long long top = g.ctl->free_top;
+    const uint32_t nbig = (uint32_t)w.queue[2];
+    // ---- big segments: one CTA each
+    for (;;) {
+        if (threadIdx.x == 0) unit_s = (uint32_t)min(atomicAdd(&w.queue[0], 1ull), 0xFFFFFFFFull);
+        __syncthreads();
+        const uint32_t bi = unit_s;
+        __syncthreads();
+        if (bi >= nbig) break;
+        const uint32_t s = w.big_list[bi];
+        const uint32_t u = w.seg_vertex[s];
+        const uint32_t st = w.seg_start[s], len = w.seg_start[s + 1] - st;
+        const uint4 rec = g.vtx[u];
+        const uint32_t fill = rec.y, nb_old = blocks_for(fill, g.logB);
+        const uint32_t *D = w.bdst + st;
+        const uint32_t *T = w.btype + st;
+        uint32_t ndel = 0;
+        for (uint32_t k0 = 0; k0 < nb_old; k0 += BIG_TAB) {
+            const uint32_t kc = min((uint32_t)BIG_TAB, nb_old - k0);
+            fill_block_table(g, rec.x, k0, kc, tab, threadIdx.x, BIG_THREADS);
+            __syncthreads();
+            const uint32_t e0 = k0 << g.logB;
+            const uint32_t e1 = min(fill, (k0 + kc) << g.logB);
+            const uint32_t nq = (e1 - e0 + 3) >> 2;
+            for (uint32_t q = threadIdx.x; q < nq; q += BIG_THREADS) {
+                const uint32_t e = e0 + (q << 2);
+                uint32_t *slot = g.pool + ((size_t)tab[(e >> g.logB) - k0] << g.logB) + (e & (g.B - 1));
+                const uint4 v = *reinterpret_cast<const uint4 *>(slot);
+                const uint32_t ev[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    if (e + j < e1 && ev[j] != GV_TOMB) {
+                        const uint32_t idx = lower_bound_u32(D, len, ev[j]);
+                        if (idx < len && D[idx] == ev[j]) {
+                            if (T[idx]) w.found[st + idx] = 1;
+                            else {
+                                slot[j] = GV_TOMB;
+                                ++ndel;
+                            }
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        ndel = cta_sum<uint32_t, BIG_THREADS>(ndel, wt);
+        uint32_t c = 0;
+        for (uint32_t i = threadIdx.x; i < len; i += BIG_THREADS) c += (T[i] && !w.found[st + i]) ? 1u : 0u;
+        const uint32_t newcnt = cta_sum<uint32_t, BIG_THREADS>(c, wt);
+        uint32_t nnew = win_new_blocks(fill, nb_old, newcnt, g.logB);
+        if (threadIdx.x == 0) base_s = nnew ? atomicAdd(&g.ctl->alloc_cursor, (unsigned long long)nnew) : 0ull;
+        __syncthreads();
+        const unsigned long long b64 = base_s;
+        uint32_t ins = newcnt;
+        if (b64 + nnew > top) {  // unreachable after the host's admission check; never write past the stack
+            if (threadIdx.x == 0) atomicOr(&g.ctl->status, GV_DEV_ERR_NOMEM);
+            ins = 0;
+            nnew = 0;
+        }
+        const uint32_t base = (uint32_t)b64;
+        if (ins) {
+            uint32_t j0 = 0;
+            for (uint32_t c0 = 0; c0 < len; c0 += BIG_THREADS) {
+                const uint32_t i = c0 + threadIdx.x;
+                const uint32_t isnew = (i < len && T[i] && !w.found[st + i]) ? 1u : 0u;
+                uint32_t tot;
+                const uint32_t pre = cta_excl_scan<uint32_t, BIG_THREADS>(isnew, wt, tot);
+                if (isnew) {
+                    const uint32_t p = fill + j0 + pre;
+                    const uint32_t k = p >> g.logB;
+                    const uint32_t b = (k < nb_old) ? rec.w : new_block(g, top, base, k - nb_old);
+                    g.pool[((size_t)b << g.logB) + (p & (g.B - 1))] = D[i];
+                }
+                j0 += tot;
+            }
+            link_new_blocks(g, u, rec, nb_old, nnew, fill + ins, top, base, threadIdx.x, BIG_THREADS,
+                            [] { __syncthreads(); });
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) win_record(g, u, rec, nb_old, ins, nnew, ndel, top, base);
+        __syncthreads();
+    }
+    // ---- small segments: chunks per warp, a lane group per segment
+    Group<TPV> G;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t gw = lane / TPV;
+    uint32_t *mytab = tabs[threadIdx.x / TPV];
+    const uint32_t nseg = (uint32_t)g.ctl->nseg;
+    for (;;) {
+        unsigned long long c0 = 0;
+        if (lane == 0) c0 = atomicAdd(&w.queue[1], (unsigned long long)WIN_CHUNK);
+        c0 = __shfl_sync(GV_FULL_MASK, c0, 0);
+        if (c0 >= nseg) break;
+        const uint32_t cend = (uint32_t)min((unsigned long long)nseg, c0 + WIN_CHUNK);
+        for (uint32_t r = (uint32_t)c0; r < cend; r += GPW) {  // warp-uniform rounds
+            const uint32_t s = r + gw;
+            bool active = s < cend;
+            uint32_t u = 0, st = 0, len = 0, fill = 0, nb_old = 0;
+            uint4 rec = make_uint4(0, 0, 0, 0);
+            if (active) {
+                u = w.seg_vertex[s];
+                st = w.seg_start[s];
+                len = w.seg_start[s + 1] - st;
+                rec = g.vtx[u];
+                fill = rec.y;
+                nb_old = blocks_for(fill, g.logB);
+                active = !is_big(nb_old, len);
+            }
+            const uint32_t *D = w.bdst + st;
+            const uint32_t *T = w.btype + st;
+            uint32_t ndel = 0;
+            if (active) {
+                fill_block_table(g, rec.x, 0, nb_old, mytab, G.gl, TPV);
+                G.sync();
+                const uint32_t nq = (fill + 3) >> 2;
+                for (uint32_t q = G.gl; q < nq; q += TPV) {
+                    const uint32_t e = q << 2;
+                    uint32_t *slot = g.pool + ((size_t)mytab[e >> g.logB] << g.logB) + (e & (g.B - 1));
+                    const uint4 v = *reinterpret_cast<const uint4 *>(slot);
+                    const uint32_t ev[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        if (e + j < fill && ev[j] != GV_TOMB) {
+                            const uint32_t idx = lower_bound_u32(D, len, ev[j]);
+                            if (idx < len && D[idx] == ev[j]) {
+                                if (T[idx]) w.found[st + idx] = 1;
+                                else {
+                                    slot[j] = GV_TOMB;
+                                    ++ndel;
+                                }
+                            }
+                        }
+                    }
+                }
+            }
+            ndel = G.sum(ndel);
+            G.sync();
+            uint32_t c = 0;
+            if (active)
+                for (uint32_t i = G.gl; i < len; i += TPV) c += (T[i] && !w.found[st + i]) ? 1u : 0u;
+            const uint32_t newcnt = G.sum(c);
+            uint32_t nnew = active ? win_new_blocks(fill, nb_old, newcnt, g.logB) : 0u;
+            const unsigned long long off = warp_agg_alloc(&g.ctl->alloc_cursor, (G.gl == 0) ? nnew : 0u);
+            const unsigned long long b64 = G.bcast(off, 0);
+            uint32_t ins = active ? newcnt : 0u;
+            if (b64 + nnew > top) {  // see the admission note above
+                if (active && G.gl == 0) atomicOr(&g.ctl->status, GV_DEV_ERR_NOMEM);
+                ins = 0;
+                nnew = 0;
+            }
+            const uint32_t base = (uint32_t)b64;
+            if (ins) {
+                uint32_t j0 = 0;
+                for (uint32_t cc = 0; cc < len; cc += TPV) {
+                    const uint32_t i = cc + G.gl;
+                    const uint32_t isnew = (i < len && T[i] && !w.found[st + i]) ? 1u : 0u;
+                    uint32_t tot;
+                    const uint32_t pre = G.excl_scan(isnew, tot);
+                    if (isnew) {
+                        const uint32_t p = fill + j0 + pre;
+                        const uint32_t k = p >> g.logB;
+                        const uint32_t b = (k < nb_old) ? rec.w : new_block(g, top, base, k - nb_old);
+                        g.pool[((size_t)b << g.logB) + (p & (g.B - 1))] = D[i];
+                    }
+                    j0 += tot;
+                }
+                link_new_blocks(g, u, rec, nb_old, nnew, fill + ins, top, base, G.gl, TPV, [&] { G.sync(); });
+            }
+            G.sync();
+            if (active && G.gl == 0) win_record(g, u, rec, nb_old, ins, nnew, ndel, top, base);
+            G.sync();
+        }
+    }
+}
+
 // -------------------------------------------------------------- compaction
 // Stable in-place compaction of one vertex: live entries keep their order,
 // tail blocks that end up empty go back to the free stack and are unlinked
@@ -832,6 +1079,26 @@ void launch_commit_keep_abort(gv_graph *g, cudaStream_t s) {
 }
 
 void launch_finish(gv_graph *g, cudaStream_t s) { GV_LAUNCH(k_finish, 1, 1, 0, s, g->d.ctl); }
+
+gv_status launch_window_apply(gv_graph *g, const uint32_t *seg_vertex, const uint32_t *seg_start,
+                              const uint32_t *bdst, const uint32_t *btype, uint8_t *found, uint32_t *big_list,
+                              unsigned long long *queue, cudaStream_t s) {
+    DevGraph d = g->d;
+    WinSegs w{seg_vertex, seg_start, bdst, btype, found, big_list, queue};
+    {
+        ProfScope ps(PROF_MEMBER, s);
+        GV_LAUNCH(k_window_classify, 148 * 4, 256, 0, s, d, w);
+    }
+    {
+        ProfScope ps(PROF_APPLY, s);
+        dispatch_tpv(g->cfg.threads_per_vertex, [&](auto t) {
+            constexpr int T = decltype(t)::value;
+            GV_LAUNCH((k_window_apply<T>), 148 * 2, BIG_THREADS, 0, s, d, w);
+        });
+    }
+    GV_LAUNCH(k_finish, 1, 1, 0, s, d.ctl);
+    return cuda_status(cudaGetLastError(), "window apply launch");
+}
 
 gv_status apply_sorted(gv_graph *g, const unsigned long long *K, const uint32_t *V, uint64_t E, bool symmetric,
                        const float *dw, bool is_delete, bool finish, cudaStream_t s) {

@@ -191,7 +191,11 @@ gv_status gv_check(gv_graph *g, uint64_t *violations, uint32_t *first_code,
  * N+(u)), "tc_probes" / "tc_core" (bit probes against the dense-core rows
  * and core vertices of the last total-only count; 0 when it merged every
  * edge), "tc_oriented_edges", "tc_subset_local" (1 if the last subset count
- * took the neighbour-hash path), "sweeps" (last PageRank).  Synchronous. */
+ * took the neighbour-hash path), "sweeps" (last PageRank), and counts of
+ * gv_batch_run windows: "window_persistent" / "window_exact" (windows that
+ * took the persistent one-launch apply / the two-stage exact path),
+ * "window_captures" / "window_replays" (CUDA graphs captured / replayed).
+ * Synchronous. */
 gv_status gv_last_stat(gv_graph *g, const char *key, double *value);
 
 /* ---- analytics ---------------------------------------------------------- */

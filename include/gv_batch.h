@@ -23,12 +23,15 @@ typedef struct gv_batch_desc {
 
 enum {
     GV_BATCH_COMPACT = 1u, /* compact once after the window */
-    GV_BATCH_GRAPH = 2u    /* capture the window into a CUDA graph and launch that */
+    GV_BATCH_GRAPH = 2u    /* run the window as a CUDA graph, captured once per capacity (entries
+                              rounded up to a power of two) and replayed for later windows */
 };
 
 /* Applies nbatches batches in order; the final graph equals applying them
  * one by one with gv_insert_edges / gv_delete_edges.  The window is reduced
- * to the last operation per pair and applied in one pass (see batch.cu).
+ * to the last operation per pair and applied by one persistent launch that
+ * scans every touched vertex once (when the free blocks cover the window's
+ * worst case; else by an exact two-stage pass, see batch.cu).
  * descs is host memory; src/dst are `mem` (total pairs = sum of the batch
  * sizes, batches laid out consecutively).  A window that names an id >= n
  * or exhausts the pool is rejected whole (gv_synchronize reports it).
@@ -44,8 +47,10 @@ gv_status gv_ppr_batch(gv_graph *g, const uint32_t *sources, uint32_t k, float a
 
 /* Autotuner: times a sample workload (build from src0/dst0, one window of
  * batches, one PageRank) for every edge-block size {32, 64, 128} and
- * threads-per-vertex {4, 8, 16, 32}; writes one result per candidate and
- * the fastest configuration into *best (base config otherwise). */
+ * threads-per-vertex {4, 8, 16, 32}: one warm-up round, then the median of
+ * three rounds, each on a freshly built graph; writes one result per
+ * candidate and the fastest configuration into *best (base config
+ * otherwise). */
 typedef struct gv_tune_result {
     uint32_t block_size;
     uint32_t threads_per_vertex;

@@ -68,6 +68,100 @@ def test_window_equals_sequential(graph_mode, device_inputs):
     assert_sound(g)
 
 
+def test_window_graph_is_captured_once_and_replayed():
+    """Windows of the same capacity replay one captured graph (sizes are read
+    on the device); every window leaves the graph the oracle's sequential
+    application leaves."""
+    scale = 11
+    n = 1 << scale
+    s, d = rmat_graph(scale, 16, seed=13)
+    o = oracle.OracleGraph(n)
+    o.insert(s, d)
+    g = make_graph(n)
+    g.batch_insert(s, d)
+    rng = np.random.default_rng(21)
+    for w in range(4):
+        off, dst, _ = o.export()
+        batches = _window(n, off, dst, rng, nb=int(rng.integers(3, 10)))
+        g.batch_run(batches, compact=True, graph=True)
+        g.synchronize()
+        for ins_s, ins_d, del_s, del_d in batches:
+            o.insert(ins_s, ins_d)
+            o.delete(del_s, del_d)
+        assert_same_adjacency(g, o)
+        assert_sound(g)
+    assert g.last_stat("window_persistent") == 4
+    assert g.last_stat("window_captures") == 1
+    assert g.last_stat("window_replays") == 3
+
+
+def test_window_hub_segments_and_mixed_operations():
+    """Segments above the lane-group limits (a hub with more than 64 blocks of
+    32 entries, a window putting thousands of entries on one vertex) go to
+    whole CTAs of the persistent launch; inserts and deletes of the same
+    vertex in one segment."""
+    n = 1 << 14
+    rng = np.random.default_rng(3)
+    others = np.setdiff1d(np.arange(n, dtype=np.uint32), [7, 11])
+    h7 = rng.permutation(others)[:6000]  # 188 blocks of 32
+    bs, bd = rmat_graph(14, 4, seed=3)
+    s = np.concatenate([np.full(len(h7), 7, np.uint32), bs])
+    d = np.concatenate([h7, bd])
+    g = make_graph(n, block_size=32, threads_per_vertex=8)
+    g.batch_insert(s, d)
+    o = oracle.OracleGraph(n)
+    o.insert(s, d)
+    batches = []
+    for b in range(6):
+        ins_d = rng.permutation(others)[:1500].astype(np.uint32)   # new and existing neighbours of 7
+        del_d = rng.choice(h7, 800, replace=False).astype(np.uint32)
+        hub11 = rng.permutation(others)[:3000].astype(np.uint32)    # a vertex that becomes a hub in the window
+        batches.append((np.concatenate([np.full(1500, 7, np.uint32), np.full(3000, 11, np.uint32)]),
+                        np.concatenate([ins_d, hub11]),
+                        np.concatenate([del_d, np.full(100, 11, np.uint32)]),
+                        np.concatenate([np.full(800, 7, np.uint32), hub11[:100]])))
+    g.batch_run(batches, compact=True)
+    g.synchronize()
+    for ins_s, ins_d, del_s, del_d in batches:
+        o.insert(ins_s, ins_d)
+        o.delete(del_s, del_d)
+    assert_same_adjacency(g, o)
+    assert_sound(g)
+    assert g.last_stat("window_persistent") == 1
+
+
+def test_window_exact_path_when_the_pool_is_tight():
+    """A pool too small for the persistent path's worst case takes the
+    two-stage path, which still applies a window that fits and rejects one
+    that does not, whole."""
+    n = 1 << 10
+    s, d = rmat_graph(10, 4, seed=9)
+    g = make_graph(n, block_size=32, pool_blocks=2600)
+    g.batch_insert(s, d)
+    g.synchronize()
+    o = oracle.OracleGraph(n)
+    o.insert(s, d)
+    rng = np.random.default_rng(4)
+    off, dst, _ = o.export()
+    batches = _window(n, off, dst, rng, nb=3)
+    g.batch_run(batches, compact=True)
+    g.synchronize()
+    for ins_s, ins_d, del_s, del_d in batches:
+        o.insert(ins_s, ins_d)
+        o.delete(del_s, del_d)
+    assert_same_adjacency(g, o)
+    assert g.last_stat("window_exact") >= 1
+    # a window far beyond the free blocks is rejected and leaves the graph as it was
+    before = g.export_csr()
+    big_s, big_d = gv_b200.gen_uniform(n, 200_000, seed=5)
+    g.batch_run([(big_s, big_d, big_s[:0], big_d[:0])], compact=True)
+    with pytest.raises(gv_b200.GvError):
+        g.synchronize()
+    after = g.export_csr()
+    assert np.array_equal(before[0], after[0])
+    assert_sound(g)
+
+
 def test_window_rejects_bad_ids_whole():
     import torch
     n = 512
