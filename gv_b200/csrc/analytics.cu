@@ -603,6 +603,12 @@ gv_status pagerank_impl(gv_graph *g, float alpha, float eps, int max_iter, const
         if (sweeps) *sweeps = sw;
         return st;
     }
+    if (plan_pagerank_enabled(g)) {  // the degree-ordered sweep plan (prplan.cu)
+        bool planned = false;
+        gv_status st = plan_pagerank(g, alpha, eps, max_iter, x_init, init_mem, source, x_out, sweeps, mem, s,
+                                     &planned);
+        if (st != GV_OK || planned) return st;
+    }
     const uint32_t parts = SWEEP_PARTS;
     void *buf = analytics_scratch(g, iter_bytes(n, parts));
     if (!buf) return GV_ERR_NOMEM;

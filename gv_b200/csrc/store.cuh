@@ -49,7 +49,7 @@ struct gv_graph {
     int32_t last_tc_local = 0;  // 1: the last subset count took the local path
     int32_t last_sweeps = 0;
     // independent auxiliary device buffers, grown on demand
-    static constexpr int AUX_SLOTS = 12;
+    static constexpr int AUX_SLOTS = 16;
     void *aux[AUX_SLOTS] = {};
     size_t aux_bytes[AUX_SLOTS] = {};
     // a view shares the parent's store and owns only analytics scratch
@@ -95,6 +95,13 @@ gv_status run_export(gv_graph *g, unsigned long long *offsets, uint32_t *dst, fl
                      cudaStream_t s);
 gv_status run_check(gv_graph *g, uint64_t *violations, uint32_t *code, uint32_t *vertex);
 void launch_degrees(gv_graph *g, uint32_t *deg, cudaStream_t s);
+// PageRank (x_init / source as gv_pagerank's internals take them) over a
+// degree-ordered padded CSR built for the call (prplan.cu).  *planned =
+// false, with nothing done, when the graph does not qualify (directed or
+// weighted stores, more than 2^32 padded entries, GV_PR_PLAN=0).
+bool plan_pagerank_enabled(gv_graph *g);
+gv_status plan_pagerank(gv_graph *g, float alpha, float eps, int max_iter, const float *x_init, int init_mem,
+                        uint32_t source, float *x_out, int32_t *sweeps, int mem, cudaStream_t s, bool *planned);
 // Incident-triangle counts of the subset d_sub[ns] (device) into d_out[ns]
 // from neighbour hash sets, without a whole-graph pass.  *done = false (and
 // nothing written) when the subset's neighbourhoods are too large for that

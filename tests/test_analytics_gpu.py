@@ -44,6 +44,44 @@ def test_pagerank_matches_oracle(graph12):
     assert abs(sweeps - o.pagerank(0.85, 1e-6, 100)[1]) <= 1
 
 
+@pytest.mark.parametrize("plan", ["1", "0"])
+def test_pagerank_plan_and_store_sweeps_match_oracle(plan, monkeypatch):
+    """The degree-ordered sweep plan (default) and the store sweep
+    (GV_PR_PLAN=0) on a graph with every tier: isolated vertices, rows below
+    8, 64 and 2048 entries, and hubs cut into several items; static,
+    warm-started and personalised runs against the oracle."""
+    monkeypatch.setenv("GV_PR_PLAN", plan)
+    n = 1 << 13
+    rng = np.random.default_rng(31)
+    s, d = rmat_graph(13, 8, seed=31)
+    hub = np.full(7000, 3, np.uint32)
+    hub_d = rng.choice(np.setdiff1d(np.arange(n, dtype=np.uint32), [3]), 7000, replace=False).astype(np.uint32)
+    s = np.concatenate([s, hub])
+    d = np.concatenate([d, hub_d])
+    g = make_graph(n, threads_per_vertex=8)
+    g.batch_insert(s, d)
+    o = oracle.OracleGraph(n)
+    o.insert(s, d)
+    deg = g.degrees()
+    assert (deg == 0).any() and deg.max() > 3 * 2048
+    x, sweeps = g.static_pagerank(0.85, 1e-6, 100)
+    xo, _ = o.pagerank(0.85, 1e-6, 100, fixed_sweeps=sweeps)
+    assert np.abs(x.astype(np.float64) - xo).sum() < PR_L1
+    # warm start after a batch: the same fixed point
+    ins_s, ins_d = gv_b200.gen_uniform(n, 3000, seed=8)
+    g.batch_insert(ins_s, ins_d)
+    o.insert(ins_s, ins_d)
+    xd, sd = g.dynamic_pagerank(x, 0.85, 1e-6, 100)
+    xod, _ = o.pagerank(0.85, 1e-6, 100, x_init=x.astype(np.float64), fixed_sweeps=sd)
+    assert np.abs(xd.astype(np.float64) - xod).sum() < PR_L1
+    # personalised from the hub and from a leaf
+    for src in (3, int(np.nonzero(deg == 1)[0][0])):
+        xp, sp = g.ppr(src, 0.85, 1e-6, 100)
+        xop, _ = o.ppr(src, 0.85, 1e-6, 100, fixed_sweeps=sp)
+        assert np.abs(xp.astype(np.float64) - xop).sum() < PR_L1
+    g.close()
+
+
 def test_pagerank_fixed_sweeps_and_tombstones(graph12):
     n, _, _ = graph12
     s, d = rmat_graph(12, 16, seed=21)
