@@ -136,14 +136,21 @@ def test_window_exact_path_when_the_pool_is_tight():
     that does not, whole."""
     n = 1 << 10
     s, d = rmat_graph(10, 4, seed=9)
-    g = make_graph(n, block_size=32, pool_blocks=2600)
+    probe = make_graph(n, block_size=32, pool_blocks=1 << 14)
+    probe.batch_insert(s, d)
+    cap, free = probe.pool_stats()
+    used = cap - free
+    probe.close()
+    # room for the window's exact needs, far less than its worst case
+    # (one block per touched vertex plus one per 32 inserted entries)
+    g = make_graph(n, block_size=32, pool_blocks=used + 150)
     g.batch_insert(s, d)
     g.synchronize()
     o = oracle.OracleGraph(n)
     o.insert(s, d)
     rng = np.random.default_rng(4)
     off, dst, _ = o.export()
-    batches = _window(n, off, dst, rng, nb=3)
+    batches = _window(n, off, dst, rng, nb=1)
     g.batch_run(batches, compact=True)
     g.synchronize()
     for ins_s, ins_d, del_s, del_d in batches:
