@@ -10,9 +10,11 @@
 // the L1 keeps holds one hot value and seven cold ones.  The plan renumbers
 // the vertices by descending degree class (stable in id order inside a
 // class), so the hot contributions are contiguous: the top 16 K fit in 64 KB
-// and stay in L1, the top 256 K in 1 MB of L2.  Rows are padded to whole
-// 16-byte quads with a sentinel neighbour whose contribution is 0, so every
-// load is an aligned uint4 and no tombstone or fill test remains.
+// and stay in L1, the top 256 K in 1 MB of L2.  A row is the vertex's used
+// slots in block order, tombstones and the padding to whole 16-byte quads
+// written as a sentinel neighbour whose contribution is 0, so every load is
+// an aligned uint4 and no tombstone or fill test remains; slot e of block k
+// lands at k*B + e, so the blocks of a hub are copied in parallel.
 //
 // The plan: perm (new row -> vertex), inv (vertex -> new row), off[n+1]
 // (uint32 row starts), col (neighbour rows, padded), the degree-class tier
@@ -106,29 +108,81 @@ __global__ void k_pl_class_starts(const uint32_t *__restrict__ start, uint32_t n
     if (i < NCLASS) out[i] = start[(size_t)i * ntiles];
 }
 
-// padded row lengths in plan order, and the old-id degrees for the export
+// Padded row lengths in plan order: a row holds the vertex's used slots
+// (tombstones included, as the sentinel) rounded up to whole quads, so slot e
+// of block k lands at k*B + e of the row and blocks are copied independently.
+// Also the inverse live degrees and, per row of two or more blocks, its
+// number of 32-block copy items.
 __global__ void k_pl_rowlen(DevGraph g, const uint32_t *__restrict__ perm, uint32_t *__restrict__ plen,
-                            float *__restrict__ rdeg) {
+                            float *__restrict__ rdeg, uint32_t *__restrict__ fitems) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += gridDim.x * blockDim.x) {
-        const uint32_t d = g.vtx[perm[i]].z;
-        plen[i] = (d + 3u) & ~3u;
-        rdeg[i] = d ? 1.0f / (float)d : 0.f;
+        const uint4 rec = g.vtx[perm[i]];
+        plen[i] = (rec.y + 3u) & ~3u;
+        rdeg[i] = rec.z ? 1.0f / (float)rec.z : 0.f;
+        const uint32_t nb = blocks_for(rec.y, g.logB);
+        fitems[i] = nb > 1 ? (nb + 31u) >> 5 : 0u;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) rdeg[g.n] = 0.f;
 }
 
-// Row i of the plan from row perm[i] of the exported CSR: neighbours
-// renumbered, the tail padded with the sentinel row n.  A warp per row.
-__global__ void k_pl_fill(uint32_t n, const uint32_t *__restrict__ perm, const uint32_t *__restrict__ inv,
-                          const unsigned long long *__restrict__ xoff, const uint32_t *__restrict__ xdst,
-                          const uint32_t *__restrict__ off, uint32_t *__restrict__ col) {
+__device__ __forceinline__ uint32_t pl_map(uint32_t e, uint32_t slot, uint32_t fill, const uint32_t *__restrict__ inv,
+                                           uint32_t n) {
+    return (slot < fill && e != GV_TOMB) ? inv[e] : n;
+}
+
+// Rows of at most one block: 8 lanes per row copy its quads, neighbours
+// renumbered, tombstones and the padding as the sentinel n.
+__global__ void k_pl_fill_small(DevGraph g, const uint32_t *__restrict__ perm, const uint32_t *__restrict__ inv,
+                                const uint32_t *__restrict__ off, uint32_t *__restrict__ col) {
+    Group<8> G;
+    const uint32_t ng = gridDim.x * (blockDim.x / 8);
+    for (uint32_t i = blockIdx.x * (blockDim.x / 8) + threadIdx.x / 8; i < g.n; i += ng) {
+        const uint4 rec = g.vtx[perm[i]];
+        if (rec.y > g.B) continue;  // the copy items take it
+        const uint32_t o = off[i], nq = (off[i + 1] - o) >> 2;
+        const uint4 *src = reinterpret_cast<const uint4 *>(g.pool + ((size_t)rec.x << g.logB));
+        uint4 *dst = reinterpret_cast<uint4 *>(col + o);
+        for (uint32_t q = G.gl; q < nq; q += 8) {
+            const uint4 v = src[q];
+            const uint32_t e = q << 2;
+            dst[q] = make_uint4(pl_map(v.x, e, rec.y, inv, g.n), pl_map(v.y, e + 1, rec.y, inv, g.n),
+                                pl_map(v.z, e + 2, rec.y, inv, g.n), pl_map(v.w, e + 3, rec.y, inv, g.n));
+        }
+    }
+}
+
+// Rows of two or more blocks: a warp per item of 32 blocks, the lanes walk
+// the tree to one block each, then copy the blocks quad by quad.
+__global__ void k_pl_fill_items(DevGraph g, const uint32_t *__restrict__ perm, const uint32_t *__restrict__ inv,
+                                const uint32_t *__restrict__ off, const uint32_t *__restrict__ frow,
+                                const uint32_t *__restrict__ ffirst, uint32_t nitems, uint32_t *__restrict__ col) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t nw = gridDim.x * (blockDim.x >> 5);
-    for (uint32_t i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += nw) {
-        const uint32_t v = perm[i];
-        const unsigned long long a = xoff[v], d = xoff[v + 1] - a;
-        const uint32_t o = off[i], len = off[i + 1] - o;
-        for (uint32_t k = lane; k < len; k += 32) col[o + k] = (k < d) ? inv[xdst[a + k]] : n;
+    const uint32_t qpb = g.B >> 2;  // quads per block
+    for (uint32_t it = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); it < nitems; it += nw) {
+        const uint32_t r = frow[it];
+        const uint4 rec = g.vtx[perm[r]];
+        const uint32_t nb = blocks_for(rec.y, g.logB);
+        const uint32_t kb0 = (it - ffirst[r]) << 5;
+        const uint32_t k = kb0 + lane;
+        const uint32_t myb = k < nb ? (k == 0 ? rec.x : cbt_block(g.left, g.right, rec.x, k)) : GV_NIL;
+        const uint32_t o = off[r];
+        const uint32_t nk = min(32u, nb - kb0);
+        for (uint32_t j = 0; j < nk; ++j) {
+            const uint32_t b = __shfl_sync(GV_FULL_MASK, myb, j);
+            const uint32_t kk = kb0 + j;
+            const uint32_t e0 = kk << g.logB;
+            const uint32_t quads = (min(g.B, rec.y - e0) + 3u) >> 2;
+            const uint4 *src = reinterpret_cast<const uint4 *>(g.pool + ((size_t)b << g.logB));
+            uint4 *dst = reinterpret_cast<uint4 *>(col + o + e0);
+            for (uint32_t q = lane; q < quads; q += 32) {
+                const uint4 v = src[q];
+                const uint32_t e = e0 + (q << 2);
+                dst[q] = make_uint4(pl_map(v.x, e, rec.y, inv, g.n), pl_map(v.y, e + 1, rec.y, inv, g.n),
+                                    pl_map(v.z, e + 2, rec.y, inv, g.n), pl_map(v.w, e + 3, rec.y, inv, g.n));
+            }
+        }
+        (void)qpb;
     }
 }
 
@@ -341,11 +395,11 @@ gv_status plan_pagerank(gv_graph *g, float alpha, float eps, int max_iter, const
     Ctl cc;
     gv_status st = read_ctl(g, &cc, s);
     if (st != GV_OK) return st;
-    const uint64_t live = cc.live_edges;
-    const uint64_t padded_max = live + 3ull * n;
+    // rows hold the used slots (at most the used blocks' slots) plus padding
+    const uint64_t padded_max = (d.P - cc.free_top) * (uint64_t)d.B + 3ull * n;
     if (padded_max >= 0xFFFFFFF0ull || n == 0) return GV_OK;  // uint32 row starts: the store sweep serves it
     const uint32_t ntiles = (n + PL_TILE - 1) / PL_TILE;
-    // scratch: plan arrays (aux slot 12), padded columns (13), export (14)
+    // scratch: plan arrays (aux slot 12), padded columns (13), copy items (14), hub items (15)
     const size_t plan_bytes = (size_t)5 * 256 + ((size_t)NCLASS * ntiles + 1) * 4 + (size_t)n * 4 * 2 +
                               ((size_t)n + 1) * 4 * 3 + ((size_t)n + 1) * 4 * 4 + (size_t)(NCLASS + 8) * 4 +
                               ((size_t)n + 1) * 8 + (size_t)PL_GRID * 8 + PL_FIN * 8 + 64 + 16 * 256;
@@ -362,7 +416,6 @@ gv_status plan_pagerank(gv_graph *g, float alpha, float eps, int max_iter, const
     float *c0 = carve<float>(p, (size_t)n + 1);
     float *c1 = carve<float>(p, (size_t)n + 1);
     uint32_t *cls = carve<uint32_t>(p, NCLASS + 8);
-    unsigned long long *xoff = carve<unsigned long long>(p, (size_t)n + 1);
     double *partial = carve<double>(p, PL_GRID + PL_FIN);
     int *state = carve<int>(p, 16);
     // class order of the rows
@@ -371,12 +424,15 @@ gv_status plan_pagerank(gv_graph *g, float alpha, float eps, int max_iter, const
     GV_LAUNCH(k_pl_place, (ntiles + PL_THREADS / 32 - 1) / (PL_THREADS / 32), PL_THREADS, 0, s, d, ntiles,
               (const uint32_t *)cnt, perm, inv);
     GV_LAUNCH(k_pl_class_starts, 1, 64, 0, s, (const uint32_t *)cnt, ntiles, cls);
-    // row lengths, starts, inverse degrees
-    GV_LAUNCH(k_pl_rowlen, grid_for(n, 256), 256, 0, s, d, (const uint32_t *)perm, off, rdeg);
+    // row lengths, starts, inverse degrees, copy items of the multi-block rows
+    uint32_t *ffirst = ifirst;  // free until the hub items are built
+    GV_LAUNCH(k_pl_rowlen, grid_for(n, 256), 256, 0, s, d, (const uint32_t *)perm, off, rdeg, ffirst);
     scan_exclusive_u32(off, off, n, off + n, g->bs.scan_tmp, s);
-    uint32_t hcls[NCLASS], total = 0;
+    scan_exclusive_u32(ffirst, ffirst, n, ffirst + n, g->bs.scan_tmp, s);
+    uint32_t hcls[NCLASS], total = 0, nfill = 0;
     cudaMemcpyAsync(hcls, cls, NCLASS * 4, cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(&total, off + n, 4, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(&nfill, ffirst + n, 4, cudaMemcpyDeviceToHost, s);
     cudaError_t e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_status(e, "plan classes");
     // rows of class c hold degrees [2^(c-1), 2^c); classes run in descending order:
@@ -386,17 +442,17 @@ gv_status plan_pagerank(gv_graph *g, float alpha, float eps, int max_iter, const
         return hcls[NCLASS - c];                                  // start of class c - 1
     };
     const uint32_t rH = first_row_below(HUB_DEG), rW = first_row_below(WARP_DEG), rG = first_row_below(GROUP_DEG);
-    // the exported CSR (vertex order), then the renumbered padded columns
+    // the padded, renumbered columns, straight from the store's blocks
     uint32_t *col = (uint32_t *)aux_scratch(g, 13, ((size_t)total + 4) * 4 + 256);
-    uint32_t *xdst = (uint32_t *)aux_scratch(g, 14, (size_t)(live + 1) * 4 + 256);
-    if (!col || !xdst) return GV_ERR_NOMEM;
-    uint32_t *deg = ifirst;  // free until the items are built
-    launch_degrees(g, deg, s);
-    scan_exclusive_u32_to_u64(deg, xoff, n, xoff + n, g->bs.scan_tmp, s);
-    st = run_export(g, xoff, xdst, nullptr, s);
-    if (st != GV_OK) return st;
-    GV_LAUNCH(k_pl_fill, 148 * 16, PL_THREADS, 0, s, n, (const uint32_t *)perm, (const uint32_t *)inv,
-              (const unsigned long long *)xoff, (const uint32_t *)xdst, (const uint32_t *)off, col);
+    uint32_t *frow = (uint32_t *)aux_scratch(g, 14, ((size_t)nfill + 1) * 4 + 256);
+    if (!col || !frow) return GV_ERR_NOMEM;
+    GV_LAUNCH(k_pl_fill_small, 148 * 16, PL_THREADS, 0, s, d, (const uint32_t *)perm, (const uint32_t *)inv,
+              (const uint32_t *)off, col);
+    if (nfill) {
+        GV_LAUNCH(k_pl_item_fill, grid_for(n, 256), 256, 0, s, (const uint32_t *)ffirst, n, frow);
+        GV_LAUNCH(k_pl_fill_items, 148 * 16, PL_THREADS, 0, s, d, (const uint32_t *)perm, (const uint32_t *)inv,
+                  (const uint32_t *)off, (const uint32_t *)frow, (const uint32_t *)ffirst, nfill, col);
+    }
     // hub items
     uint32_t nitems = 0;
     uint32_t *irow = nullptr;

@@ -141,16 +141,20 @@ def test_window_exact_path_when_the_pool_is_tight():
     cap, free = probe.pool_stats()
     used = cap - free
     probe.close()
-    # room for the window's exact needs, far less than its worst case
-    # (one block per touched vertex plus one per 32 inserted entries)
-    g = make_graph(n, block_size=32, pool_blocks=used + 150)
-    g.batch_insert(s, d)
-    g.synchronize()
     o = oracle.OracleGraph(n)
     o.insert(s, d)
     rng = np.random.default_rng(4)
     off, dst, _ = o.export()
     batches = _window(n, off, dst, rng, nb=1)
+    # one block short of the window's worst case (one block per 32 of its
+    # directed entries plus one per touched vertex), which is more than the
+    # blocks it really needs
+    E = 2 * sum(len(a) + len(c) for a, b, c, e in batches)
+    worst = (E + 31) // 32 + min(E, n)
+    g = make_graph(n, block_size=32, pool_blocks=used + worst - 1)
+    g.batch_insert(s, d)
+    g.synchronize()
+    assert g.pool_stats()[1] == worst - 1
     g.batch_run(batches, compact=True)
     g.synchronize()
     for ins_s, ins_d, del_s, del_d in batches:
