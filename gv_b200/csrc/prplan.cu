@@ -272,8 +272,9 @@ __device__ __forceinline__ void pl_items(const PlanSweep &a, uint32_t vb, uint32
     }
 }
 
-// rows of TPV lanes each over [r0, r1): quads strided by TPV, two in flight
-template <int TPV>
+// rows of TPV lanes each over [r0, r1): quads strided by TPV, QF of them
+// (4 QF gathers) in flight per lane
+template <int TPV, int QF>
 __device__ __forceinline__ void pl_rows(const PlanSweep &a, uint32_t r0, uint32_t r1, uint32_t vb, uint32_t vg,
                                         double &res) {
     Group<TPV> G;
@@ -284,11 +285,15 @@ __device__ __forceinline__ void pl_rows(const PlanSweep &a, uint32_t r0, uint32_
         const uint32_t nq = (a.off[i + 1] - o) >> 2;
         const uint4 *q = reinterpret_cast<const uint4 *>(a.col + o);
         float sum = 0.f;
-        for (uint32_t j = G.gl; j < nq; j += 2 * TPV) {
-            const uint4 v0 = __ldcs(q + j);
-            uint4 v1 = make_uint4(a.n, a.n, a.n, a.n);
-            if (j + TPV < nq) v1 = __ldcs(q + j + TPV);
-            sum += gather4(a.gather, v0) + gather4(a.gather, v1);
+        for (uint32_t j = G.gl; j < nq; j += QF * TPV) {
+            uint4 v[QF];
+#pragma unroll
+            for (int t = 0; t < QF; ++t)
+                v[t] = (j + t * TPV < nq) ? __ldcs(q + j + t * TPV) : make_uint4(a.n, a.n, a.n, a.n);
+            float part = 0.f;
+#pragma unroll
+            for (int t = 0; t < QF; ++t) part += gather4(a.gather, v[t]);
+            sum += part;
         }
         if (TPV > 1) sum = G.sum(sum);
         if (G.gl == 0) pl_finish(a, i, sum, res);
@@ -303,9 +308,9 @@ __global__ void __launch_bounds__(PL_THREADS) k_pl_sweep(PlanSweep a) {
     const uint32_t r = blockIdx.x % PL_PERIOD, w = blockIdx.x / PL_PERIOD, waves = gridDim.x / PL_PERIOD;
     double res = 0.0;
     if (r < t0) pl_items(a, w * t0 + r, waves * t0);
-    else if (r < t0 + t1) pl_rows<32>(a, a.rH, a.rW, w * t1 + (r - t0), waves * t1, res);
-    else if (r < t0 + t1 + t2) pl_rows<8>(a, a.rW, a.rG, w * t2 + (r - t0 - t1), waves * t2, res);
-    else pl_rows<1>(a, a.rG, a.n, w * t3 + (r - t0 - t1 - t2), waves * t3, res);
+    else if (r < t0 + t1) pl_rows<32, 4>(a, a.rH, a.rW, w * t1 + (r - t0), waves * t1, res);
+    else if (r < t0 + t1 + t2) pl_rows<8, 2>(a, a.rW, a.rG, w * t2 + (r - t0 - t1), waves * t2, res);
+    else pl_rows<1, 2>(a, a.rG, a.n, w * t3 + (r - t0 - t1 - t2), waves * t3, res);
     res = warp_sum(res);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = res;
     __syncthreads();
