@@ -58,6 +58,7 @@ def parse():
     ap.add_argument("--no-batching", action="store_true", help="skip the scale-24 batched-vs-plain section")
     ap.add_argument("--batch-scale", type=int, default=24)
     ap.add_argument("--c3-batches", type=int, default=64)
+    ap.add_argument("--no-autotune", action="store_true", help="batching section: use --block/--tpv, skip the autotuner")
     ap.add_argument("--no-incremental", action="store_true", help="skip the incremental triangle-count section")
     ap.add_argument("--no-ingest", action="store_true", help="skip the Matrix-Market / snapshot section")
     ap.add_argument("--ingest-scale", type=int, default=20)
@@ -350,13 +351,16 @@ def run_batching(args, dev, hbm_peak):
     n = 1 << scale
     seed = args.seed + 100
     # autotune on a scale-20 sample of the same workload shape
-    ts, td = gv_b200.gen_rmat(20, 16 << 20, seed)
-    to = gv_b200.GraphVine(1 << 20, hbm_budget_bytes=4 << 30)
-    to.batch_insert(ts, td)
-    toff, tdst, _ = to.export_csr()
-    to.close()
-    tune_batches = make_c3_batches(1 << 20, toff, tdst, 16, seed, hi=200_000)
-    best, tune = gv_b200.autotune(1 << 20, ts, td, tune_batches, hbm_budget_bytes=4 << 30)
+    if args.no_autotune:
+        best, tune = {"block_size": args.block, "threads_per_vertex": args.tpv}, []
+    else:
+        ts, td = gv_b200.gen_rmat(20, 16 << 20, seed)
+        to = gv_b200.GraphVine(1 << 20, hbm_budget_bytes=4 << 30)
+        to.batch_insert(ts, td)
+        toff, tdst, _ = to.export_csr()
+        to.close()
+        tune_batches = make_c3_batches(1 << 20, toff, tdst, 16, seed, hi=200_000)
+        best, tune = gv_b200.autotune(1 << 20, ts, td, tune_batches, hbm_budget_bytes=4 << 30)
     cfg = dict(block_size=best["block_size"], threads_per_vertex=best["threads_per_vertex"],
                hbm_budget_bytes=24 << 30, max_batch_pairs=1 << 22, device=dev.index or 0)
     s_dev, d_dev = gv_b200.gen_rmat(scale, args.edge_factor << scale, seed, device=dev)
