@@ -23,7 +23,8 @@
 // contiguous per tier): hubs of at least HUB_DEG entries are cut into items
 // of ITEM_ENTRIES for one warp each (partials combined in item order), rows
 // of WARP_DEG or more take a warp, rows of GROUP_DEG or more 8 lanes, the
-// rest one thread.  One launch runs the four tiers, CTAs interleaved in
+// rest one thread; isolated rows take their value once and are not swept.
+// One launch runs the four tiers, CTAs interleaved in
 // proportion to their work; a finish kernel combines the hub partials and a
 // one-CTA kernel sums the per-CTA residuals in a fixed order (deterministic).
 //
@@ -50,8 +51,8 @@ constexpr uint32_t ITEM_ENTRIES = 2048;
 constexpr uint32_t WARP_DEG = 64;
 constexpr uint32_t GROUP_DEG = 8;
 constexpr unsigned PL_PERIOD = 16;
-constexpr unsigned PL_WAVES = 148 * 16 / PL_PERIOD;
-constexpr unsigned PL_GRID = PL_PERIOD * PL_WAVES;
+constexpr unsigned PL_WAVES_MAX = 148 * 16 / PL_PERIOD;
+constexpr unsigned PL_GRID = PL_PERIOD * PL_WAVES_MAX;  // residual slots (the most CTAs a sweep launches)
 constexpr unsigned PL_FIN = 148;
 
 __device__ __forceinline__ uint32_t deg_class(uint32_t d) { return d ? 32u - __clz(d) : 0u; }
@@ -199,13 +200,25 @@ __global__ void k_pl_item_fill(const uint32_t *__restrict__ ifirst, uint32_t nhu
 
 // x0 in plan order (from the caller's start, or 1/n, or the source), its
 // contributions; x_out in vertex order at the end
+// Isolated rows [rz, n) take their final value (the base, plus the source
+// term) in both iterate buffers here and are left out of the sweeps.
 __global__ void k_pl_init(uint32_t n, const uint32_t *__restrict__ perm, const float *__restrict__ xin,
                           float fill, uint32_t src_row, float src_val, const float *__restrict__ rdeg,
-                          float *__restrict__ x, float *__restrict__ c) {
+                          uint32_t rz, float base, float src_base, float *__restrict__ x, float *__restrict__ c,
+                          float *__restrict__ x_other, float *__restrict__ c_other) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i <= n; i += gridDim.x * blockDim.x) {
         if (i == n) {
             x[n] = 0.f;
             c[n] = 0.f;
+            c_other[n] = 0.f;
+            continue;
+        }
+        if (i >= rz) {
+            const float v = base + (i == src_row ? src_base : 0.f);
+            x[i] = v;
+            x_other[i] = v;
+            c[i] = 0.f;
+            c_other[i] = 0.f;
             continue;
         }
         const float v = xin ? xin[perm[i]] : (i == src_row ? src_val : fill);
@@ -232,7 +245,7 @@ struct PlanSweep {
     float alpha, base;
     uint32_t src_row;     // personalised source (plan order) or GV_NIL
     float src_val;
-    uint32_t rH, rW, rG, n, nitems;
+    uint32_t rH, rW, rG, rZ, n, nitems;  // tier row boundaries; rows [rZ, n) are isolated
     uint32_t split;       // CTAs per period: items | warp << 8 | group << 16 | thread << 24
 };
 
@@ -310,7 +323,7 @@ __global__ void __launch_bounds__(PL_THREADS) k_pl_sweep(PlanSweep a) {
     if (r < t0) pl_items(a, w * t0 + r, waves * t0);
     else if (r < t0 + t1) pl_rows<32, 4>(a, a.rH, a.rW, w * t1 + (r - t0), waves * t1, res);
     else if (r < t0 + t1 + t2) pl_rows<8, 2>(a, a.rW, a.rG, w * t2 + (r - t0 - t1), waves * t2, res);
-    else pl_rows<1, 2>(a, a.rG, a.n, w * t3 + (r - t0 - t1 - t2), waves * t3, res);
+    else pl_rows<1, 2>(a, a.rG, a.rZ, w * t3 + (r - t0 - t1 - t2), waves * t3, res);
     res = warp_sum(res);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = res;
     __syncthreads();
@@ -407,7 +420,8 @@ gv_status plan_pagerank(gv_graph *g, float alpha, float eps, int max_iter, const
     // scratch: plan arrays (aux slot 12), padded columns (13), copy items (14), hub items (15)
     const size_t plan_bytes = (size_t)5 * 256 + ((size_t)NCLASS * ntiles + 1) * 4 + (size_t)n * 4 * 2 +
                               ((size_t)n + 1) * 4 * 3 + ((size_t)n + 1) * 4 * 4 + (size_t)(NCLASS + 8) * 4 +
-                              ((size_t)n + 1) * 8 + (size_t)PL_GRID * 8 + PL_FIN * 8 + 64 + 16 * 256;
+                              ((size_t)n + 1) * 8 + (size_t)PL_GRID * 8 + PL_FIN * 8 + 64 + 16 * 256 +
+                              (size_t)n * 4;
     char *p = (char *)aux_scratch(g, 12, plan_bytes);
     if (!p) return GV_ERR_NOMEM;
     uint32_t *cnt = carve<uint32_t>(p, (size_t)NCLASS * ntiles + 1);
@@ -423,6 +437,7 @@ gv_status plan_pagerank(gv_graph *g, float alpha, float eps, int max_iter, const
     uint32_t *cls = carve<uint32_t>(p, NCLASS + 8);
     double *partial = carve<double>(p, PL_GRID + PL_FIN);
     int *state = carve<int>(p, 16);
+    float *xstage = carve<float>(p, n);  // a host start vector, vertex order
     // class order of the rows
     GV_LAUNCH(k_pl_count, std::min<uint32_t>(ntiles, 148 * 8), PL_THREADS, 0, s, d, ntiles, cnt);
     scan_exclusive_u32(cnt, cnt, (uint64_t)NCLASS * ntiles, cnt + (size_t)NCLASS * ntiles, g->bs.scan_tmp, s);
@@ -447,6 +462,7 @@ gv_status plan_pagerank(gv_graph *g, float alpha, float eps, int max_iter, const
         return hcls[NCLASS - c];                                  // start of class c - 1
     };
     const uint32_t rH = first_row_below(HUB_DEG), rW = first_row_below(WARP_DEG), rG = first_row_below(GROUP_DEG);
+    const uint32_t rZ = hcls[NCLASS - 1];  // first isolated row (class 0 comes last)
     // the padded, renumbered columns, straight from the store's blocks
     uint32_t *col = (uint32_t *)aux_scratch(g, 13, ((size_t)total + 4) * 4 + 256);
     uint32_t *frow = (uint32_t *)aux_scratch(g, 14, ((size_t)nfill + 1) * 4 + 256);
@@ -481,29 +497,29 @@ gv_status plan_pagerank(gv_graph *g, float alpha, float eps, int max_iter, const
     if (x_init) {
         if (init_mem == GV_MEM_DEVICE) xin = x_init;
         else {
-            e = cudaMemcpyAsync(x1, x_init, (size_t)n * 4, cudaMemcpyHostToDevice, s);
+            e = cudaMemcpyAsync(xstage, x_init, (size_t)n * 4, cudaMemcpyHostToDevice, s);
             if (e != cudaSuccess) return cuda_status(e, "pagerank init");
-            xin = x1;
+            xin = xstage;
         }
     }
     e = cudaStreamSynchronize(s);  // src_row
     if (e != cudaSuccess) return cuda_status(e, "plan source");
     const float fill = source == GV_NIL ? 1.0f / (float)n : 0.f;
-    // x0 and its contributions in plan order (a host start was staged in x1)
+    // x0 and its contributions in plan order; the isolated rows, which the
+    // sweeps never reach, get their value in x1 too
+    const float base = source == GV_NIL ? (1.0f - alpha) / (float)n : 0.f;
     GV_LAUNCH(k_pl_init, grid_for((uint64_t)n + 1, 256), 256, 0, s, n, (const uint32_t *)perm, xin, fill, src_row,
-              1.f, (const float *)rdeg, x0, c0);
-    // c1[n] stays 0 for the padding sentinel
-    cudaMemsetAsync(c1 + n, 0, 4, s);
+              1.f, (const float *)rdeg, rZ, base, source == GV_NIL ? 0.f : 1.0f - alpha, x0, c0, x1, c1);
     cudaMemsetAsync(state, 0, 16, s);
     cudaMemsetAsync(partial, 0, (PL_GRID + PL_FIN) * 8, s);
     // tier work (entries + 16 per row) from the row starts
     uint32_t hoff[4] = {0, 0, 0, 0};
-    const uint32_t rows[4] = {rH, rW, rG, n};
+    const uint32_t rows[4] = {rH, rW, rG, rZ};
     for (int i = 0; i < 4; ++i) cudaMemcpyAsync(&hoff[i], off + rows[i], 4, cudaMemcpyDeviceToHost, s);
     e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_status(e, "plan tiers");
     const double w[4] = {(double)hoff[0], (double)(hoff[1] - hoff[0]) + 16.0 * (rW - rH),
-                         (double)(hoff[2] - hoff[1]) + 16.0 * (rG - rW), (double)(hoff[3] - hoff[2]) + 16.0 * (n - rG)};
+                         (double)(hoff[2] - hoff[1]) + 16.0 * (rG - rW), (double)(hoff[3] - hoff[2]) + 16.0 * (rZ - rG)};
     // the sweep uses little shared memory: give the SM's on-chip memory to L1,
     // where the hot contributions live
     cudaFuncSetAttribute(k_pl_sweep, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
@@ -518,15 +534,23 @@ gv_status plan_pagerank(gv_graph *g, float alpha, float eps, int max_iter, const
     a.state = state;
     a.ipart = ipart;
     a.alpha = alpha;
-    a.base = source == GV_NIL ? (1.0f - alpha) / (float)n : 0.f;
+    a.base = base;
     a.src_row = src_row;
     a.src_val = source == GV_NIL ? 0.f : 1.0f - alpha;
     a.rH = rH;
     a.rW = rW;
     a.rG = rG;
+    a.rZ = rZ;
     a.n = n;
     a.nitems = nitems;
     a.split = plan_split(w);
+    // CTAs of the sweep: rounds of PL_PERIOD; GV_PL_WAVES overrides the number of rounds
+    unsigned waves = 148 * 8 / PL_PERIOD;  // one wave of 8 resident CTAs per SM
+    if (const char *env = std::getenv("GV_PL_WAVES")) {
+        const unsigned w = (unsigned)std::strtoul(env, nullptr, 10);
+        if (w >= 1 && w <= PL_WAVES_MAX) waves = w;
+    }
+    const unsigned grid = waves * PL_PERIOD;
     float *xa = x0, *xb = x1, *ca = c0, *cb = c1;
     int h_state[2] = {0, 0};
     int launched = 0;
@@ -539,7 +563,7 @@ gv_status plan_pagerank(gv_graph *g, float alpha, float eps, int max_iter, const
             a.cnew = cb;
             {
                 ProfScope ps(PROF_PULL, s);
-                GV_LAUNCH(k_pl_sweep, PL_GRID, PL_THREADS, 0, s, a);
+                GV_LAUNCH(k_pl_sweep, grid, PL_THREADS, 0, s, a);
                 if (rH) GV_LAUNCH(k_pl_hub_fin, PL_FIN, PL_THREADS, 0, s, a, PL_GRID);
             }
             GV_LAUNCH(k_pl_done, 1, 256, 0, s, (const double *)partial, PL_GRID + PL_FIN, eps, state);
