@@ -51,7 +51,7 @@ constexpr uint32_t ITEM_ENTRIES = 2048;
 constexpr uint32_t WARP_DEG = 64;
 constexpr uint32_t GROUP_DEG = 8;
 constexpr unsigned PL_PERIOD = 16;
-constexpr unsigned PL_WAVES_MAX = 148 * 32 / PL_PERIOD;
+constexpr unsigned PL_WAVES_MAX = 148 * 64 / PL_PERIOD;
 constexpr unsigned PL_GRID = PL_PERIOD * PL_WAVES_MAX;  // residual slots (the most CTAs a sweep launches)
 constexpr unsigned PL_FIN = 148;
 
@@ -543,9 +543,10 @@ gv_status plan_pagerank(gv_graph *g, float alpha, float eps, int max_iter, const
     a.nitems = nitems;
     a.split = plan_split(w);
     // CTAs of the sweep: rounds of PL_PERIOD; GV_PL_WAVES overrides the number of rounds
-    // two waves of 8 resident CTAs per SM: 0.359 ms per sweep at R-MAT scale
-    // 22 against 0.406 with one wave and 0.395 with one and a half
-    unsigned waves = 148 * 16 / PL_PERIOD;
+    // four waves of 8 resident CTAs per SM: at R-MAT scale 22 a sweep takes
+    // 0.325 ms with four, 0.338 with three, 0.359 with two and 0.406 with one
+    // (smaller CTA shares even out the tiers' tails)
+    unsigned waves = 148 * 32 / PL_PERIOD;
     if (const char *env = std::getenv("GV_PL_WAVES")) {
         const unsigned w = (unsigned)std::strtoul(env, nullptr, 10);
         if (w >= 1 && w <= PL_WAVES_MAX) waves = w;
