@@ -51,7 +51,7 @@ constexpr uint32_t ITEM_ENTRIES = 2048;
 constexpr uint32_t WARP_DEG = 64;
 constexpr uint32_t GROUP_DEG = 8;
 constexpr unsigned PL_PERIOD = 16;
-constexpr unsigned PL_WAVES_MAX = 148 * 64 / PL_PERIOD;
+constexpr unsigned PL_WAVES_MAX = 148 * 128 / PL_PERIOD;
 constexpr unsigned PL_GRID = PL_PERIOD * PL_WAVES_MAX;  // residual slots (the most CTAs a sweep launches)
 constexpr unsigned PL_FIN = 148;
 
@@ -543,10 +543,10 @@ gv_status plan_pagerank(gv_graph *g, float alpha, float eps, int max_iter, const
     a.nitems = nitems;
     a.split = plan_split(w);
     // CTAs of the sweep: rounds of PL_PERIOD; GV_PL_WAVES overrides the number of rounds
-    // four waves of 8 resident CTAs per SM: at R-MAT scale 22 a sweep takes
-    // 0.325 ms with four, 0.338 with three, 0.359 with two and 0.406 with one
-    // (smaller CTA shares even out the tiers' tails)
-    unsigned waves = 148 * 32 / PL_PERIOD;
+    // eight waves of 8 resident CTAs per SM: at R-MAT scale 22 a sweep takes
+    // 0.309 ms with eight, 0.314 with six, 0.325 with four, 0.359 with two and
+    // 0.406 with one (smaller CTA shares even out the tiers' tails)
+    unsigned waves = 148 * 64 / PL_PERIOD;
     if (const char *env = std::getenv("GV_PL_WAVES")) {
         const unsigned w = (unsigned)std::strtoul(env, nullptr, 10);
         if (w >= 1 && w <= PL_WAVES_MAX) waves = w;
@@ -565,9 +565,9 @@ gv_status plan_pagerank(gv_graph *g, float alpha, float eps, int max_iter, const
             {
                 ProfScope ps(PROF_PULL, s);
                 GV_LAUNCH(k_pl_sweep, grid, PL_THREADS, 0, s, a);
-                if (rH) GV_LAUNCH(k_pl_hub_fin, PL_FIN, PL_THREADS, 0, s, a, PL_GRID);
+                if (rH) GV_LAUNCH(k_pl_hub_fin, PL_FIN, PL_THREADS, 0, s, a, grid);
             }
-            GV_LAUNCH(k_pl_done, 1, 256, 0, s, (const double *)partial, PL_GRID + PL_FIN, eps, state);
+            GV_LAUNCH(k_pl_done, 1, 256, 0, s, (const double *)partial, grid + PL_FIN, eps, state);
             std::swap(xa, xb);
             std::swap(ca, cb);
         }

@@ -330,6 +330,13 @@ extern "C" gv_status gv_serve_trace(gv_graph *g, const gv_serve_config *cfg, con
         if (!bc.reqs.empty()) jobs.push_back(bc);
         if (!ppr.reqs.empty()) jobs.push_back(ppr);
         if (!tc.reqs.empty()) jobs.push_back(tc);
+        // shortest kinds first: PPR batches and the triangle count start
+        // before the BC passes, which would otherwise hold the slots and the
+        // HBM budget while they queue
+        std::stable_sort(jobs.begin(), jobs.end(), [](const Job &x, const Job &y) {
+            auto rank = [](uint32_t k) { return k == GV_REQ_BC ? 2 : k == GV_REQ_PPR ? 1 : 0; };
+            return rank(x.kind) < rank(y.kind);
+        });
         for (Job &jb : jobs) {
             jb.epoch = epoch;
             jb.group = ++group;

@@ -9,7 +9,8 @@
  * admitted as slots free up (continuous batching): arrived PPR queries are
  * merged into batched launches, arrived triangle-subset queries share one
  * triangle count, arrived BC queries run in pairs whose sources share one
- * set of BFS passes (gv_bc_multi).  Epochs: with fresh = 0 a query sees exactly the updates
+ * set of BFS passes (gv_bc_multi); the triangle count and the PPR batches are
+ * dispatched before the BC passes (shortest kinds first).  Epochs: with fresh = 0 a query sees exactly the updates
  * that arrived before it; with fresh = 1 (the default) it sees at least
  * those, so queries that arrive behind an update wait for it and run
  * together after it.  results[i].epoch names the updates each query saw (the
