@@ -415,6 +415,17 @@ gv_status gv_view_create(gv_graph *g, gv_graph **out) {
     return GV_OK;
 }
 
+void release_analytics_scratch(gv_graph *g) {
+    if (g->an_buf) cudaFree(g->an_buf);
+    g->an_buf = nullptr;
+    g->an_bytes = 0;
+    for (int i = 0; i < gv_graph::AUX_SLOTS; ++i) {
+        if (g->aux[i]) cudaFree(g->aux[i]);
+        g->aux[i] = nullptr;
+        g->aux_bytes[i] = 0;
+    }
+}
+
 gv_status gv_destroy(gv_graph *g) {
     if (!g) return GV_OK;
     DeviceGuard dg(g->cfg.device);

@@ -16,6 +16,7 @@
 #include <cstring>
 #include <deque>
 #include <mutex>
+#include <string>
 #include <thread>
 #include <vector>
 #include "../../include/gv_serve.h"
@@ -50,6 +51,7 @@ struct Server {
     uint32_t inflight = 0;
     bool stop = false;
     gv_status first_error = GV_OK;
+    std::string err;
 
     double now() const { return std::chrono::duration<double>(clk::now() - t0).count(); }
 
@@ -69,19 +71,21 @@ struct Server {
         size_t bytes = 0;
         void *get(size_t want) {
             if (want <= bytes) return p;
-            if (p) cudaFree(p);
-            p = nullptr;
-            bytes = 0;
+            release();
             if (cudaMalloc(&p, want) != cudaSuccess) {
                 cudaGetLastError();
+                set_error("serving result buffer of " + std::to_string(want) + " B");
                 return nullptr;
             }
             bytes = want;
             return p;
         }
-        ~DevBuf() {
+        void release() {
             if (p) cudaFree(p);
+            p = nullptr;
+            bytes = 0;
         }
+        ~DevBuf() { release(); }
     };
 
     void run_job(gv_graph *view, cudaStream_t s, DevBuf &buf, Job &jb) {
@@ -165,7 +169,10 @@ struct Server {
             rr.group = jb.group;
         }
         std::lock_guard<std::mutex> lk(mu);
-        if (st != GV_OK && first_error == GV_OK) first_error = st;
+        if (st != GV_OK && first_error == GV_OK) {
+            first_error = st;
+            err = gv_last_error_string();  // the message lives in this worker thread
+        }
     }
 
     void worker(int w) {
@@ -183,8 +190,14 @@ struct Server {
                 if (busy[w] != 1 && stop) break;
                 jb = job[w];
             }
-            if (vs == GV_OK) run_job(view, s, buf, jb);
-            else {
+            if (vs == GV_OK) {
+                run_job(view, s, buf, jb);
+                // The admission budget counts the scratch of the jobs in
+                // flight; a view keeping the scratch of its last job would
+                // hold memory the budget has handed to the next ones.
+                release_analytics_scratch(view);
+                buf.release();
+            } else {
                 std::lock_guard<std::mutex> lk(mu);
                 if (first_error == GV_OK) first_error = vs;
             }
@@ -405,5 +418,6 @@ extern "C" gv_status gv_serve_trace(gv_graph *g, const gv_serve_config *cfg, con
     for (auto &t : pool) t.join();
     cudaStreamDestroy(us);
     if (st != GV_OK) return st;
+    if (S.first_error != GV_OK) set_error(S.err);
     return S.first_error;
 }

@@ -66,6 +66,8 @@ gv_status ensure_batch_scratch(gv_graph *g, uint64_t entries, uint64_t pairs);
 void *analytics_scratch(gv_graph *g, size_t bytes);
 // Auxiliary buffer `slot` (0..AUX_SLOTS-1) of at least `bytes`, kept across calls.
 void *aux_scratch(gv_graph *g, int slot, size_t bytes);
+// Frees the analytics and auxiliary scratch (it is allocated again on demand).
+void release_analytics_scratch(gv_graph *g);
 // Device-to-host copy of the control block (synchronises the stream).
 gv_status read_ctl(gv_graph *g, Ctl *out, cudaStream_t s);
 
