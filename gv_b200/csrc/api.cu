@@ -175,6 +175,17 @@ void *analytics_scratch(gv_graph *g, size_t bytes) {
     return g->an_buf;
 }
 
+void release_analytics_scratch(gv_graph *g) {
+    if (g->an_buf) cudaFree(g->an_buf);
+    g->an_buf = nullptr;
+    g->an_bytes = 0;
+    for (int i = 0; i < gv_graph::AUX_SLOTS; ++i) {
+        if (g->aux[i]) cudaFree(g->aux[i]);
+        g->aux[i] = nullptr;
+        g->aux_bytes[i] = 0;
+    }
+}
+
 void *aux_scratch(gv_graph *g, int slot, size_t bytes) {
     if (bytes > g->aux_bytes[slot]) {
         if (g->aux[slot]) cudaFree(g->aux[slot]);
@@ -413,17 +424,6 @@ gv_status gv_view_create(gv_graph *g, gv_graph **out) {
     }
     *out = v;
     return GV_OK;
-}
-
-void release_analytics_scratch(gv_graph *g) {
-    if (g->an_buf) cudaFree(g->an_buf);
-    g->an_buf = nullptr;
-    g->an_bytes = 0;
-    for (int i = 0; i < gv_graph::AUX_SLOTS; ++i) {
-        if (g->aux[i]) cudaFree(g->aux[i]);
-        g->aux[i] = nullptr;
-        g->aux_bytes[i] = 0;
-    }
 }
 
 gv_status gv_destroy(gv_graph *g) {

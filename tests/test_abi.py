@@ -92,3 +92,16 @@ def test_mtx_header_parse_without_gpu():
     bad = b"%%MatrixMarket matrix coordinate real general\nnot a size line\n"
     buf = C.create_string_buffer(bad, len(bad))
     assert L.gv_mtx_parse(buf, len(bad), 0, C.byref(info), None, None, None, 0, C.byref(cnt), None) == _lib.GV_ERR_INVALID
+
+
+def test_library_leaves_none_of_its_own_symbols_undefined():
+    """Every gv:: function the library calls is defined in it (a missing one
+    would only show when the library is loaded with immediate binding)."""
+    import os
+    import subprocess
+    from gv_b200 import _lib
+    out = subprocess.run(["nm", "-D", "--undefined-only", str(_lib.LIB_PATH)], capture_output=True, text=True).stdout
+    own = [ln for ln in out.splitlines() if "_ZN2gv" in ln]
+    assert not own, own
+    C.CDLL(str(_lib.LIB_PATH), mode=os.RTLD_NOW)
+
