@@ -340,6 +340,39 @@ class GraphVine:
         _check(_lib.lib().gv_batch_run(self._h, arr, len(descs), ps, pd, mem, flags, _stream(stream)), "gv_batch_run")
         self._keep = (k1, k2, arr)
 
+    def batch_run_ppr(self, batches, sources, compact: bool = True, graph: bool = False, alpha: float = 0.85,
+                      epsilon: float = 1e-6, max_iter: int = 100, out=None, stream=None):
+        """A window of batches (as batch_run takes them), then k <= 32 PPR
+        queries on the resulting graph in the same unit of device work
+        (gv_batch_run_ppr); returns (x[n, k], sweeps).  out: a device tensor
+        when the batches are device tensors, else a host array."""
+        if isinstance(batches, tuple) and len(batches) == 3 and not isinstance(batches[0], tuple):
+            descs, src, dst = batches
+        else:
+            descs, srcs, dsts, off = [], [], [], 0
+            for ins_s, ins_d, del_s, del_d in batches:
+                descs.append((off, len(ins_s), len(del_s)))
+                srcs += [np.asarray(ins_s, np.uint32), np.asarray(del_s, np.uint32)]
+                dsts += [np.asarray(ins_d, np.uint32), np.asarray(del_d, np.uint32)]
+                off += len(ins_s) + len(del_s)
+            src = np.concatenate(srcs) if srcs else np.zeros(1, np.uint32)
+            dst = np.concatenate(dsts) if dsts else np.zeros(1, np.uint32)
+        sv = np.ascontiguousarray(sources, dtype=np.uint32)
+        k = len(sv)
+        arr = (_lib.gv_batch_desc * max(len(descs), 1))(*[_lib.gv_batch_desc(o, i, d) for o, i, d in descs])
+        ps, mem, k1 = _ptr(src, np.uint32)
+        pd, _, k2 = _ptr(dst, np.uint32)
+        x = np.empty((self.n, k), np.float32) if out is None else out
+        px, xmem, _ = _ptr(x, np.float32)
+        if xmem != mem:
+            raise ValueError("the result must live where the batches do (host or device)")
+        sw = C.c_int32()
+        flags = (_lib.GV_BATCH_COMPACT if compact else 0) | (_lib.GV_BATCH_GRAPH if graph else 0)
+        _check(_lib.lib().gv_batch_run_ppr(self._h, arr, len(descs), ps, pd, mem, flags, sv.ctypes.data, k, alpha,
+                                           epsilon, max_iter, px, C.byref(sw), _stream(stream)), "gv_batch_run_ppr")
+        self._keep = (k1, k2, arr)
+        return x, sw.value
+
     def ppr_batch(self, sources, alpha: float = 0.85, epsilon: float = 1e-6, max_iter: int = 100, out=None,
                   stream=None):
         """k <= 32 personalised PageRank queries at once; returns (x[n, k], sweeps)."""

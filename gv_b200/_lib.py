@@ -115,6 +115,8 @@ SIGNATURES = {
     "gv_last_error_string": (C.c_char_p, []),
     "gv_version": (C.c_char_p, []),
     "gv_batch_run": (C.c_int, [P, C.POINTER(gv_batch_desc), u32, P, P, C.c_int, u32, P]),
+    "gv_batch_run_ppr": (C.c_int, [P, C.POINTER(gv_batch_desc), u32, P, P, C.c_int, u32, P, u32, C.c_float,
+                                   C.c_float, C.c_int32, P, P, P]),
     "gv_ppr_batch": (C.c_int, [P, P, u32, f32, f32, i32, P, pi32, C.c_int, P]),
     "gv_autotune": (C.c_int, [C.POINTER(gv_config), P, P, u64, C.POINTER(gv_batch_desc), u32, P, P, C.c_int,
                               C.POINTER(gv_tune_result), pu32, C.POINTER(gv_config)]),

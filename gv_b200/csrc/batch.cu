@@ -296,11 +296,189 @@ __global__ void k_window_expand_dev(const uint32_t *__restrict__ src, const uint
     }
 }
 
+// ------------------------------------------------------- window queries
+// k <= 32 personalised PageRank queries answered on the graph a window
+// leaves, inside the window's graph: every size is read on the device, so
+// the sweeps can be captured with the window and replayed.  A warp serves a
+// vertex with lane j on query j (x and contributions vertex-major, x[v*k+j]);
+// vertices of more than WQ_LIGHT_BLOCKS blocks are cut into items of 32
+// blocks whose partials a finish kernel adds in item order.  The item count
+// is bounded by the pool (an item covers more than 8 blocks of one vertex,
+// so there are at most P/8), which sizes the buffers at capture time.
+constexpr uint32_t WQ_LIGHT_BLOCKS = 8;
+constexpr int WQ_THREADS = 256;
+constexpr unsigned WQ_GRID = 148 * 8;   // light CTAs; as many item CTAs, interleaved
+constexpr unsigned WQ_FIN = 148;
+
+struct WinQuery {
+    uint32_t k;
+    const uint32_t *sources;   // device, k
+    float alpha;
+    const float *gather;       // contributions, n * k
+    const float *xold;
+    float *xnew, *cnew;
+    double *partial;           // [WQ_GRID + WQ_FIN][32]
+    const int *state;          // [0] done, [1] sweeps
+    const uint32_t *first;     // [n + 1] first item of each vertex; first[n] = items
+    const uint32_t *ivert;     // item -> vertex
+    float *ipart;              // [items][32]
+    uint64_t icap;             // items the buffers hold
+};
+
+__global__ void k_wq_count(DevGraph g, uint32_t *__restrict__ first) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < g.n; v += gridDim.x * blockDim.x) {
+        const uint32_t nb = blocks_for(g.vtx[v].y, g.logB);
+        first[v] = nb > WQ_LIGHT_BLOCKS ? (nb + 31u) >> 5 : 0u;
+    }
+}
+
+__global__ void k_wq_fill(uint32_t n, const uint32_t *__restrict__ first, uint32_t *__restrict__ ivert, uint64_t icap) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+        for (uint32_t i = first[v]; i < first[v + 1] && i < icap; ++i) ivert[i] = v;
+}
+
+__global__ void k_wq_init(DevGraph g, const uint32_t *__restrict__ sources, uint32_t k, float *__restrict__ x,
+                          float *__restrict__ c) {
+    const size_t total = (size_t)g.n * k;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        const uint32_t v = (uint32_t)(i / k), j = (uint32_t)(i % k);
+        const float xv = (sources[j] == v) ? 1.f : 0.f;
+        x[i] = xv;
+        const uint32_t d = g.vtx[v].z;
+        c[i] = d ? xv / (float)d : 0.f;
+    }
+}
+
+__device__ __forceinline__ void wq_finish(const DevGraph &g, const WinQuery &a, uint32_t v, float acc, uint32_t lane,
+                                          double &res) {
+    if (lane >= a.k) return;
+    const float xv = ((a.sources[lane] == v) ? (1.0f - a.alpha) : 0.f) + a.alpha * acc;
+    const size_t at = (size_t)v * a.k + lane;
+    a.xnew[at] = xv;
+    const uint32_t d = g.vtx[v].z;
+    a.cnew[at] = d ? xv / (float)d : 0.f;
+    res += (double)fabsf(xv - a.xold[at]);
+}
+
+// adds the contributions of entries [e0, e1) of a vertex whose blocks from
+// kb0 on are held by the lanes (lane i: block kb0 + i)
+__device__ __forceinline__ float wq_entries(const DevGraph &g, const WinQuery &a, uint32_t my_blk, uint32_t kb0,
+                                            uint32_t e0, uint32_t e1, uint32_t lane) {
+    float acc = 0.f;
+    for (uint32_t q0 = e0; q0 < e1; q0 += 32) {
+        const uint32_t el = q0 - (kb0 << g.logB) + lane;
+        const uint32_t pb = __shfl_sync(GV_FULL_MASK, my_blk, (el >> g.logB) & 31u);
+        const uint32_t u = (q0 + lane < e1) ? g.pool[((size_t)pb << g.logB) + (el & (g.B - 1))] : GV_TOMB;
+        const uint32_t cnt = min(32u, e1 - q0);
+#pragma unroll 8
+        for (uint32_t j = 0; j < cnt; ++j) {
+            const uint32_t w = __shfl_sync(GV_FULL_MASK, u, j);
+            if (w != GV_TOMB && lane < a.k) acc += __ldg(a.gather + (size_t)w * a.k + lane);
+        }
+    }
+    return acc;
+}
+
+__device__ __forceinline__ uint32_t wq_block(const DevGraph &g, uint4 rec, uint32_t kb0, uint32_t nb, uint32_t lane) {
+    const uint32_t kk = kb0 + lane;
+    if (kk >= nb) return GV_NIL;
+    return kk == 0 ? rec.x : cbt_block(g.left, g.right, rec.x, kk);
+}
+
+// even CTAs: a warp per vertex of at most WQ_LIGHT_BLOCKS blocks (residual
+// slot blockIdx / 2); odd CTAs: the items of the larger vertices
+__global__ void __launch_bounds__(WQ_THREADS) k_wq_sweep(DevGraph g, WinQuery a) {
+    __shared__ double red[WQ_THREADS / 32][32];
+    if (a.state[0]) return;
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    const uint32_t vb = blockIdx.x >> 1, vg = gridDim.x >> 1;
+    const uint32_t nw = vg * (WQ_THREADS / 32);
+    if ((blockIdx.x & 1u) == 0) {
+        double res = 0.0;
+        for (uint32_t v = vb * (WQ_THREADS / 32) + warp; v < g.n; v += nw) {
+            const uint4 rec = g.vtx[v];
+            const uint32_t nb = blocks_for(rec.y, g.logB);
+            if (nb > WQ_LIGHT_BLOCKS) continue;
+            const float acc = wq_entries(g, a, wq_block(g, rec, 0, nb, lane), 0, 0, rec.y, lane);
+            wq_finish(g, a, v, acc, lane, res);
+        }
+        red[warp][lane] = res;
+        __syncthreads();
+        if (warp == 0) {
+            double t = 0.0;
+            for (int w = 0; w < WQ_THREADS / 32; ++w) t += red[w][lane];
+            a.partial[(size_t)vb * 32 + lane] = t;
+        }
+    } else {
+        const uint64_t items = min((uint64_t)a.first[g.n], a.icap);
+        for (uint64_t i = vb * (WQ_THREADS / 32) + warp; i < items; i += nw) {
+            const uint32_t v = a.ivert[i];
+            const uint4 rec = g.vtx[v];
+            const uint32_t nb = blocks_for(rec.y, g.logB);
+            const uint32_t kb0 = (uint32_t)(i - a.first[v]) << 5;
+            const uint32_t e0 = kb0 << g.logB, e1 = min(rec.y, (kb0 + 32) << g.logB);
+            const float acc = wq_entries(g, a, wq_block(g, rec, kb0, nb, lane), kb0, e0, e1, lane);
+            a.ipart[i * 32 + lane] = acc;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(WQ_THREADS) k_wq_fin(DevGraph g, WinQuery a) {
+    __shared__ double red[WQ_THREADS / 32][32];
+    if (a.state[0]) return;
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    const uint32_t nw = gridDim.x * (WQ_THREADS / 32);
+    double res = 0.0;
+    for (uint32_t v = blockIdx.x * (WQ_THREADS / 32) + warp; v < g.n; v += nw) {
+        const uint32_t i0 = a.first[v], i1 = a.first[v + 1];
+        if (i0 == i1) continue;
+        float acc = 0.f;
+        for (uint32_t i = i0; i < i1 && i < a.icap; ++i) acc += a.ipart[(size_t)i * 32 + lane];
+        wq_finish(g, a, v, acc, lane, res);
+    }
+    red[warp][lane] = res;
+    __syncthreads();
+    if (warp == 0) {
+        double t = 0.0;
+        for (int w = 0; w < WQ_THREADS / 32; ++w) t += red[w][lane];
+        a.partial[(size_t)(WQ_GRID + blockIdx.x) * 32 + lane] = t;
+    }
+}
+
+// per query, the sum of its residual slots in a fixed order; done when every query is
+__global__ void k_wq_done(const double *__restrict__ partial, uint32_t k, float eps, int *state) {
+    __shared__ int all_ok;
+    if (state[0]) return;
+    if (threadIdx.x == 0) all_ok = 1;
+    __syncthreads();
+    if (threadIdx.x < k) {
+        double t = 0.0;
+        for (uint32_t p = 0; p < WQ_GRID + WQ_FIN; ++p) t += partial[(size_t)p * 32 + threadIdx.x];
+        if (!(t < (double)eps)) atomicAnd(&all_ok, 0);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        state[1] += 1;
+        if (all_ok) state[0] = 1;
+    }
+}
+
+// the last iterate (sweep i, 1-based, wrote buffer i & 1) into the result
+__global__ void k_wq_select(const float *__restrict__ x0, const float *__restrict__ x1, const int *__restrict__ state,
+                            size_t total, float *__restrict__ out) {
+    const float *src = (state[1] & 1) ? x1 : x0;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x)
+        out[i] = src[i];
+}
+
 // A captured window graph and what it was captured against: it is replayed
 // while the buffers, the store arrays and the capacity are unchanged.
 struct WinGraph {
     uint64_t E = 0, nb_cap = 0;
     uint32_t flags = 0;
+    uint32_t qk = 0;            // queries captured with the window (0: none)
+    int32_t qiters = 0;
+    float qalpha = 0.f, qeps = 0.f;
     std::vector<const void *> ptrs;
     DevGraph d{};
     cudaGraphExec_t exec = nullptr;
@@ -318,6 +496,15 @@ struct WindowBufs {
     void *wctl = nullptr;
     std::vector<WinGraph> graphs;
     unsigned long long captures = 0, replays = 0, persistent = 0, exact = 0;  // window counts by path
+    // window queries: iterates, result, items, residuals (grown on demand)
+    uint64_t cap_q = 0, cap_items = 0;
+    float *qbuf = nullptr;      // x0 | x1 | c0 | c1 | result, n * k each
+    uint32_t *qfirst = nullptr; // n + 1
+    uint32_t *qivert = nullptr; // items
+    float *qipart = nullptr;    // items * 32
+    double *qpartial = nullptr; // (WQ_GRID + WQ_FIN) * 32
+    int *qstate = nullptr;      // 4
+    uint32_t *qsrc = nullptr;   // 32
     WinHeader *hdr() const { return (WinHeader *)wctl; }
     unsigned long long *queue() const { return (unsigned long long *)((char *)wctl + 16); }
     uint32_t *net_count() const { return (uint32_t *)((char *)wctl + 48); }
@@ -374,7 +561,8 @@ void release_window(gv_graph *g) {
             for (WinGraph &wg : b.graphs)
                 if (wg.exec) cudaGraphExecDestroy(wg.exec);
             for (void *p : {(void *)b.src, (void *)b.dst, (void *)b.vals, (void *)b.vals_alt, (void *)b.bstart,
-                            (void *)b.bsplit, (void *)b.tile_cnt, b.wctl})
+                            (void *)b.bsplit, (void *)b.tile_cnt, b.wctl, (void *)b.qbuf, (void *)b.qfirst,
+                            (void *)b.qivert, (void *)b.qipart, (void *)b.qpartial, (void *)b.qstate, (void *)b.qsrc})
                 if (p) cudaFree(p);
             if (b.cap_stream) cudaStreamDestroy(b.cap_stream);
             g_windows.erase(g_windows.begin() + i);
@@ -451,23 +639,96 @@ static void enqueue_window_persistent(gv_graph *g, WindowBufs &wb, uint64_t E, u
     if (flags & GV_BATCH_COMPACT) run_compact(g, s);
 }
 
+// Queries answered after a window (gv_batch_run_ppr).
+struct QuerySpec {
+    uint32_t k = 0;
+    const uint32_t *sources = nullptr;  // host, k
+    float alpha = 0.85f, eps = 1e-6f;
+    int32_t max_iter = 0;
+    float *x_out = nullptr;
+    int mem = GV_MEM_HOST;
+    int32_t *sweeps = nullptr;
+};
+
+static gv_status grow_queries(gv_graph *g, WindowBufs &wb, uint32_t k) {
+    const uint64_t n = g->d.n;
+    const uint64_t want_q = 5 * n * k, want_items = g->d.P / WQ_LIGHT_BLOCKS + 1;
+    gv_status st = GV_OK;
+    if (want_q > wb.cap_q || !wb.qbuf) {
+        if (wb.qbuf) cudaFree(wb.qbuf);
+        wb.qbuf = nullptr;
+        wb.cap_q = 0;
+        cudaError_t e = cudaMalloc(&wb.qbuf, want_q * 4);
+        if (e != cudaSuccess) return cuda_status(e, "window query iterates");
+        wb.cap_q = want_q;
+    }
+    if (!wb.qfirst) {
+        cudaError_t e = cudaMalloc(&wb.qfirst, (n + 1) * 4);
+        if (e == cudaSuccess) e = cudaMalloc(&wb.qivert, want_items * 4);
+        if (e == cudaSuccess) e = cudaMalloc(&wb.qipart, want_items * 32 * 4);
+        if (e == cudaSuccess) e = cudaMalloc(&wb.qpartial, (size_t)(WQ_GRID + WQ_FIN) * 32 * 8);
+        if (e == cudaSuccess) e = cudaMalloc(&wb.qstate, 16);
+        if (e == cudaSuccess) e = cudaMalloc(&wb.qsrc, 32 * 4);
+        if (e != cudaSuccess) return cuda_status(e, "window query scratch");
+        wb.cap_items = want_items;
+    }
+    return st;
+}
+
+// Enqueues the queries' sweeps (launch only, no host sync; max_iter sweeps
+// are launched and those after convergence exit at once), then the result
+// copy into the result block.
+static void enqueue_queries(gv_graph *g, WindowBufs &wb, uint32_t k, float alpha, float eps, int32_t max_iter,
+                            cudaStream_t s) {
+    const DevGraph d = g->d;
+    const uint32_t n = d.n;
+    const size_t nk = (size_t)n * k;
+    float *x[2] = {wb.qbuf, wb.qbuf + nk};
+    float *c[2] = {wb.qbuf + 2 * nk, wb.qbuf + 3 * nk};
+    float *xr = wb.qbuf + 4 * nk;
+    GV_LAUNCH(k_wq_count, grid_for(n, 256), 256, 0, s, d, wb.qfirst);
+    scan_exclusive_u32(wb.qfirst, wb.qfirst, n, wb.qfirst + n, g->bs.scan_tmp, s);
+    GV_LAUNCH(k_wq_fill, grid_for(n, 256), 256, 0, s, n, (const uint32_t *)wb.qfirst, wb.qivert, wb.cap_items);
+    cudaMemsetAsync(wb.qstate, 0, 16, s);
+    cudaMemsetAsync(wb.qpartial, 0, (size_t)(WQ_GRID + WQ_FIN) * 32 * 8, s);
+    GV_LAUNCH(k_wq_init, grid_for(nk, 256, 148 * 16), 256, 0, s, d, (const uint32_t *)wb.qsrc, k, x[0], c[0]);
+    int cur = 0;
+    for (int32_t it = 0; it < max_iter; ++it) {
+        WinQuery a{k, wb.qsrc, alpha, c[cur], x[cur], x[cur ^ 1], c[cur ^ 1], wb.qpartial, wb.qstate, wb.qfirst,
+                   wb.qivert, wb.qipart, wb.cap_items};
+        {
+            ProfScope ps(PROF_PULL, s);
+            GV_LAUNCH(k_wq_sweep, 2 * WQ_GRID, WQ_THREADS, 0, s, d, a);
+            GV_LAUNCH(k_wq_fin, WQ_FIN, WQ_THREADS, 0, s, d, a);
+        }
+        GV_LAUNCH(k_wq_done, 1, 32, 0, s, (const double *)wb.qpartial, k, eps, wb.qstate);
+        cur ^= 1;
+    }
+    GV_LAUNCH(k_wq_select, grid_for(nk, 256, 148 * 16), 256, 0, s, (const float *)x[0], (const float *)x[1],
+              (const int *)wb.qstate, nk, xr);
+}
+
 // The buffers a persistent-path graph captures.
 static std::vector<const void *> window_ptrs(gv_graph *g, WindowBufs &wb) {
     const BatchScratch &bs = g->bs;
     return {wb.src, wb.dst, wb.vals, wb.vals_alt, wb.bstart, wb.bsplit, wb.tile_cnt, wb.wctl, bs.keys, bs.keys_alt,
-            bs.rs_counts, bs.scan_tmp, bs.bdst, bs.found, bs.seg_vertex, bs.seg_start, bs.big_list};
+            bs.rs_counts, bs.scan_tmp, bs.bdst, bs.found, bs.seg_vertex, bs.seg_start, bs.big_list, wb.qbuf,
+            wb.qfirst, wb.qivert, wb.qipart, wb.qpartial, wb.qstate, wb.qsrc};
 }
 
 // Runs the persistent-path window of capacity E on stream s: replays the
 // graph captured for (E, batch capacity, flags) when the buffers and the
 // store are those it was captured with, else captures it first.
 static gv_status run_window_graph(gv_graph *g, WindowBufs &wb, uint64_t E, uint64_t nb_cap, uint32_t flags,
-                                  cudaStream_t s) {
+                                  const QuerySpec *q, cudaStream_t s) {
     const std::vector<const void *> ptrs = window_ptrs(g, wb);
+    const uint32_t qk = q ? q->k : 0;
+    const int32_t qit = q ? q->max_iter : 0;
+    const float qa = q ? q->alpha : 0.f, qe = q ? q->eps : 0.f;
     WinGraph *hit = nullptr;
     for (WinGraph &wg : wb.graphs)
-        if (wg.E == E && wg.nb_cap == nb_cap && wg.flags == flags && wg.ptrs == ptrs &&
-            std::memcmp(&wg.d, &g->d, sizeof(DevGraph)) == 0)
+        if (wg.E == E && wg.nb_cap == nb_cap && wg.flags == flags && wg.ptrs == ptrs && wg.qk == qk &&
+            wg.qiters == qit && wg.qalpha == qa && wg.qeps == qe && std::memcmp(&wg.d, &g->d, sizeof(DevGraph)) == 0)
             hit = &wg;
     if (!hit) {
         // graphs captured against buffers that have since moved are useless
@@ -488,6 +749,7 @@ static gv_status run_window_graph(gv_graph *g, WindowBufs &wb, uint64_t E, uint6
         cudaError_t e = cudaStreamBeginCapture(wb.cap_stream, cudaStreamCaptureModeThreadLocal);
         if (e == cudaSuccess) {
             enqueue_window_persistent(g, wb, E, flags, wb.cap_stream);
+            if (qk) enqueue_queries(g, wb, qk, qa, qe, qit, wb.cap_stream);
             e = cudaStreamEndCapture(wb.cap_stream, &graph);
         }
         WinGraph wg;
@@ -500,6 +762,10 @@ static gv_status run_window_graph(gv_graph *g, WindowBufs &wb, uint64_t E, uint6
         wg.E = E;
         wg.nb_cap = nb_cap;
         wg.flags = flags;
+        wg.qk = qk;
+        wg.qiters = qit;
+        wg.qalpha = qa;
+        wg.qeps = qe;
         wg.ptrs = ptrs;
         wg.d = g->d;
         wg.launches = g_launches.load() - l0;
@@ -525,19 +791,19 @@ static uint64_t pow2_at_least(uint64_t x, uint64_t lo) {
 
 using namespace gv;
 
-extern "C" gv_status gv_batch_run(gv_graph *g, const gv_batch_desc *descs, uint32_t nbatches, const uint32_t *src,
-                                  const uint32_t *dst, int mem, uint32_t flags, void *stream) {
+static gv_status batch_run_impl(gv_graph *g, const gv_batch_desc *descs, uint32_t nbatches, const uint32_t *src,
+                                const uint32_t *dst, int mem, uint32_t flags, void *stream, const QuerySpec *q) {
     if (!g || (nbatches && !descs)) { set_error("null argument"); return GV_ERR_INVALID; }
     if (g->parent) { set_error("a view is read-only"); return GV_ERR_STATE; }
     if (g->cfg.weighted) { set_error("gv_batch_run handles unweighted stores"); return GV_ERR_UNSUPPORTED; }
-    if (nbatches == 0) return GV_OK;
+    if (nbatches == 0 && !q) return GV_OK;
     uint64_t total = 0;
     for (uint32_t i = 0; i < nbatches; ++i) {
         if (descs[i].offset != total) { set_error("batches must be laid out consecutively"); return GV_ERR_INVALID; }
         total += (uint64_t)descs[i].n_insert + descs[i].n_delete;
     }
-    if (total == 0) return GV_OK;
-    if (!src || !dst) { set_error("null src/dst"); return GV_ERR_INVALID; }
+    if (total == 0 && !q) return GV_OK;
+    if (total && (!src || !dst)) { set_error("null src/dst"); return GV_ERR_INVALID; }
     if (total > 0x7FFFFFFFull) { set_error("window too large"); return GV_ERR_CAPACITY; }
     int prev = -1;
     cudaGetDevice(&prev);
@@ -565,6 +831,7 @@ extern "C" gv_status gv_batch_run(gv_graph *g, const gv_batch_desc *descs, uint3
         cudaError_t e = cudaMalloc(&wb.wctl, 64);
         if (e != cudaSuccess) st = cuda_status(e, "window control");
     }
+    if (st == GV_OK && q) st = grow_queries(g, wb, q->k);
     if (st == GV_OK && mem == GV_MEM_HOST) {
         const uint32_t n = g->d.n;
         for (uint64_t i = 0; i < total; ++i)
@@ -573,16 +840,18 @@ extern "C" gv_status gv_batch_run(gv_graph *g, const gv_batch_desc *descs, uint3
     Ctl cc{};
     if (st == GV_OK) {
         const cudaMemcpyKind k = mem == GV_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
-        cudaError_t e = cudaMemcpyAsync(wb.src, src, total * 4, k, s);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(wb.dst, dst, total * 4, k, s);
+        cudaError_t e = cudaSuccess;
+        if (total) e = cudaMemcpyAsync(wb.src, src, total * 4, k, s);
+        if (e == cudaSuccess && total) e = cudaMemcpyAsync(wb.dst, dst, total * 4, k, s);
+        if (e == cudaSuccess && q) e = cudaMemcpyAsync(wb.qsrc, q->sources, q->k * 4, cudaMemcpyHostToDevice, s);
         std::vector<unsigned long long> hs(nbatches), hp(nbatches);
         for (uint32_t i = 0; i < nbatches; ++i) {
             hs[i] = descs[i].offset;
             hp[i] = descs[i].offset + descs[i].n_insert;
         }
         WinHeader h{total, nbatches, 0};
-        if (e == cudaSuccess) e = cudaMemcpyAsync(wb.bstart, hs.data(), nbatches * 8, cudaMemcpyHostToDevice, s);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(wb.bsplit, hp.data(), nbatches * 8, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess && nbatches) e = cudaMemcpyAsync(wb.bstart, hs.data(), nbatches * 8, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess && nbatches) e = cudaMemcpyAsync(wb.bsplit, hp.data(), nbatches * 8, cudaMemcpyHostToDevice, s);
         if (e == cudaSuccess) e = cudaMemcpyAsync(wb.hdr(), &h, sizeof(h), cudaMemcpyHostToDevice, s);
         if (e == cudaSuccess) e = cudaMemcpyAsync(&cc, g->d.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s);
         // the host vectors and the header die here: wait for the copies before returning
@@ -597,19 +866,57 @@ extern "C" gv_status gv_batch_run(gv_graph *g, const gv_batch_desc *descs, uint3
         const uint64_t worst = (E + g->d.B - 1) / g->d.B + std::min<uint64_t>(E, g->d.n);
         if (worst <= cc.free_top) {
             ++wb.persistent;
-            if (flags & GV_BATCH_GRAPH) st = run_window_graph(g, wb, Ecap, nb_cap, flags, s);
+            if (flags & GV_BATCH_GRAPH) st = run_window_graph(g, wb, Ecap, nb_cap, flags, q, s);
             else {
                 enqueue_window_persistent(g, wb, Ecap, flags, s);
+                if (q) enqueue_queries(g, wb, q->k, q->alpha, q->eps, q->max_iter, s);
                 st = cuda_status(cudaGetLastError(), "window launch");
             }
         } else {
             ++wb.exact;
-            enqueue_window(g, wb, nbatches, wb.src, wb.dst, total, flags, s);
+            if (total) enqueue_window(g, wb, nbatches, wb.src, wb.dst, total, flags, s);
+            if (q) enqueue_queries(g, wb, q->k, q->alpha, q->eps, q->max_iter, s);
             st = cuda_status(cudaGetLastError(), "window launch");
         }
     }
+    if (st == GV_OK && q) {
+        // the answers: the result block to the caller, and the sweeps run
+        const size_t nk = (size_t)g->d.n * q->k;
+        int32_t hs[2] = {0, 0};
+        cudaError_t e = cudaMemcpyAsync(q->x_out, wb.qbuf + 4 * nk, nk * 4,
+                                        q->mem == GV_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(hs, wb.qstate, 8, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) st = cuda_status(e, "window queries");
+        else if (q->sweeps) *q->sweeps = hs[1];
+    }
     if (prev >= 0 && prev != g->cfg.device) cudaSetDevice(prev);
     return st;
+}
+
+extern "C" gv_status gv_batch_run(gv_graph *g, const gv_batch_desc *descs, uint32_t nbatches, const uint32_t *src,
+                                  const uint32_t *dst, int mem, uint32_t flags, void *stream) {
+    return batch_run_impl(g, descs, nbatches, src, dst, mem, flags, stream, nullptr);
+}
+
+extern "C" gv_status gv_batch_run_ppr(gv_graph *g, const gv_batch_desc *descs, uint32_t nbatches, const uint32_t *src,
+                                      const uint32_t *dst, int mem, uint32_t flags, const uint32_t *sources,
+                                      uint32_t k, float alpha, float epsilon, int32_t max_iter, float *x_out,
+                                      int32_t *sweeps, void *stream) {
+    if (!g || !sources || !x_out || k == 0 || k > 32 || max_iter < 0) { set_error("bad argument"); return GV_ERR_INVALID; }
+    if (g->cfg.directed) { set_error("window queries need an undirected (symmetric) store"); return GV_ERR_STATE; }
+    for (uint32_t j = 0; j < k; ++j)
+        if (sources[j] >= g->d.n) { set_error("source out of range"); return GV_ERR_INVALID; }
+    QuerySpec q;
+    q.k = k;
+    q.sources = sources;
+    q.alpha = alpha;
+    q.eps = epsilon;
+    q.max_iter = max_iter;
+    q.x_out = x_out;
+    q.mem = mem;
+    q.sweeps = sweeps;
+    return batch_run_impl(g, descs, nbatches, src, dst, mem, flags, stream, &q);
 }
 
 // Autotuner: for every candidate (edge-block size x threads per vertex)

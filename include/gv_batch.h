@@ -39,6 +39,22 @@ enum {
 gv_status gv_batch_run(gv_graph *g, const gv_batch_desc *descs, uint32_t nbatches, const uint32_t *src,
                        const uint32_t *dst, int mem, uint32_t flags, void *stream);
 
+/* A window of update batches, then k <= 32 personalised PageRank queries on
+ * the graph the window leaves, as one unit of device work: with
+ * GV_BATCH_GRAPH the window and the queries' sweeps are one CUDA graph,
+ * captured once per (capacity, k, max_iter, alpha, epsilon) and replayed
+ * for later windows (every size is read on the device).  max_iter sweeps
+ * are issued; once every query's L1 step is below epsilon the remaining ones
+ * return at once.  sources: host array of k ids.  x_out: n * k floats,
+ * vertex-major (x_out[v * k + j] is query j at v), in `mem` memory like
+ * src/dst; *sweeps gets the sweeps that ran.  nbatches may be 0 (queries
+ * only).  Synchronous.  No reference counterpart (the reference answers one
+ * query per host call). */
+gv_status gv_batch_run_ppr(gv_graph *g, const gv_batch_desc *descs, uint32_t nbatches, const uint32_t *src,
+                           const uint32_t *dst, int mem, uint32_t flags, const uint32_t *sources, uint32_t k,
+                           float alpha, float epsilon, int32_t max_iter, float *x_out, int32_t *sweeps,
+                           void *stream);
+
 /* k personalised PageRank queries (k <= 32) in one pass per sweep: every
  * adjacency read serves all k sources.  x_out[v * k + j] is query j's value
  * at v (vertex-major), sweeps stop when every query's L1 step < epsilon. */

@@ -173,6 +173,45 @@ def test_window_exact_path_when_the_pool_is_tight():
     assert_sound(g)
 
 
+@pytest.mark.parametrize("graph_mode", [True, False])
+def test_window_with_ppr_queries(graph_mode):
+    """gv_batch_run_ppr: windows of updates followed by PPR queries on the
+    graph they leave, as one unit (one replayed CUDA graph in graph mode);
+    each window's graph against the oracle, each query against the oracle's
+    PPR at the same sweep count; hubs large enough to be cut into items."""
+    n = 1 << 12
+    rng = np.random.default_rng(41)
+    s, d = rmat_graph(12, 8, seed=41)
+    others = np.setdiff1d(np.arange(n, dtype=np.uint32), [5])
+    hub = rng.permutation(others)[:2500]       # 79 blocks of 32: several items
+    s = np.concatenate([s, np.full(len(hub), 5, np.uint32)])
+    d = np.concatenate([d, hub])
+    g = make_graph(n, block_size=32, threads_per_vertex=8)
+    g.batch_insert(s, d)
+    o = oracle.OracleGraph(n)
+    o.insert(s, d)
+    for w in range(3):
+        off, dst, _ = o.export()
+        batches = _window(n, off, dst, rng, nb=4)
+        sources = np.concatenate([[5], rng.choice(n, 11, replace=False)]).astype(np.uint32)
+        x, sweeps = g.batch_run_ppr(batches, sources, compact=True, graph=graph_mode, max_iter=60)
+        for ins_s, ins_d, del_s, del_d in batches:
+            o.insert(ins_s, ins_d)
+            o.delete(del_s, del_d)
+        assert_same_adjacency(g, o)
+        assert 0 < sweeps <= 60
+        for j, src in enumerate(sources):
+            xo, _ = o.ppr(int(src), 0.85, 1e-6, 60, fixed_sweeps=sweeps)
+            assert np.abs(x[:, j].astype(np.float64) - xo).sum() < PR_L1, (w, j)
+    # queries alone (no batches)
+    x, sweeps = g.batch_run_ppr([], np.array([5, 17], np.uint32), graph=graph_mode, max_iter=60)
+    xo, _ = o.ppr(17, 0.85, 1e-6, 60, fixed_sweeps=sweeps)
+    assert np.abs(x[:, 1].astype(np.float64) - xo).sum() < PR_L1
+    if graph_mode:
+        assert g.last_stat("window_replays") >= 2
+    g.close()
+
+
 def test_window_rejects_bad_ids_whole():
     import torch
     n = 512
