@@ -429,11 +429,14 @@ __global__ void __launch_bounds__(WQ_THREADS) k_wq_fin(DevGraph g, WinQuery a) {
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     const uint32_t nw = gridDim.x * (WQ_THREADS / 32);
     double res = 0.0;
-    for (uint32_t v = blockIdx.x * (WQ_THREADS / 32) + warp; v < g.n; v += nw) {
+    // the warp on a vertex's first item adds that vertex's items in order
+    const uint64_t items = min((uint64_t)a.first[g.n], a.icap);
+    for (uint64_t i = blockIdx.x * (WQ_THREADS / 32) + warp; i < items; i += nw) {
+        const uint32_t v = a.ivert[i];
         const uint32_t i0 = a.first[v], i1 = a.first[v + 1];
-        if (i0 == i1) continue;
+        if (i != i0) continue;
         float acc = 0.f;
-        for (uint32_t i = i0; i < i1 && i < a.icap; ++i) acc += a.ipart[(size_t)i * 32 + lane];
+        for (uint32_t t = i0; t < i1 && t < a.icap; ++t) acc += a.ipart[(size_t)t * 32 + lane];
         wq_finish(g, a, v, acc, lane, res);
     }
     red[warp][lane] = res;
