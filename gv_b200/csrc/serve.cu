@@ -55,11 +55,15 @@ struct Server {
 
     double now() const { return std::chrono::duration<double>(clk::now() - t0).count(); }
 
+    uint64_t live_edges = 0;  // stored entries when the queries were grouped
+
     uint64_t estimate(uint32_t kind, uint32_t k) const {
         const uint64_t n = g->d.n;
         switch (kind) {
             case GV_REQ_PPR: return 20ull * n * k + 16ull * n;  // 4 iterate blocks + the result block
-            case GV_REQ_TC: return 64ull * n + 8ull * g->d.P * g->d.B / 2;
+            // the whole-graph path: an oriented snapshot (two words per stored
+            // entry), per-vertex arrays and the dense core's rows
+            case GV_REQ_TC: return 64ull * n + 8ull * live_edges + (1ull << 30);
             default: return 512ull * n + 8ull * 32 * n + 48ull * n + 12ull * n * k;  // BC: sigma rows, 32 level masks, lists, scores
         }
     }
@@ -350,6 +354,11 @@ extern "C" gv_status gv_serve_trace(gv_graph *g, const gv_serve_config *cfg, con
             auto rank = [](uint32_t k) { return k == GV_REQ_BC ? 2 : k == GV_REQ_PPR ? 1 : 0; };
             return rank(x.kind) < rank(y.kind);
         });
+        if (!tc.reqs.empty() || std::any_of(jobs.begin(), jobs.end(), [](const Job &j) { return j.kind == GV_REQ_TC; })) {
+            Ctl cc{};
+            if (read_ctl(g, &cc, us) == GV_OK) S.live_edges = cc.live_edges;
+            else S.live_edges = g->d.P * (uint64_t)g->d.B;  // fall back to the pool's capacity
+        }
         for (Job &jb : jobs) {
             jb.epoch = epoch;
             jb.group = ++group;
