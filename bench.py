@@ -1173,6 +1173,8 @@ def run_gv(args, rank, world, local_rank):
         parity, cpu = cpu_legs(args, n, seed, batches, srcs, par_gpu)
         if parity is not None:
             line["parity"] = {"plain_step_graph": parity}
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
     # one place for every parity result of the run
     par = line.setdefault("parity", {})
     if "batching" in line:
@@ -1184,8 +1186,6 @@ def run_gv(args, rank, world, local_rank):
                            "tolerance": 1e-4}
     if "serving" in line and line["serving"].get("parity"):
         par["serving_sample"] = line["serving"]["parity"]
-        if cpu is not None:
-            line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)
 
 
