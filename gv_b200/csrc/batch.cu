@@ -301,11 +301,12 @@ __global__ void k_window_expand_dev(const uint32_t *__restrict__ src, const uint
 // leaves, inside the window's graph: every size is read on the device, so
 // the sweeps can be captured with the window and replayed.  A warp serves a
 // vertex with lane j on query j (x and contributions vertex-major, x[v*k+j]);
-// vertices of more than WQ_LIGHT_BLOCKS blocks are cut into items of 32
-// blocks whose partials a finish kernel adds in item order.  The item count
-// is bounded by the pool (an item covers more than 8 blocks of one vertex,
-// so there are at most P/8), which sizes the buffers at capture time.
-constexpr uint32_t WQ_LIGHT_BLOCKS = 8;
+// vertices of more than WQ_LIGHT_FILL entries are cut into items of 32
+// blocks whose partials a finish kernel adds in item order (the split of
+// gv_ppr_batch).  The item count is bounded by the pool: at most one item
+// per 32 used blocks plus one per vertex of more than WQ_LIGHT_FILL entries,
+// which sizes the buffers at capture time.
+constexpr uint32_t WQ_LIGHT_FILL = 256;
 constexpr int WQ_THREADS = 256;
 constexpr unsigned WQ_GRID = 148 * 8;   // light CTAs; as many item CTAs, interleaved
 constexpr unsigned WQ_FIN = 148;
@@ -327,8 +328,8 @@ struct WinQuery {
 
 __global__ void k_wq_count(DevGraph g, uint32_t *__restrict__ first) {
     for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < g.n; v += gridDim.x * blockDim.x) {
-        const uint32_t nb = blocks_for(g.vtx[v].y, g.logB);
-        first[v] = nb > WQ_LIGHT_BLOCKS ? (nb + 31u) >> 5 : 0u;
+        const uint32_t fill = g.vtx[v].y;
+        first[v] = fill > WQ_LIGHT_FILL ? (blocks_for(fill, g.logB) + 31u) >> 5 : 0u;
     }
 }
 
@@ -385,7 +386,7 @@ __device__ __forceinline__ uint32_t wq_block(const DevGraph &g, uint4 rec, uint3
     return kk == 0 ? rec.x : cbt_block(g.left, g.right, rec.x, kk);
 }
 
-// even CTAs: a warp per vertex of at most WQ_LIGHT_BLOCKS blocks (residual
+// even CTAs: a warp per vertex of at most WQ_LIGHT_FILL entries (residual
 // slot blockIdx / 2); odd CTAs: the items of the larger vertices
 __global__ void __launch_bounds__(WQ_THREADS) k_wq_sweep(DevGraph g, WinQuery a) {
     __shared__ double red[WQ_THREADS / 32][32];
@@ -397,8 +398,8 @@ __global__ void __launch_bounds__(WQ_THREADS) k_wq_sweep(DevGraph g, WinQuery a)
         double res = 0.0;
         for (uint32_t v = vb * (WQ_THREADS / 32) + warp; v < g.n; v += nw) {
             const uint4 rec = g.vtx[v];
+            if (rec.y > WQ_LIGHT_FILL) continue;
             const uint32_t nb = blocks_for(rec.y, g.logB);
-            if (nb > WQ_LIGHT_BLOCKS) continue;
             const float acc = wq_entries(g, a, wq_block(g, rec, 0, nb, lane), 0, 0, rec.y, lane);
             wq_finish(g, a, v, acc, lane, res);
         }
@@ -500,7 +501,7 @@ struct WindowBufs {
     std::vector<WinGraph> graphs;
     unsigned long long captures = 0, replays = 0, persistent = 0, exact = 0;  // window counts by path
     // window queries: iterates, result, items, residuals (grown on demand)
-    uint64_t cap_q = 0, cap_items = 0;
+    uint64_t cap_q = 0, cap_items = 0, cap_qn = 0;
     float *qbuf = nullptr;      // x0 | x1 | c0 | c1 | result, n * k each
     uint32_t *qfirst = nullptr; // n + 1
     uint32_t *qivert = nullptr; // items
@@ -655,7 +656,8 @@ struct QuerySpec {
 
 static gv_status grow_queries(gv_graph *g, WindowBufs &wb, uint32_t k) {
     const uint64_t n = g->d.n;
-    const uint64_t want_q = 5 * n * k, want_items = g->d.P / WQ_LIGHT_BLOCKS + 1;
+    const uint64_t heavy_max = std::min<uint64_t>(n, g->d.P * (uint64_t)g->d.B / (WQ_LIGHT_FILL + 1));
+    const uint64_t want_q = 5 * n * k, want_items = g->d.P / 32 + heavy_max + 1;
     gv_status st = GV_OK;
     if (want_q > wb.cap_q || !wb.qbuf) {
         if (wb.qbuf) cudaFree(wb.qbuf);
@@ -665,7 +667,15 @@ static gv_status grow_queries(gv_graph *g, WindowBufs &wb, uint32_t k) {
         if (e != cudaSuccess) return cuda_status(e, "window query iterates");
         wb.cap_q = want_q;
     }
-    if (!wb.qfirst) {
+    if (!wb.qfirst || wb.cap_items < want_items || wb.cap_qn < n) {
+        for (void *p : {(void *)wb.qfirst, (void *)wb.qivert, (void *)wb.qipart, (void *)wb.qpartial,
+                        (void *)wb.qstate, (void *)wb.qsrc})
+            if (p) cudaFree(p);
+        wb.qfirst = wb.qivert = wb.qsrc = nullptr;
+        wb.qipart = nullptr;
+        wb.qpartial = nullptr;
+        wb.qstate = nullptr;
+        wb.cap_items = wb.cap_qn = 0;
         cudaError_t e = cudaMalloc(&wb.qfirst, (n + 1) * 4);
         if (e == cudaSuccess) e = cudaMalloc(&wb.qivert, want_items * 4);
         if (e == cudaSuccess) e = cudaMalloc(&wb.qipart, want_items * 32 * 4);
@@ -674,6 +684,7 @@ static gv_status grow_queries(gv_graph *g, WindowBufs &wb, uint32_t k) {
         if (e == cudaSuccess) e = cudaMalloc(&wb.qsrc, 32 * 4);
         if (e != cudaSuccess) return cuda_status(e, "window query scratch");
         wb.cap_items = want_items;
+        wb.cap_qn = n;
     }
     return st;
 }
