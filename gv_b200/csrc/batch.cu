@@ -338,15 +338,28 @@ __global__ void k_wq_fill(uint32_t n, const uint32_t *__restrict__ first, uint32
         for (uint32_t i = first[v]; i < first[v + 1] && i < icap; ++i) ivert[i] = v;
 }
 
-__global__ void k_wq_init(DevGraph g, const uint32_t *__restrict__ sources, uint32_t k, float *__restrict__ x,
-                          float *__restrict__ c) {
+// x0 = e_source per query and its contributions; a vertex with no slots
+// takes its final value (1 - alpha at its own query's source, else 0) in both
+// iterate buffers here and is left out of the sweeps.
+__global__ void k_wq_init(DevGraph g, const uint32_t *__restrict__ sources, uint32_t k, float alpha,
+                          float *__restrict__ x, float *__restrict__ c, float *__restrict__ x_other,
+                          float *__restrict__ c_other) {
     const size_t total = (size_t)g.n * k;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
         const uint32_t v = (uint32_t)(i / k), j = (uint32_t)(i % k);
-        const float xv = (sources[j] == v) ? 1.f : 0.f;
+        const bool src = sources[j] == v;
+        const uint4 rec = g.vtx[v];
+        if (rec.y == 0) {
+            const float xv = src ? 1.0f - alpha : 0.f;
+            x[i] = xv;
+            x_other[i] = xv;
+            c[i] = 0.f;
+            c_other[i] = 0.f;
+            continue;
+        }
+        const float xv = src ? 1.f : 0.f;
         x[i] = xv;
-        const uint32_t d = g.vtx[v].z;
-        c[i] = d ? xv / (float)d : 0.f;
+        c[i] = rec.z ? xv / (float)rec.z : 0.f;
     }
 }
 
@@ -398,7 +411,7 @@ __global__ void __launch_bounds__(WQ_THREADS) k_wq_sweep(DevGraph g, WinQuery a)
         double res = 0.0;
         for (uint32_t v = vb * (WQ_THREADS / 32) + warp; v < g.n; v += nw) {
             const uint4 rec = g.vtx[v];
-            if (rec.y > WQ_LIGHT_FILL) continue;
+            if (rec.y == 0 || rec.y > WQ_LIGHT_FILL) continue;  // set once by k_wq_init / items
             const uint32_t nb = blocks_for(rec.y, g.logB);
             const float acc = wq_entries(g, a, wq_block(g, rec, 0, nb, lane), 0, 0, rec.y, lane);
             wq_finish(g, a, v, acc, lane, res);
@@ -705,7 +718,8 @@ static void enqueue_queries(gv_graph *g, WindowBufs &wb, uint32_t k, float alpha
     GV_LAUNCH(k_wq_fill, grid_for(n, 256), 256, 0, s, n, (const uint32_t *)wb.qfirst, wb.qivert, wb.cap_items);
     cudaMemsetAsync(wb.qstate, 0, 16, s);
     cudaMemsetAsync(wb.qpartial, 0, (size_t)(WQ_GRID + WQ_FIN) * 32 * 8, s);
-    GV_LAUNCH(k_wq_init, grid_for(nk, 256, 148 * 16), 256, 0, s, d, (const uint32_t *)wb.qsrc, k, x[0], c[0]);
+    GV_LAUNCH(k_wq_init, grid_for(nk, 256, 148 * 16), 256, 0, s, d, (const uint32_t *)wb.qsrc, k, alpha, x[0], c[0],
+              x[1], c[1]);
     int cur = 0;
     for (int32_t it = 0; it < max_iter; ++it) {
         WinQuery a{k, wb.qsrc, alpha, c[cur], x[cur], x[cur ^ 1], c[cur ^ 1], wb.qpartial, wb.qstate, wb.qfirst,
