@@ -69,6 +69,9 @@ def parse():
     ap.add_argument("--serve-scale", type=int, default=25)
     ap.add_argument("--serve-requests", type=int, default=120)
     ap.add_argument("--serve-slots", type=int, default=4)
+    ap.add_argument("--serve-ppr-batch", type=int, default=1,
+                    help="most PPR queries per served job (at scale 25 a batched sweep gathers from HBM what one "
+                         "query's sweep finds in L2, so single queries on parallel slots serve the trace faster)")
     ap.add_argument("--serve-load", type=float, default=0.7, help="Poisson rate as a fraction of served capacity")
     ap.add_argument("--serve-hbm", type=int, default=96, help="GB of HBM the serving loop may give queries")
     ap.add_argument("--serve-parity-prefix", type=int, default=40,
@@ -806,7 +809,7 @@ def run_serving(args, dev, hbm_peak):
     parity = None
     if prefix:
         g = build()
-        res_p, outs_p = g.serve(trace(np.zeros(prefix), prefix), slots=args.serve_slots, ppr_batch=32,
+        res_p, outs_p = g.serve(trace(np.zeros(prefix), prefix), slots=args.serve_slots, ppr_batch=args.serve_ppr_batch,
                                 pace=False, alpha=ALPHA, epsilon=EPS, max_iter=MAX_ITER,
                                 hbm_budget_bytes=args.serve_hbm << 30, outputs=True, fresh=False)
         g.close()
@@ -831,7 +834,7 @@ def run_serving(args, dev, hbm_peak):
 
     g = build()
     t0 = time.perf_counter()
-    res, _ = g.serve(trace(np.zeros(len(items))), slots=args.serve_slots, ppr_batch=32, pace=False,
+    res, _ = g.serve(trace(np.zeros(len(items))), slots=args.serve_slots, ppr_batch=args.serve_ppr_batch, pace=False,
                      alpha=ALPHA, epsilon=EPS, max_iter=MAX_ITER, hbm_budget_bytes=args.serve_hbm << 30)
     served_s = time.perf_counter() - t0
     g.close()
@@ -862,7 +865,7 @@ def run_serving(args, dev, hbm_peak):
     arr = np.cumsum(np.random.default_rng(seed + 1).exponential(1.0 / rate, len(items)))
     arr -= arr[0]
     g = build()
-    res, _ = g.serve(trace(arr), slots=args.serve_slots, ppr_batch=32, pace=True, alpha=ALPHA, epsilon=EPS,
+    res, _ = g.serve(trace(arr), slots=args.serve_slots, ppr_batch=args.serve_ppr_batch, pace=True, alpha=ALPHA, epsilon=EPS,
                      max_iter=MAX_ITER, hbm_budget_bytes=args.serve_hbm << 30)
     g.close()
     del s_dev, d_dev
@@ -886,6 +889,7 @@ def run_serving(args, dev, hbm_peak):
             "served_vs_plain": {"requests": plain_s / served_s,
                                 "updates_per_s": served["updates_per_s"] / plain["updates_per_s"],
                                 "ppr_gteps": served["ppr_gteps"] / plain["ppr_gteps"] if plain["ppr_gteps"] else None},
+            "ppr_batch": args.serve_ppr_batch,
             "paced": {"poisson_rate_per_s": rate, "load": args.serve_load, "slots": args.serve_slots,
                       "hbm_budget_gb": args.serve_hbm, "p50_ms": _pct(lat, 50), "p99_ms": _pct(lat, 99),
                       "throughput_requests_per_s": len(items) / span, "updates_per_s": upd_pairs / span,

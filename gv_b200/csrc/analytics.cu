@@ -2349,6 +2349,24 @@ __global__ void k_ppr_init(DevGraph g, const uint32_t *__restrict__ sources, uin
 
 gv_status ppr_batch_impl(gv_graph *g, const uint32_t *sources, uint32_t k, float alpha, float eps, int max_iter,
                          float *x_out, int32_t *sweeps, int mem, cudaStream_t s) {
+    if (plan_pagerank_enabled(g)) {  // the degree-ordered sweep plan (prplan.cu)
+        bool planned = false;
+        gv_status st = GV_OK;
+        if (k == 1) {  // one query: the single-vector sweeps
+            uint32_t src = GV_NIL;
+            if (mem != GV_MEM_DEVICE) src = sources[0];
+            else {
+                cudaError_t e = cudaMemcpyAsync(&src, sources, 4, cudaMemcpyDeviceToHost, s);
+                if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+                if (e != cudaSuccess) return cuda_status(e, "ppr batch source");
+            }
+            if (src < g->d.n)
+                st = plan_pagerank(g, alpha, eps, max_iter, nullptr, GV_MEM_HOST, src, x_out, sweeps, mem, s, &planned);
+        } else {
+            st = plan_ppr_batch(g, sources, mem, k, alpha, eps, max_iter, x_out, sweeps, mem, s, &planned);
+        }
+        if (st != GV_OK || planned) return st;
+    }
     DevGraph d = g->d;
     const uint32_t n = d.n;
     const size_t vec = (size_t)n * k * sizeof(float);

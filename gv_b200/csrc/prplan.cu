@@ -396,6 +396,257 @@ T *carve(char *&p, size_t count) {
     return r;
 }
 
+// ------------------------------------------------ batched PPR over the plan
+// k personalised queries (2 <= k <= 8) share every adjacency read of a
+// sweep.  Values are row-major in plan order with a power-of-two stride K >= k
+// (x[row * K + q]), so the k contributions of one neighbour are one aligned
+// load of at most 32 bytes (one sector).  A group of K lanes owns a row (lane q = query
+// q); 32 / K groups share a warp.  Rows of WARP_DEG or more entries take the
+// whole warp (groups interleave over the entries, then combine), hub rows are
+// cut into the single sweep's items.  Entries are summed in row order inside a
+// group and the groups combine in a fixed butterfly, so results repeat bit
+// for bit.  Same iteration as the store's batched sweep (one lane per query,
+// residual per query, every query under epsilon to stop).
+struct PlanBatch {
+    const uint32_t *off, *col, *irow, *ifirst;
+    const float *rdeg;
+    const float *gather;  // contributions [(n + 1) K], plan order
+    const float *xold;
+    float *xnew, *cnew;
+    float *ipart;         // [nitems][K]
+    double *partial;      // [CTA][32]
+    const int *state;
+    const uint32_t *srow; // [32]: query q's source row, GV_NIL past k
+    float alpha, src_val;
+    uint32_t k, rH, rW, rZ, n, nitems;
+    uint32_t split;       // CTAs per period: items | warp rows << 8 (the rest: group rows)
+};
+
+// Entries [e0, e1) by the whole warp: group g takes the entries at g K + t of
+// each run of 32 (U runs in flight); returns, in every lane, the sum for its
+// query over all the entries.
+template <int K>
+__device__ __forceinline__ float plk_warp_segment(const PlanBatch &a, uint32_t e0, uint32_t e1) {
+    constexpr int U = K >= 8 ? 1 : 8 / K;
+    const uint32_t lane = threadIdx.x & 31u, q = lane % K, grp = lane / K;
+    const bool live = q < a.k;
+    float acc = 0.f;
+    for (uint32_t b = e0; b < e1; b += 32 * U) {
+        uint32_t c[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const uint32_t e = b + 32 * u + lane;
+            c[u] = e < e1 ? __ldcs(a.col + e) : a.n;
+        }
+        float v[U][K];
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int t = 0; t < K; ++t) {
+                const uint32_t ct = __shfl_sync(GV_FULL_MASK, c[u], grp * K + t);
+                v[u][t] = (ct < a.n && live) ? __ldg(a.gather + (size_t)ct * K + q) : 0.f;
+            }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int t = 0; t < K; ++t) acc += v[u][t];
+    }
+#pragma unroll
+    for (int o = K; o < 32; o <<= 1) acc += __shfl_xor_sync(GV_FULL_MASK, acc, o);
+    return acc;
+}
+
+template <int K>
+__device__ __forceinline__ void plk_finish(const PlanBatch &a, uint32_t r, uint32_t q, uint32_t my_src, float acc,
+                                           double &res) {
+    const float b = my_src == r ? a.src_val : 0.f;
+    const float xv = b + a.alpha * acc;
+    const size_t at = (size_t)r * K + q;
+    a.xnew[at] = xv;
+    a.cnew[at] = xv * a.rdeg[r];
+    res += (double)fabsf(xv - a.xold[at]);
+}
+
+template <int K>
+__device__ __forceinline__ void plk_items(const PlanBatch &a, uint32_t vb, uint32_t vg) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t nw = vg * (PL_THREADS / 32);
+    for (uint32_t it = vb * (PL_THREADS / 32) + (threadIdx.x >> 5); it < a.nitems; it += nw) {
+        const uint32_t r = a.irow[it];
+        const uint32_t e0 = a.off[r] + (it - a.ifirst[r]) * ITEM_ENTRIES;
+        const uint32_t e1 = min(a.off[r + 1], e0 + ITEM_ENTRIES);
+        const float acc = plk_warp_segment<K>(a, e0, e1);
+        if (lane < K) a.ipart[(size_t)it * K + lane] = acc;
+    }
+}
+
+template <int K>
+__device__ __forceinline__ void plk_warp_rows(const PlanBatch &a, uint32_t my_src, uint32_t vb, uint32_t vg,
+                                              double &res) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t nw = vg * (PL_THREADS / 32);
+    for (uint32_t r = a.rH + vb * (PL_THREADS / 32) + (threadIdx.x >> 5); r < a.rW; r += nw) {
+        const float acc = plk_warp_segment<K>(a, a.off[r], a.off[r + 1]);
+        if (lane < a.k) plk_finish<K>(a, r, lane, my_src, acc, res);
+    }
+}
+
+// Rows [rW, rZ): a group of K lanes per row, 32 / K rows per warp; lane q
+// loads entry j + u K + q of its row, the group's lanes take turns as the
+// neighbour.
+template <int K>
+__device__ __forceinline__ void plk_group_rows(const PlanBatch &a, uint32_t my_src, uint32_t vb, uint32_t vg,
+                                               double &res) {
+    constexpr int U = K >= 8 ? 1 : 8 / K;
+    constexpr uint32_t G = 32 / K;
+    const uint32_t lane = threadIdx.x & 31u, q = lane % K, grp = lane / K;
+    const bool live = q < a.k;
+    const uint32_t nw = vg * (PL_THREADS / 32);
+    for (uint32_t rb = a.rW + (vb * (PL_THREADS / 32) + (threadIdx.x >> 5)) * G; rb < a.rZ; rb += nw * G) {
+        const uint32_t r = rb + grp;
+        const bool ok = r < a.rZ;
+        const uint32_t o = ok ? a.off[r] : 0u, len = ok ? a.off[r + 1] - o : 0u;
+        const uint32_t most = __reduce_max_sync(GV_FULL_MASK, len);
+        float acc = 0.f;
+        for (uint32_t j = 0; j < most; j += K * U) {
+            uint32_t c[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const uint32_t e = j + u * K + q;
+                c[u] = e < len ? __ldcs(a.col + o + e) : a.n;
+            }
+            float v[U][K];
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+#pragma unroll
+                for (int t = 0; t < K; ++t) {
+                    const uint32_t ct = __shfl_sync(GV_FULL_MASK, c[u], grp * K + t);
+                    v[u][t] = (ct < a.n && live) ? __ldg(a.gather + (size_t)ct * K + q) : 0.f;
+                }
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+#pragma unroll
+                for (int t = 0; t < K; ++t) acc += v[u][t];
+        }
+        if (ok && live) plk_finish<K>(a, r, q, my_src, acc, res);
+    }
+}
+
+// Per-query residual of a CTA into partial[slot][0, K): lanes of one query
+// are combined across warps, then across the groups of a warp (fixed orders).
+template <int K>
+__device__ __forceinline__ void plk_residual(double res, double *__restrict__ partial, uint32_t slot) {
+    __shared__ double red[PL_THREADS / 32][32];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    red[warp][lane] = res;
+    __syncthreads();
+    if (warp == 0) {
+        double t = 0.0;
+        for (int w = 0; w < PL_THREADS / 32; ++w) t += red[w][lane];
+#pragma unroll
+        for (int o = K; o < 32; o <<= 1) t += __shfl_xor_sync(GV_FULL_MASK, t, o);
+        if (lane < K) partial[(size_t)slot * 32 + lane] = t;
+    }
+}
+
+template <int K>
+__global__ void __launch_bounds__(PL_THREADS) k_plk_sweep(PlanBatch a) {
+    if (a.state[0]) return;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t my_src = a.srow[lane % K];
+    const uint32_t t0 = a.split & 0xFFu, t1 = (a.split >> 8) & 0xFFu, t2 = PL_PERIOD - t0 - t1;
+    const uint32_t r = blockIdx.x % PL_PERIOD, w = blockIdx.x / PL_PERIOD, waves = gridDim.x / PL_PERIOD;
+    double res = 0.0;
+    if (r < t0) plk_items<K>(a, w * t0 + r, waves * t0);
+    else if (r < t0 + t1) plk_warp_rows<K>(a, my_src, w * t1 + (r - t0), waves * t1, res);
+    else plk_group_rows<K>(a, my_src, w * t2 + (r - t0 - t1), waves * t2, res);
+    plk_residual<K>(res, a.partial, blockIdx.x);
+}
+
+// hub rows: a thread per (row, query), the row's item partials in item order
+template <int K>
+__global__ void __launch_bounds__(PL_THREADS) k_plk_hub_fin(PlanBatch a, uint32_t part_base) {
+    if (a.state[0]) return;
+    const uint32_t q = threadIdx.x % K;  // the stride is a multiple of K
+    const uint32_t my_src = a.srow[q];
+    double res = 0.0;
+    const uint32_t total = a.rH * K;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        const uint32_t r = i / K;
+        if (q >= a.k) continue;
+        float t = 0.f;
+        for (uint32_t it = a.ifirst[r]; it < a.ifirst[r + 1]; ++it) t += a.ipart[(size_t)it * K + q];
+        plk_finish<K>(a, r, q, my_src, t, res);
+    }
+    plk_residual<K>(res, a.partial, part_base + blockIdx.x);
+}
+
+// per query (a warp each): its residual slots summed lane-strided, then
+// across the lanes in a fixed order; converged when every query is
+__global__ void k_plk_done(const double *__restrict__ partial, uint32_t nparts, uint32_t k, float eps, int *state) {
+    __shared__ int all_ok;
+    if (state[0]) return;
+    if (threadIdx.x == 0) all_ok = 1;
+    __syncthreads();
+    const uint32_t q = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    if (q < k) {
+        double t = 0.0;
+        for (uint32_t p = lane; p < nparts; p += 32) t += partial[(size_t)p * 32 + q];
+        t = warp_sum(t);
+        if (lane == 0 && !(t < (double)eps)) atomicAnd(&all_ok, 0);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        state[1] += 1;
+        if (all_ok) state[0] = 1;
+    }
+}
+
+// source rows of the k queries; GV_NIL in the unused slots
+__global__ void k_plk_sources(const uint32_t *__restrict__ sources, uint32_t k, uint32_t n,
+                              const uint32_t *__restrict__ inv, uint32_t *__restrict__ srow) {
+    const uint32_t q = threadIdx.x;
+    if (q >= 32) return;
+    const uint32_t v = q < k ? sources[q] : GV_NIL;
+    srow[q] = v < n ? inv[v] : GV_NIL;  // a source out of range matches no row
+}
+
+// x0 = the source indicator per query and its contributions; isolated rows
+// [rz, n) take their final value in both iterate buffers; row n (the
+// sentinel) is zero.  Lanes past k are never read.
+template <int K>
+__global__ void k_plk_init(uint32_t n, const uint32_t *__restrict__ srow, const float *__restrict__ rdeg, uint32_t rz,
+                           float src_base, float *__restrict__ x, float *__restrict__ c, float *__restrict__ x_other,
+                           float *__restrict__ c_other) {
+    const size_t total = ((size_t)n + 1) * K;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        const uint32_t r = (uint32_t)(i / K), q = (uint32_t)(i % K);
+        const bool src = srow[q] == r;
+        if (r == n) {
+            x[i] = c[i] = x_other[i] = c_other[i] = 0.f;
+        } else if (r >= rz) {
+            const float v = src ? src_base : 0.f;
+            x[i] = x_other[i] = v;
+            c[i] = c_other[i] = 0.f;
+        } else {  // both buffers: lanes past k are read (and never used) by the vector loads
+            const float v = src ? 1.f : 0.f;
+            x[i] = x_other[i] = v;
+            c[i] = c_other[i] = v * rdeg[r];
+        }
+    }
+}
+
+// x_out[v][q] (stride k, vertex order) from the plan-order rows
+template <int K>
+__global__ void k_plk_out(uint32_t n, uint32_t k, const uint32_t *__restrict__ inv, const float *__restrict__ x,
+                          float *__restrict__ out) {
+    const size_t total = (size_t)n * k;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        const uint32_t v = (uint32_t)(i / k), q = (uint32_t)(i % k);
+        out[i] = x[(size_t)inv[v] * K + q];
+    }
+}
+
 }  // namespace
 
 bool plan_pagerank_enabled(gv_graph *g) {
@@ -404,10 +655,24 @@ bool plan_pagerank_enabled(gv_graph *g) {
     return !(env && env[0] == '0');
 }
 
-gv_status plan_pagerank(gv_graph *g, float alpha, float eps, int max_iter, const float *x_init, int init_mem,
-                        uint32_t source, float *x_out, int32_t *sweeps, int mem, cudaStream_t s,
-                        bool *planned) {
-    *planned = false;
+namespace {
+
+// The plan of the store's current adjacency (see the top of this file).
+struct Plan {
+    uint32_t *perm, *inv, *off, *ifirst, *col, *irow;
+    float *rdeg;
+    float *ipart;      // nitems x the caller's width
+    char *extra;       // the caller's bytes at the end of the plan scratch
+    uint32_t nitems, rH, rW, rG, rZ;
+    uint32_t hoff[4];  // row starts of rows rH, rW, rG, rZ
+};
+
+// Builds the plan into auxiliary slots 12-15 (plan arrays and extra_bytes,
+// padded columns, copy items, hub items with ipart_width floats each).
+// *ok is false, with nothing built, when the padded rows would not fit
+// uint32 row starts.
+gv_status plan_build(gv_graph *g, size_t extra_bytes, uint32_t ipart_width, cudaStream_t s, Plan &P, bool *ok) {
+    *ok = false;
     DevGraph d = g->d;
     const uint32_t n = d.n;
     Ctl cc;
@@ -417,27 +682,20 @@ gv_status plan_pagerank(gv_graph *g, float alpha, float eps, int max_iter, const
     const uint64_t padded_max = (d.P - cc.free_top) * (uint64_t)d.B + 3ull * n;
     if (padded_max >= 0xFFFFFFF0ull || n == 0) return GV_OK;  // uint32 row starts: the store sweep serves it
     const uint32_t ntiles = (n + PL_TILE - 1) / PL_TILE;
-    // scratch: plan arrays (aux slot 12), padded columns (13), copy items (14), hub items (15)
-    const size_t plan_bytes = (size_t)5 * 256 + ((size_t)NCLASS * ntiles + 1) * 4 + (size_t)n * 4 * 2 +
-                              ((size_t)n + 1) * 4 * 3 + ((size_t)n + 1) * 4 * 4 + (size_t)(NCLASS + 8) * 4 +
-                              ((size_t)n + 1) * 8 + (size_t)PL_GRID * 8 + PL_FIN * 8 + 64 + 16 * 256 +
-                              (size_t)n * 4;
+    // seven arrays, each carved to a 256-byte boundary, then the caller's bytes
+    const size_t plan_bytes = (size_t)8 * 256 + ((size_t)NCLASS * ntiles + 1) * 4 + (size_t)n * 4 * 2 +
+                              ((size_t)n + 1) * 4 * 3 + (size_t)(NCLASS + 8) * 4 + extra_bytes;
     char *p = (char *)aux_scratch(g, 12, plan_bytes);
     if (!p) return GV_ERR_NOMEM;
     uint32_t *cnt = carve<uint32_t>(p, (size_t)NCLASS * ntiles + 1);
-    uint32_t *perm = carve<uint32_t>(p, n);
-    uint32_t *inv = carve<uint32_t>(p, n);
-    uint32_t *off = carve<uint32_t>(p, (size_t)n + 1);
-    uint32_t *ifirst = carve<uint32_t>(p, (size_t)n + 1);
-    float *rdeg = carve<float>(p, (size_t)n + 1);
-    float *x0 = carve<float>(p, (size_t)n + 1);
-    float *x1 = carve<float>(p, (size_t)n + 1);
-    float *c0 = carve<float>(p, (size_t)n + 1);
-    float *c1 = carve<float>(p, (size_t)n + 1);
+    P.perm = carve<uint32_t>(p, n);
+    P.inv = carve<uint32_t>(p, n);
+    P.off = carve<uint32_t>(p, (size_t)n + 1);
+    P.ifirst = carve<uint32_t>(p, (size_t)n + 1);
+    P.rdeg = carve<float>(p, (size_t)n + 1);
     uint32_t *cls = carve<uint32_t>(p, NCLASS + 8);
-    double *partial = carve<double>(p, PL_GRID + PL_FIN);
-    int *state = carve<int>(p, 16);
-    float *xstage = carve<float>(p, n);  // a host start vector, vertex order
+    P.extra = p;
+    uint32_t *perm = P.perm, *inv = P.inv, *off = P.off, *ifirst = P.ifirst;
     // class order of the rows
     GV_LAUNCH(k_pl_count, std::min<uint32_t>(ntiles, 148 * 8), PL_THREADS, 0, s, d, ntiles, cnt);
     scan_exclusive_u32(cnt, cnt, (uint64_t)NCLASS * ntiles, cnt + (size_t)NCLASS * ntiles, g->bs.scan_tmp, s);
@@ -446,7 +704,7 @@ gv_status plan_pagerank(gv_graph *g, float alpha, float eps, int max_iter, const
     GV_LAUNCH(k_pl_class_starts, 1, 64, 0, s, (const uint32_t *)cnt, ntiles, cls);
     // row lengths, starts, inverse degrees, copy items of the multi-block rows
     uint32_t *ffirst = ifirst;  // free until the hub items are built
-    GV_LAUNCH(k_pl_rowlen, grid_for(n, 256), 256, 0, s, d, (const uint32_t *)perm, off, rdeg, ffirst);
+    GV_LAUNCH(k_pl_rowlen, grid_for(n, 256), 256, 0, s, d, (const uint32_t *)perm, off, P.rdeg, ffirst);
     scan_exclusive_u32(off, off, n, off + n, g->bs.scan_tmp, s);
     scan_exclusive_u32(ffirst, ffirst, n, ffirst + n, g->bs.scan_tmp, s);
     uint32_t hcls[NCLASS], total = 0, nfill = 0;
@@ -461,41 +719,74 @@ gv_status plan_pagerank(gv_graph *g, float alpha, float eps, int max_iter, const
         const uint32_t c = 32u - (uint32_t)__builtin_clz(deg);  // class of deg itself
         return hcls[NCLASS - c];                                  // start of class c - 1
     };
-    const uint32_t rH = first_row_below(HUB_DEG), rW = first_row_below(WARP_DEG), rG = first_row_below(GROUP_DEG);
-    const uint32_t rZ = hcls[NCLASS - 1];  // first isolated row (class 0 comes last)
+    P.rH = first_row_below(HUB_DEG);
+    P.rW = first_row_below(WARP_DEG);
+    P.rG = first_row_below(GROUP_DEG);
+    P.rZ = hcls[NCLASS - 1];  // first isolated row (class 0 comes last)
     // the padded, renumbered columns, straight from the store's blocks
-    uint32_t *col = (uint32_t *)aux_scratch(g, 13, ((size_t)total + 4) * 4 + 256);
+    P.col = (uint32_t *)aux_scratch(g, 13, ((size_t)total + 4) * 4 + 256);
     uint32_t *frow = (uint32_t *)aux_scratch(g, 14, ((size_t)nfill + 1) * 4 + 256);
-    if (!col || !frow) return GV_ERR_NOMEM;
+    if (!P.col || !frow) return GV_ERR_NOMEM;
     GV_LAUNCH(k_pl_fill_small, 148 * 16, PL_THREADS, 0, s, d, (const uint32_t *)perm, (const uint32_t *)inv,
-              (const uint32_t *)off, col);
+              (const uint32_t *)off, P.col);
     if (nfill) {
         GV_LAUNCH(k_pl_item_fill, grid_for(n, 256), 256, 0, s, (const uint32_t *)ffirst, n, frow);
         GV_LAUNCH(k_pl_fill_items, 148 * 16, PL_THREADS, 0, s, d, (const uint32_t *)perm, (const uint32_t *)inv,
-                  (const uint32_t *)off, (const uint32_t *)frow, (const uint32_t *)ffirst, nfill, col);
+                  (const uint32_t *)off, (const uint32_t *)frow, (const uint32_t *)ffirst, nfill, P.col);
     }
-    // hub items
-    uint32_t nitems = 0;
-    uint32_t *irow = nullptr;
-    float *ipart = nullptr;
-    if (rH) {
-        GV_LAUNCH(k_pl_item_count, grid_for(rH, 256), 256, 0, s, (const uint32_t *)off, rH, ifirst);
-        scan_exclusive_u32(ifirst, ifirst, rH, ifirst + rH, g->bs.scan_tmp, s);
-        cudaMemcpyAsync(&nitems, ifirst + rH, 4, cudaMemcpyDeviceToHost, s);
-        e = cudaStreamSynchronize(s);
-        if (e != cudaSuccess) return cuda_status(e, "plan items");
-        char *q = (char *)aux_scratch(g, 15, (size_t)nitems * 8 + 512);
+    // hub items, and the entry offsets of the tier boundaries
+    P.nitems = 0;
+    P.irow = nullptr;
+    P.ipart = nullptr;
+    if (P.rH) {
+        GV_LAUNCH(k_pl_item_count, grid_for(P.rH, 256), 256, 0, s, (const uint32_t *)off, P.rH, ifirst);
+        scan_exclusive_u32(ifirst, ifirst, P.rH, ifirst + P.rH, g->bs.scan_tmp, s);
+        cudaMemcpyAsync(&P.nitems, ifirst + P.rH, 4, cudaMemcpyDeviceToHost, s);
+    }
+    const uint32_t rows[4] = {P.rH, P.rW, P.rG, P.rZ};
+    for (int i = 0; i < 4; ++i) cudaMemcpyAsync(&P.hoff[i], off + rows[i], 4, cudaMemcpyDeviceToHost, s);
+    e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_status(e, "plan items");
+    if (P.rH) {
+        char *q = (char *)aux_scratch(g, 15, (size_t)P.nitems * 4 * (1 + ipart_width) + 512);
         if (!q) return GV_ERR_NOMEM;
-        irow = carve<uint32_t>(q, nitems);
-        ipart = carve<float>(q, nitems);
-        GV_LAUNCH(k_pl_item_fill, grid_for(rH, 256), 256, 0, s, (const uint32_t *)ifirst, rH, irow);
+        P.irow = carve<uint32_t>(q, P.nitems);
+        P.ipart = carve<float>(q, (size_t)P.nitems * ipart_width);
+        GV_LAUNCH(k_pl_item_fill, grid_for(P.rH, 256), 256, 0, s, (const uint32_t *)ifirst, P.rH, P.irow);
     }
+    *ok = true;
+    return GV_OK;
+}
+
+}  // namespace
+
+gv_status plan_pagerank(gv_graph *g, float alpha, float eps, int max_iter, const float *x_init, int init_mem,
+                        uint32_t source, float *x_out, int32_t *sweeps, int mem, cudaStream_t s,
+                        bool *planned) {
+    *planned = false;
+    const uint32_t n = g->d.n;
+    // the single sweep's vectors and residual slots follow the plan arrays
+    const size_t extra = ((size_t)n + 1) * 4 * 4 + 4 * 256 + (size_t)PL_GRID * 8 + PL_FIN * 8 + 256 + 64 + 256 +
+                         (size_t)n * 4 + 256;
+    Plan P{};
+    bool ok = false;
+    gv_status st = plan_build(g, extra, 1, s, P, &ok);
+    if (st != GV_OK || !ok) return st;
+    char *p = P.extra;
+    float *x0 = carve<float>(p, (size_t)n + 1);
+    float *x1 = carve<float>(p, (size_t)n + 1);
+    float *c0 = carve<float>(p, (size_t)n + 1);
+    float *c1 = carve<float>(p, (size_t)n + 1);
+    double *partial = carve<double>(p, PL_GRID + PL_FIN);
+    int *state = carve<int>(p, 16);
+    float *xstage = carve<float>(p, n);  // a host start vector, vertex order
+    const uint32_t *perm = P.perm, *inv = P.inv;
+    const uint32_t rH = P.rH, rW = P.rW, rG = P.rG, rZ = P.rZ;
+    cudaError_t e = cudaSuccess;
     // start vector
     uint32_t src_row = GV_NIL;
     if (source != GV_NIL) cudaMemcpyAsync(&src_row, inv + source, 4, cudaMemcpyDeviceToHost, s);
-    uint32_t hoff[4] = {0, 0, 0, 0};
-    const uint32_t rows[4] = {rH, rW, rG, rZ};
-    for (int i = 0; i < 4; ++i) cudaMemcpyAsync(&hoff[i], off + rows[i], 4, cudaMemcpyDeviceToHost, s);
+    const uint32_t *hoff = P.hoff;
     const float *xin = nullptr;
     if (x_init) {
         if (init_mem == GV_MEM_DEVICE) xin = x_init;
@@ -505,14 +796,14 @@ gv_status plan_pagerank(gv_graph *g, float alpha, float eps, int max_iter, const
             xin = xstage;
         }
     }
-    e = cudaStreamSynchronize(s);  // src_row, tier row starts
+    e = cudaStreamSynchronize(s);  // src_row
     if (e != cudaSuccess) return cuda_status(e, "plan source");
     const float fill = source == GV_NIL ? 1.0f / (float)n : 0.f;
     // x0 and its contributions in plan order; the isolated rows, which the
     // sweeps never reach, get their value in x1 too
     const float base = source == GV_NIL ? (1.0f - alpha) / (float)n : 0.f;
     GV_LAUNCH(k_pl_init, grid_for((uint64_t)n + 1, 256), 256, 0, s, n, (const uint32_t *)perm, xin, fill, src_row,
-              1.f, (const float *)rdeg, rZ, base, source == GV_NIL ? 0.f : 1.0f - alpha, x0, c0, x1, c1);
+              1.f, (const float *)P.rdeg, rZ, base, source == GV_NIL ? 0.f : 1.0f - alpha, x0, c0, x1, c1);
     cudaMemsetAsync(state, 0, 16, s);
     cudaMemsetAsync(partial, 0, (PL_GRID + PL_FIN) * 8, s);
     // tier work (entries + 16 per row) from the row starts read back above
@@ -523,14 +814,14 @@ gv_status plan_pagerank(gv_graph *g, float alpha, float eps, int max_iter, const
     cudaFuncSetAttribute(k_pl_sweep, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
     cudaGetLastError();
     PlanSweep a{};
-    a.off = off;
-    a.col = col;
-    a.irow = irow;
-    a.ifirst = ifirst;
-    a.rdeg = rdeg;
+    a.off = P.off;
+    a.col = P.col;
+    a.irow = P.irow;
+    a.ifirst = P.ifirst;
+    a.rdeg = P.rdeg;
     a.partial = partial;
     a.state = state;
-    a.ipart = ipart;
+    a.ipart = P.ipart;
     a.alpha = alpha;
     a.base = base;
     a.src_row = src_row;
@@ -540,7 +831,7 @@ gv_status plan_pagerank(gv_graph *g, float alpha, float eps, int max_iter, const
     a.rG = rG;
     a.rZ = rZ;
     a.n = n;
-    a.nitems = nitems;
+    a.nitems = P.nitems;
     a.split = plan_split(w);
     // CTAs of the sweep: rounds of PL_PERIOD; GV_PL_WAVES overrides the number of rounds
     // eight waves of 8 resident CTAs per SM: at R-MAT scale 22 a sweep takes
@@ -588,6 +879,130 @@ gv_status plan_pagerank(gv_graph *g, float alpha, float eps, int max_iter, const
     if (sweeps) *sweeps = h_state[1];
     *planned = true;
     return cuda_status(cudaGetLastError(), "plan pagerank");
+}
+
+namespace {
+
+template <int K>
+gv_status plan_ppr_batch_k(gv_graph *g, const Plan &P, const uint32_t *sources, int src_mem, uint32_t k, float alpha,
+                           float eps, int max_iter, float *x_out, int32_t *sweeps, int mem, cudaStream_t s) {
+    const uint32_t n = g->d.n;
+    const size_t vec = ((size_t)n + 1) * K * sizeof(float);
+    // many small CTA shares: the block scheduler evens out the tiers' tails
+    const unsigned waves_default = 148 * 64 / PL_PERIOD;
+    unsigned waves = waves_default;
+    if (const char *env = std::getenv("GV_PLK_WAVES")) {
+        const unsigned w = (unsigned)std::strtoul(env, nullptr, 10);
+        if (w >= 1 && w <= PL_WAVES_MAX) waves = w;
+    }
+    const unsigned grid = waves * PL_PERIOD;
+    const uint32_t nparts = grid + PL_FIN;
+    // iterates and contributions (4 vectors of n + 1 rows), residual slots,
+    // state, sources and their rows; a host result is staged in a free iterate
+    const size_t bytes = 4 * vec + (size_t)nparts * 32 * 8 + 3 * 256;
+    char *p = (char *)analytics_scratch(g, bytes + 4 * 256);
+    if (!p) return GV_ERR_NOMEM;
+    float *x0 = carve<float>(p, vec / 4), *x1 = carve<float>(p, vec / 4);
+    float *c0 = carve<float>(p, vec / 4), *c1 = carve<float>(p, vec / 4);
+    double *partial = carve<double>(p, (size_t)nparts * 32);
+    int *state = carve<int>(p, 16);
+    uint32_t *srow = carve<uint32_t>(p, 32);
+    uint32_t *dsrc = carve<uint32_t>(p, 32);
+    cudaError_t e = cudaMemcpyAsync(dsrc, sources, (size_t)k * 4,
+                                    src_mem == GV_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return cuda_status(e, "plan ppr sources");
+    GV_LAUNCH(k_plk_sources, 1, 32, 0, s, (const uint32_t *)dsrc, k, n, (const uint32_t *)P.inv, srow);
+    GV_LAUNCH(k_plk_init<K>, grid_for(((uint64_t)n + 1) * K, 256, 148 * 16), 256, 0, s, n, (const uint32_t *)srow,
+              (const float *)P.rdeg, P.rZ, 1.0f - alpha, x0, c0, x1, c1);
+    cudaMemsetAsync(state, 0, 16, s);
+    cudaMemsetAsync(partial, 0, (size_t)nparts * 32 * 8, s);
+    // tier work: entries, plus 16 per row of a warp and 16 per group of rows
+    constexpr uint32_t G = 32 / K;
+    const double w[4] = {(double)P.hoff[0], (double)(P.hoff[1] - P.hoff[0]) + 16.0 * (P.rW - P.rH),
+                         (double)(P.hoff[3] - P.hoff[1]) + 16.0 * ((P.rZ - P.rW + G - 1) / G), 0.0};
+    cudaFuncSetAttribute(k_plk_sweep<K>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+    cudaGetLastError();
+    PlanBatch a{};
+    a.off = P.off;
+    a.col = P.col;
+    a.irow = P.irow;
+    a.ifirst = P.ifirst;
+    a.rdeg = P.rdeg;
+    a.ipart = P.ipart;
+    a.partial = partial;
+    a.state = state;
+    a.srow = srow;
+    a.alpha = alpha;
+    a.src_val = 1.0f - alpha;
+    a.k = k;
+    a.rH = P.rH;
+    a.rW = P.rW;
+    a.rZ = P.rZ;
+    a.n = n;
+    a.nitems = P.nitems;
+    a.split = plan_split(w) & 0xFFFFu;  // items | warp rows; the group rows take the rest
+    float *xa = x0, *xb = x1, *ca = c0, *cb = c1;
+    int h_state[2] = {0, 0};
+    int launched = 0;
+    while (launched < max_iter) {
+        const int chunk = std::min(8, max_iter - launched);
+        for (int i = 0; i < chunk; ++i) {
+            a.gather = ca;
+            a.xold = xa;
+            a.xnew = xb;
+            a.cnew = cb;
+            {
+                ProfScope ps(PROF_PULL, s);
+                GV_LAUNCH(k_plk_sweep<K>, grid, PL_THREADS, 0, s, a);
+                if (P.rH) GV_LAUNCH(k_plk_hub_fin<K>, PL_FIN, PL_THREADS, 0, s, a, grid);
+            }
+            GV_LAUNCH(k_plk_done, 1, 32 * k, 0, s, (const double *)partial, nparts, k, eps, state);
+            std::swap(xa, xb);
+            std::swap(ca, cb);
+        }
+        launched += chunk;
+        e = cudaMemcpyAsync(h_state, state, 8, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return cuda_status(e, "plan ppr sweeps");
+        if (h_state[0]) break;
+    }
+    const float *res = (h_state[1] & 1) ? x1 : x0;
+    float *dst = mem == GV_MEM_DEVICE ? x_out : (h_state[1] & 1) ? x0 : x1;  // n k floats fit an iterate
+    GV_LAUNCH(k_plk_out<K>, grid_for((uint64_t)n * k, 256, 148 * 16), 256, 0, s, n, k, (const uint32_t *)P.inv, res,
+              dst);
+    if (mem != GV_MEM_DEVICE) e = cudaMemcpyAsync(x_out, dst, (size_t)n * k * 4, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_status(e, "plan ppr out");
+    g->last_sweeps = h_state[1];
+    if (sweeps) *sweeps = h_state[1];
+    return cuda_status(cudaGetLastError(), "plan ppr batch");
+}
+
+}  // namespace
+
+gv_status plan_ppr_batch(gv_graph *g, const uint32_t *sources, int src_mem, uint32_t k, float alpha, float eps,
+                         int max_iter, float *x_out, int32_t *sweeps, int mem, cudaStream_t s, bool *planned) {
+    *planned = false;
+    // Up to 8 queries: the k contributions of a neighbour fit one 32-byte
+    // sector.  Measured per sweep at R-MAT scale 25 (1.05 G entries): 7.4 ms
+    // for 2 queries, 14.6 for 4 and 25.2 for 8, against 31.3, 33.7 and 36.0
+    // for the store's batched sweep; at 16 queries both take 39 ms and at 32
+    // the store's sweep is ahead (42.8 against 58.6), so wider batches stay
+    // there.  Either way the gathers of a batch miss the L2 that one
+    // vector's contributions fit: per query a plan sweep costs about what a
+    // single query's sweep does (3.3 ms).
+    if (k < 2 || k > 8) return GV_OK;
+    const uint32_t K = k <= 2 ? 2 : k <= 4 ? 4 : 8;
+    Plan P{};
+    bool ok = false;
+    gv_status st = plan_build(g, 0, K, s, P, &ok);
+    if (st != GV_OK || !ok) return st;
+    *planned = true;
+    switch (K) {
+        case 2: return plan_ppr_batch_k<2>(g, P, sources, src_mem, k, alpha, eps, max_iter, x_out, sweeps, mem, s);
+        case 4: return plan_ppr_batch_k<4>(g, P, sources, src_mem, k, alpha, eps, max_iter, x_out, sweeps, mem, s);
+        default: return plan_ppr_batch_k<8>(g, P, sources, src_mem, k, alpha, eps, max_iter, x_out, sweeps, mem, s);
+    }
 }
 
 }  // namespace gv

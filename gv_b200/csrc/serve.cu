@@ -47,6 +47,17 @@ struct Server {
     std::condition_variable cv;
     std::vector<int> busy;        // per worker
     std::vector<Job> job;         // per worker
+    // Scratch a worker keeps between jobs: its view's analytics buffers and
+    // its result buffer stay allocated for the next job of the same kind, so
+    // a job does not end in cudaFree (which waits for the whole device, the
+    // other workers' jobs included).  held[w] charges it to the budget (the
+    // estimate of the job that left it); it is released when the worker
+    // takes a job of another kind, or when an admission needs the room.
+    std::vector<gv_graph *> views;
+    std::vector<int> held_kind;   // kind of the held scratch, -1: none
+    std::vector<uint64_t> held;
+    std::vector<int> release;     // the worker frees its scratch before its next job
+    uint64_t held_mem = 0;        // sum of held
     uint64_t inflight_mem = 0;
     uint32_t inflight = 0;
     bool stop = false;
@@ -185,22 +196,36 @@ struct Server {
         cudaStream_t s = nullptr;
         cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
         gv_status vs = gv_view_create(g, &view);
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            views[w] = view;
+        }
         DevBuf buf;
         for (;;) {
             Job jb;
+            bool drop = false, have = false;
             {
                 std::unique_lock<std::mutex> lk(mu);
-                cv.wait(lk, [&] { return stop || busy[w] == 1; });
-                if (busy[w] != 1 && stop) break;
-                jb = job[w];
+                cv.wait(lk, [&] { return stop || busy[w] == 1 || release[w] != 0; });
+                drop = release[w] != 0;
+                have = busy[w] == 1;
+                if (!have && !drop && stop) break;
+                if (have) jb = job[w];
             }
-            if (vs == GV_OK) {
-                run_job(view, s, buf, jb);
-                // The admission budget counts the scratch of the jobs in
-                // flight; a view keeping the scratch of its last job would
-                // hold memory the budget has handed to the next ones.
+            if (drop && view) {  // another kind's scratch, or the budget wants it back
                 release_analytics_scratch(view);
                 buf.release();
+            }
+            if (drop) {
+                {
+                    std::lock_guard<std::mutex> lk(mu);
+                    release[w] = 0;
+                }
+                cv.notify_all();
+            }
+            if (!have) continue;
+            if (vs == GV_OK) {
+                run_job(view, s, buf, jb);
             } else {
                 std::lock_guard<std::mutex> lk(mu);
                 if (first_error == GV_OK) first_error = vs;
@@ -210,11 +235,46 @@ struct Server {
                 busy[w] = 0;
                 inflight -= 1;
                 inflight_mem -= jb.mem;
+                held[w] = jb.mem;
+                held_kind[w] = (int)jb.kind;
+                held_mem += jb.mem;
             }
             cv.notify_all();
         }
         if (view) gv_destroy(view);
         if (s) cudaStreamDestroy(s);
+    }
+
+    // Under mu: the idle worker for job jb, or -1 to wait.  A worker holding
+    // scratch of jb's kind is preferred (it reuses it); a worker holding
+    // another kind's frees it before the job.  Admitted when the jobs in
+    // flight, the scratch held by the other workers and jb fit the budget,
+    // or when nothing else runs; short of room, idle workers holding scratch
+    // are woken to free it, and the job waits until they have.
+    int pick_worker(const Job &jb, uint32_t W) {
+        int best = -1;
+        for (uint32_t w = 0; w < W; ++w) {
+            if (release[w]) return -1;  // a release in progress: its memory is not back yet
+            if (busy[w]) continue;
+            if (best < 0 || (held_kind[w] == (int)jb.kind && held_kind[best] != (int)jb.kind)) best = (int)w;
+        }
+        if (best < 0) return -1;
+        auto fits = [&](int w) { return inflight_mem + held_mem - held[w] + jb.mem <= cfg.hbm_budget_bytes; };
+        if (fits(best)) return best;
+        bool asked = false;
+        for (uint32_t w = 0; w < W && !fits(best); ++w)
+            if (!busy[w] && (int)w != best && held[w]) {
+                held_mem -= held[w];
+                held[w] = 0;
+                held_kind[w] = -1;
+                release[w] = 1;
+                asked = true;
+            }
+        if (asked) {
+            cv.notify_all();
+            return -1;
+        }
+        return inflight == 0 ? best : -1;  // always admit into an otherwise idle device
     }
 };
 
@@ -264,6 +324,10 @@ extern "C" gv_status gv_serve_trace(gv_graph *g, const gv_serve_config *cfg, con
     const uint32_t W = cfg->slots;
     S.busy.assign(W, 0);
     S.job.assign(W, Job{});
+    S.views.assign(W, nullptr);
+    S.held_kind.assign(W, -1);
+    S.held.assign(W, 0);
+    S.release.assign(W, 0);
     cudaSetDevice(g->cfg.device);
     cudaStream_t us = nullptr;
     cudaStreamCreateWithFlags(&us, cudaStreamNonBlocking);
@@ -375,21 +439,16 @@ extern "C" gv_status gv_serve_trace(gv_graph *g, const gv_serve_config *cfg, con
                 short_jobs = false;
             }
             std::unique_lock<std::mutex> lk(S.mu);
-            S.cv.wait(lk, [&] {
-                if (S.inflight == 0) return true;  // always admit into an idle device
-                if (S.inflight_mem + jb.mem > cfg->hbm_budget_bytes) return false;
-                for (uint32_t w = 0; w < W; ++w)
-                    if (!S.busy[w]) return true;
-                return false;
-            });
-            for (uint32_t w = 0; w < W; ++w)
-                if (!S.busy[w]) {
-                    S.job[w] = jb;
-                    S.busy[w] = 1;
-                    S.inflight += 1;
-                    S.inflight_mem += jb.mem;
-                    break;
-                }
+            int w = -1;
+            S.cv.wait(lk, [&] { return (w = S.pick_worker(jb, W)) >= 0; });
+            if (S.held_kind[w] != (int)jb.kind && S.held_kind[w] >= 0) S.release[w] = 1;
+            S.held_mem -= S.held[w];
+            S.held[w] = 0;
+            S.held_kind[w] = -1;
+            S.job[w] = jb;
+            S.busy[w] = 1;
+            S.inflight += 1;
+            S.inflight_mem += jb.mem;
             lk.unlock();
             S.cv.notify_all();
         }

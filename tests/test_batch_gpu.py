@@ -12,6 +12,7 @@ gv_b200 = pytest.importorskip("gv_b200")
 pytestmark = pytest.mark.gpu
 
 PR_L1 = 1e-6
+HUB_PR_L1 = 1e-5  # fp32 floor of a graph with a 7000-entry hub row (see its test)
 
 
 def _window(n, off, dst, rng, nb=12):
@@ -244,6 +245,63 @@ def test_ppr_batch_matches_oracle_per_query():
     for j, src in enumerate(sources):
         xo, _ = o.ppr(int(src), 0.85, 1e-6, 100, fixed_sweeps=sweeps)
         assert np.abs(x[:, j] - xo).sum() < PR_L1, j
+
+
+@pytest.fixture(scope="module")
+def hub_graph13():
+    """R-MAT scale 13 plus a hub of 7000 entries (cut into several items),
+    isolated vertices, and tombstones left by a delete batch."""
+    n = 1 << 13
+    rng = np.random.default_rng(41)
+    s, d = rmat_graph(13, 8, seed=41)
+    hub_d = rng.choice(np.arange(1, n, dtype=np.uint32), 7000, replace=False).astype(np.uint32)
+    s = np.concatenate([s, np.zeros(7000, np.uint32)])
+    d = np.concatenate([d, hub_d])
+    o = oracle.OracleGraph(n)
+    o.insert(s, d)
+    off, dst, _ = o.export()
+    es, ed = sample_existing(off, dst, 2000, rng)
+    o.delete(es, ed)
+    return n, s, d, es, ed, o
+
+
+@pytest.mark.parametrize("k", [1, 2, 3, 8, 13, 16, 24, 32])
+@pytest.mark.parametrize("plan", ["1", "0"])
+def test_ppr_batch_plan_and_store_match_oracle(hub_graph13, k, plan, monkeypatch):
+    """Batched PPR over the sweep plan (default; strides 2 to 8, the
+    single-vector sweep for one query, the store's batched sweep above 8
+    queries) and over the store (GV_PR_PLAN=0):
+    sources that are the hub, leaves, isolated vertices and a repeated
+    source, per query against the oracle.  Twenty sweeps exactly (epsilon
+    0): with epsilon 1e-6 some queries on this graph reach the fp32 floor of
+    the residual and run to max_iter, where the iterate only drifts with
+    rounding.  The tolerance is the fp32 floor of this graph: the hub's value
+    (about 0.2) is a sum over 7000 entries, whose rounding alone gives an L1
+    of 1e-6 to 7e-6 against the fp64 oracle, whatever the summation order
+    (the store sweep shows 6.9e-6 on the query from vertex 191)."""
+    import torch
+    monkeypatch.setenv("GV_PR_PLAN", plan)
+    n, s, d, es, ed, o = hub_graph13
+    g = make_graph(n, threads_per_vertex=8)
+    g.batch_insert(s, d)
+    g.batch_delete(es, ed)  # tombstones stay: the plan maps them to its sentinel
+    deg = g.degrees()
+    assert deg[0] > 3 * 2048 and (deg == 0).any()
+    rng = np.random.default_rng(k)
+    pick = [0, int(np.nonzero(deg == 0)[0][0]), int(np.nonzero(deg == 1)[0][0])]
+    pick += list(rng.choice(n, 32, replace=False))
+    sources = np.array((pick[:k - 1] + [pick[0]])[:k] if k > 3 else pick[:k], np.uint32)
+    x, sweeps = g.ppr_batch(sources, 0.85, 0.0, 20)
+    assert sweeps == 20
+    for j, src in enumerate(sources):
+        xo, _ = o.ppr(int(src), 0.85, 0.0, 20, fixed_sweeps=20)
+        assert np.abs(x[:, j].astype(np.float64) - xo).sum() < HUB_PR_L1, (j, int(src))
+    # device sources and output: the same values
+    xd = torch.empty((n, k), dtype=torch.float32, device="cuda")
+    _, sweeps_d = g.ppr_batch(sources, 0.85, 0.0, 20, out=xd)
+    assert sweeps_d == sweeps
+    assert np.array_equal(xd.cpu().numpy(), x)
+    g.close()
 
 
 def test_autotune_returns_a_candidate():
