@@ -632,24 +632,53 @@ __device__ __forceinline__ void ms_bwd_light(const DevGraph &g, const MsBufs<NW>
                                              const typename MaskOf<NW>::type *__restrict__ mask,
                                              const typename MaskOf<NW>::type *__restrict__ deeper, uint32_t vb,
                                              uint32_t vg) {
+    using M = typename MaskOf<NW>::type;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t nl = b.cnt[0];
-    for (uint32_t i = vb * MS_WARPS + (threadIdx.x >> 5); i < nl; i += vg * MS_WARPS) {
-        const uint32_t v = b.light[i];
-        const typename MaskOf<NW>::type A = mask[v];
-        unsigned long long sig[NW];
-        ms_load_sig<NW>(b, v, A, sig);
+    const uint32_t stride = vg * MS_WARPS;
+    // A two-stage prefetch: while a vertex runs, the id of the vertex after
+    // next and the source mask and record of the next one are in flight, and
+    // the next one's sigma row is loaded before this one finishes, so a
+    // vertex starts with its header at hand.  (Rows read here belong to
+    // vertices of this level, which only their own warp writes.)
+    uint32_t i = vb * MS_WARPS + (threadIdx.x >> 5);
+    uint32_t v1 = i < nl ? b.light[i] : 0u;
+    uint32_t v2 = i + stride < nl ? b.light[i + stride] : 0u;
+    M A1 = i < nl ? mask[v1] : (M)0;
+    uint2 rec1 = make_uint2(0u, 0u);
+    if (i < nl) {
+        const uint4 r = g.vtx[v1];
+        rec1 = make_uint2(r.x, r.y);
+    }
+    unsigned long long sig1[NW];
+    ms_load_sig<NW>(b, v1, A1, sig1);
+    for (; i < nl; i += stride) {
+        const bool has2 = i + stride < nl;
+        const uint32_t v3 = i + 2 * stride < nl ? b.light[i + 2 * stride] : 0u;
+        const M A2 = has2 ? mask[v2] : (M)0;
+        uint2 rec2 = make_uint2(0u, 0u);
+        if (has2) {
+            const uint4 r = g.vtx[v2];
+            rec2 = make_uint2(r.x, r.y);
+        }
         double acc[NW];
 #pragma unroll
         for (int k = 0; k < NW; ++k) acc[k] = 0.0;
-        const uint4 rec = g.vtx[v];
-        const uint32_t fill = rec.y, nb = blocks_for(fill, g.logB);
-        const uint32_t blk = lane < nb ? ms_block(g, rec.x, lane) : GV_NIL;
+        const uint32_t fill = rec1.y, nb = blocks_for(fill, g.logB);
+        const uint32_t blk = lane < nb ? ms_block(g, rec1.x, lane) : GV_NIL;
         for (uint32_t k = 0; k < nb; ++k) {
             const uint32_t bk = __shfl_sync(GV_FULL_MASK, blk, k);
-            ms_bwd_block<NW>(g, b, deeper, bk, min(g.B, fill - (k << g.logB)), A, acc);
+            ms_bwd_block<NW>(g, b, deeper, bk, min(g.B, fill - (k << g.logB)), A1, acc);
         }
-        ms_finish<NW>(b, v, A, sig, acc);
+        unsigned long long sig2[NW];
+        ms_load_sig<NW>(b, v2, A2, sig2);
+        ms_finish<NW>(b, v1, A1, sig1, acc);
+        v1 = v2;
+        v2 = v3;
+        A1 = A2;
+        rec1 = rec2;
+#pragma unroll
+        for (int k = 0; k < NW; ++k) sig1[k] = sig2[k];
     }
 }
 
