@@ -286,30 +286,80 @@ __device__ __forceinline__ void pl_items(const PlanSweep &a, uint32_t vb, uint32
 }
 
 // rows of TPV lanes each over [r0, r1): quads strided by TPV, QF of them
-// (4 QF gathers) in flight per lane
+// (4 QF gathers) in flight per lane.  Rows of a group or a thread (TPV < 32)
+// are short, so a row's dependent loads (bounds, quads, gathers, finish)
+// would each wait in turn: the next row's bounds and first quads are loaded
+// while this row's gathers are in flight.  Sums are formed in the same order
+// either way.
 template <int TPV, int QF>
 __device__ __forceinline__ void pl_rows(const PlanSweep &a, uint32_t r0, uint32_t r1, uint32_t vb, uint32_t vg,
                                         double &res) {
     Group<TPV> G;
     constexpr uint32_t GPC = PL_THREADS / TPV;
     const uint32_t ng = vg * GPC;
-    for (uint32_t i = r0 + vb * GPC + threadIdx.x / TPV; i < r1; i += ng) {
-        const uint32_t o = a.off[i];
-        const uint32_t nq = (a.off[i + 1] - o) >> 2;
-        const uint4 *q = reinterpret_cast<const uint4 *>(a.col + o);
-        float sum = 0.f;
-        for (uint32_t j = G.gl; j < nq; j += QF * TPV) {
-            uint4 v[QF];
+    const uint4 sent = make_uint4(a.n, a.n, a.n, a.n);
+    uint32_t i = r0 + vb * GPC + threadIdx.x / TPV;
+    if constexpr (TPV == 32) {
+        for (; i < r1; i += ng) {
+            const uint32_t o = a.off[i];
+            const uint32_t nq = (a.off[i + 1] - o) >> 2;
+            const uint4 *q = reinterpret_cast<const uint4 *>(a.col + o);
+            float sum = 0.f;
+            for (uint32_t j = G.gl; j < nq; j += QF * TPV) {
+                uint4 v[QF];
 #pragma unroll
-            for (int t = 0; t < QF; ++t)
-                v[t] = (j + t * TPV < nq) ? __ldcs(q + j + t * TPV) : make_uint4(a.n, a.n, a.n, a.n);
-            float part = 0.f;
+                for (int t = 0; t < QF; ++t) v[t] = (j + t * TPV < nq) ? __ldcs(q + j + t * TPV) : sent;
+                float part = 0.f;
 #pragma unroll
-            for (int t = 0; t < QF; ++t) part += gather4(a.gather, v[t]);
-            sum += part;
+                for (int t = 0; t < QF; ++t) part += gather4(a.gather, v[t]);
+                sum += part;
+            }
+            sum = G.sum(sum);
+            if (G.gl == 0) pl_finish(a, i, sum, res);
         }
-        if (TPV > 1) sum = G.sum(sum);
-        if (G.gl == 0) pl_finish(a, i, sum, res);
+    } else {
+        uint32_t o = 0, nq = 0;
+        if (i < r1) {
+            o = a.off[i];
+            nq = (a.off[i + 1] - o) >> 2;
+        }
+        uint4 v[QF];
+#pragma unroll
+        for (int t = 0; t < QF; ++t)
+            v[t] = (G.gl + t * TPV < nq) ? __ldcs(reinterpret_cast<const uint4 *>(a.col + o) + G.gl + t * TPV) : sent;
+        while (i < r1) {
+            const uint32_t in = i + ng;
+            uint32_t on = 0, nqn = 0;
+            if (in < r1) {
+                on = a.off[in];
+                nqn = (a.off[in + 1] - on) >> 2;
+            }
+            float sum = 0.f;
+            {
+                float part = 0.f;
+#pragma unroll
+                for (int t = 0; t < QF; ++t) part += gather4(a.gather, v[t]);
+                sum += part;
+            }
+            const uint4 *q = reinterpret_cast<const uint4 *>(a.col + o);
+            for (uint32_t j = G.gl + QF * TPV; j < nq; j += QF * TPV) {
+                uint4 w[QF];
+#pragma unroll
+                for (int t = 0; t < QF; ++t) w[t] = (j + t * TPV < nq) ? __ldcs(q + j + t * TPV) : sent;
+                float part = 0.f;
+#pragma unroll
+                for (int t = 0; t < QF; ++t) part += gather4(a.gather, w[t]);
+                sum += part;
+            }
+            const uint4 *qn = reinterpret_cast<const uint4 *>(a.col + on);
+#pragma unroll
+            for (int t = 0; t < QF; ++t) v[t] = (G.gl + t * TPV < nqn) ? __ldcs(qn + G.gl + t * TPV) : sent;
+            if (TPV > 1) sum = G.sum(sum);
+            if (G.gl == 0) pl_finish(a, i, sum, res);
+            i = in;
+            o = on;
+            nq = nqn;
+        }
     }
 }
 

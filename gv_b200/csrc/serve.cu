@@ -4,11 +4,11 @@
 // run of arrived update requests becomes one coalesced window, applied once
 // every query of the current epoch has finished.  Arrived queries are
 // grouped (PPR queries into batched launches of up to ppr_batch, triangle
-// subsets into one shared count, BC requests in pairs that share their BFS
-// passes) and handed to worker
-// threads; each worker owns a read-only view of the graph and a stream, so
-// groups run concurrently on the device.  A group is admitted when a worker
-// is free and its scratch estimate fits the HBM budget.
+// subsets into one shared count per worker, BC requests in pairs that share
+// their BFS passes) and handed to worker threads; each worker owns a
+// read-only view of the graph and a stream, so groups of one kind run
+// concurrently on the device, the kinds taking turns.  A group is admitted
+// when a worker is free and its scratch estimate fits the HBM budget.
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -410,33 +410,55 @@ extern "C" gv_status gv_serve_trace(gv_graph *g, const gv_serve_config *cfg, con
         }
         if (!bc.reqs.empty()) jobs.push_back(bc);
         if (!ppr.reqs.empty()) jobs.push_back(ppr);
-        if (!tc.reqs.empty()) jobs.push_back(tc);
-        // shortest kinds first: PPR batches and the triangle count start
-        // before the BC passes, which would otherwise hold the slots and the
-        // HBM budget while they queue
+        // triangle subsets: one shared count per worker, the requests dealt
+        // round-robin, so every slot takes part in the kind's turn
+        const uint32_t ntc = std::min<uint32_t>((uint32_t)tc.reqs.size(), W);
+        for (uint32_t j = 0; j < ntc; ++j) {
+            Job part;
+            part.kind = GV_REQ_TC;
+            for (size_t r = j; r < tc.reqs.size(); r += ntc) part.reqs.push_back(tc.reqs[r]);
+            jobs.push_back(part);
+        }
+        // shortest kinds first: the triangle counts and PPR start before the
+        // BC passes, which would otherwise hold the slots and the HBM budget
+        // while they queue
         std::stable_sort(jobs.begin(), jobs.end(), [](const Job &x, const Job &y) {
             auto rank = [](uint32_t k) { return k == GV_REQ_BC ? 2 : k == GV_REQ_PPR ? 1 : 0; };
             return rank(x.kind) < rank(y.kind);
         });
-        if (!tc.reqs.empty() || std::any_of(jobs.begin(), jobs.end(), [](const Job &j) { return j.kind == GV_REQ_TC; })) {
+        if (ntc) {
             Ctl cc{};
             if (read_ctl(g, &cc, us) == GV_OK) S.live_edges = cc.live_edges;
             else S.live_edges = g->d.P * (uint64_t)g->d.B;  // fall back to the pool's capacity
         }
-        bool short_jobs = false;
-        for (Job &jb : jobs) {
+        for (size_t j = 0; j < jobs.size(); ++j) {
+            Job &jb = jobs[j];
             jb.epoch = epoch;
             jb.group = ++group;
             jb.mem = S.estimate(jb.kind, (uint32_t)jb.reqs.size());
-            if (jb.kind != GV_REQ_BC) short_jobs = true;
-            else if (short_jobs) {
-                // the BC passes start once the short jobs of this dispatch are
-                // done: run beside them, the passes slowed the triangle count
-                // and the PPR batch several times over (scale 25: 1.5 and 2.2 s
-                // against about 0.3 and 0.4 s), which held every result back
+            if (j && jobs[j - 1].kind != jb.kind) {
+                // Each kind takes its turn alone: beside one another the
+                // kinds ran several times slower (at scale 25 the triangle
+                // count and PPR took 1.3 to 2.2 s beside BC passes, against
+                // about 0.3 s each alone), which held every result back.
                 std::unique_lock<std::mutex> lk(S.mu);
                 S.cv.wait(lk, [&] { return S.inflight == 0; });
-                short_jobs = false;
+                // The device is idle: the workers free the previous kinds'
+                // scratch now, while their cudaFree waits for nothing (later,
+                // it would wait for the new kind's groups on the other workers).
+                for (uint32_t w = 0; w < W; ++w)
+                    if (S.held[w] && S.held_kind[w] != (int)jb.kind) {
+                        S.held_mem -= S.held[w];
+                        S.held[w] = 0;
+                        S.held_kind[w] = -1;
+                        S.release[w] = 1;
+                    }
+                S.cv.notify_all();
+                S.cv.wait(lk, [&] {
+                    for (uint32_t w = 0; w < W; ++w)
+                        if (S.release[w]) return false;
+                    return true;
+                });
             }
             std::unique_lock<std::mutex> lk(S.mu);
             int w = -1;

@@ -7,10 +7,13 @@
  * read-only view, admitted while a slot is free and the group's scratch
  * estimate fits the HBM budget.  Queries that arrive while others run are
  * admitted as slots free up (continuous batching): arrived PPR queries are
- * merged into batched launches, arrived triangle-subset queries share one
- * triangle count, arrived BC queries run in pairs whose sources share one
- * set of BFS passes (gv_bc_multi); the triangle count and the PPR batches are
- * dispatched before the BC passes (shortest kinds first).  Epochs: with fresh = 0 a query sees exactly the updates
+ * merged into batched launches of up to ppr_batch, arrived triangle-subset
+ * queries share one count per slot, arrived BC queries run in pairs whose
+ * sources share one set of BFS passes (gv_bc_multi).  The kinds of one
+ * dispatch take turns, shortest first (triangle counts, PPR, BC): a kind's
+ * groups start once the previous kind's have finished.  A worker keeps its
+ * scratch for its next group of the same kind, charged to the budget.
+ * Epochs: with fresh = 0 a query sees exactly the updates
  * that arrived before it; with fresh = 1 (the default) it sees at least
  * those, so queries that arrive behind an update wait for it and run
  * together after it.  results[i].epoch names the updates each query saw (the
