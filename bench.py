@@ -69,9 +69,7 @@ def parse():
     ap.add_argument("--serve-scale", type=int, default=25)
     ap.add_argument("--serve-requests", type=int, default=120)
     ap.add_argument("--serve-slots", type=int, default=4)
-    ap.add_argument("--serve-ppr-batch", type=int, default=1,
-                    help="most PPR queries per served job (at scale 25 a batched sweep gathers from HBM what one "
-                         "query's sweep finds in L2, so single queries on parallel slots serve the trace faster)")
+    ap.add_argument("--serve-ppr-batch", type=int, default=32, help="most PPR queries per served job")
     ap.add_argument("--serve-load", type=float, default=0.7, help="Poisson rate as a fraction of served capacity")
     ap.add_argument("--serve-hbm", type=int, default=96, help="GB of HBM the serving loop may give queries")
     ap.add_argument("--serve-parity-prefix", type=int, default=40,
@@ -450,6 +448,20 @@ def run_batching(args, dev, hbm_peak):
     e[3].record()
     torch.cuda.synchronize()
     pr_plain_ms, pr_batched_ms = e[0].elapsed_time(e[1]), e[2].elapsed_time(e[3])
+    # 8 queries: one at a time against one batched call over the sweep plan
+    x8 = torch.empty((n, 8), dtype=torch.float32, device=dev)
+    e[0].record()
+    for sq in srcs_q[:8]:
+        gp.ppr(int(sq), out=xq)
+    e[1].record()
+    e[2].record()
+    _, sw_8 = gb.ppr_batch(srcs_q[:8], out=x8)
+    e[3].record()
+    torch.cuda.synchronize()
+    pr8 = {"plain_ms": e[0].elapsed_time(e[1]), "batched_ms": e[2].elapsed_time(e[3]), "sweeps": sw_8,
+           "max_query_l1_vs_32_batch": float((x8.double() - xb[:, :8].double()).abs().sum(0).max())}
+    pr8["speedup"] = pr8["plain_ms"] / pr8["batched_ms"]
+    del x8
     gteps_plain = m_p * sw_plain / (pr_plain_ms / 1e3) / 1e9
     gteps_batched = m_b * sw_b * 32 / (pr_batched_ms / 1e3) / 1e9
     # PPR bytes: per single-query sweep 4m + 12n; per batched sweep of k
@@ -504,6 +516,7 @@ def run_batching(args, dev, hbm_peak):
             "capture_window_s": capture_s,
             "pagerank_gteps_plain": gteps_plain, "pagerank_gteps_batched": gteps_batched,
             "pagerank_speedup": pr_plain_ms / pr_batched_ms,
+            "pagerank_8_queries": pr8,
             "roofline": {
                 "unit": "GB/s", "peak": hbm_peak,
                 "updates_plain": {"algorithmic_bytes": alg_plain, "achieved": alg_plain / plain_ms / 1e6,

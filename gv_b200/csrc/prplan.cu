@@ -447,10 +447,10 @@ T *carve(char *&p, size_t count) {
 }
 
 // ------------------------------------------------ batched PPR over the plan
-// k personalised queries (2 <= k <= 8) share every adjacency read of a
+// k personalised queries (2 <= k <= 32) share every adjacency read of a
 // sweep.  Values are row-major in plan order with a power-of-two stride K >= k
 // (x[row * K + q]), so the k contributions of one neighbour are one aligned
-// load of at most 32 bytes (one sector).  A group of K lanes owns a row (lane q = query
+// load of at most 128 bytes.  A group of K lanes owns a row (lane q = query
 // q); 32 / K groups share a warp.  Rows of WARP_DEG or more entries take the
 // whole warp (groups interleave over the entries, then combine), hub rows are
 // cut into the single sweep's items.  Entries are summed in row order inside a
@@ -970,7 +970,10 @@ gv_status plan_ppr_batch_k(gv_graph *g, const Plan &P, const uint32_t *sources, 
     constexpr uint32_t G = 32 / K;
     const double w[4] = {(double)P.hoff[0], (double)(P.hoff[1] - P.hoff[0]) + 16.0 * (P.rW - P.rH),
                          (double)(P.hoff[3] - P.hoff[1]) + 16.0 * ((P.rZ - P.rW + G - 1) / G), 0.0};
-    cudaFuncSetAttribute(k_plk_sweep<K>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+    // most of the SM's on-chip memory to L1, but room for the residual
+    // tables (2 KB, plus 1 KB the system keeps per CTA) of 8 resident CTAs: a
+    // zero carveout held the SM to two CTAs (25% of its warps)
+    cudaFuncSetAttribute(k_plk_sweep<K>, cudaFuncAttributePreferredSharedMemoryCarveout, 12);
     cudaGetLastError();
     PlanBatch a{};
     a.off = P.off;
@@ -1033,16 +1036,12 @@ gv_status plan_ppr_batch_k(gv_graph *g, const Plan &P, const uint32_t *sources, 
 gv_status plan_ppr_batch(gv_graph *g, const uint32_t *sources, int src_mem, uint32_t k, float alpha, float eps,
                          int max_iter, float *x_out, int32_t *sweeps, int mem, cudaStream_t s, bool *planned) {
     *planned = false;
-    // Up to 8 queries: the k contributions of a neighbour fit one 32-byte
-    // sector.  Measured per sweep at R-MAT scale 25 (1.05 G entries): 7.4 ms
-    // for 2 queries, 14.6 for 4 and 25.2 for 8, against 31.3, 33.7 and 36.0
-    // for the store's batched sweep; at 16 queries both take 39 ms and at 32
-    // the store's sweep is ahead (42.8 against 58.6), so wider batches stay
-    // there.  Either way the gathers of a batch miss the L2 that one
-    // vector's contributions fit: per query a plan sweep costs about what a
-    // single query's sweep does (3.3 ms).
-    if (k < 2 || k > 8) return GV_OK;
-    const uint32_t K = k <= 2 ? 2 : k <= 4 ? 4 : 8;
+    // Per sweep at R-MAT scale 25 (1.05 G entries): 3.9 ms for 2 queries,
+    // 9.8 for 8, 17.8 for 16 and 32.3 for 32, against 32.0, 37.1, 39.6 and
+    // 43.8 for the store's batched sweep and 3.3 ms for one query's plan
+    // sweep; at scale 22, 0.45 to 3.5 ms against 4.4 to 5.6.
+    if (k < 2 || k > 32) return GV_OK;
+    const uint32_t K = k <= 2 ? 2 : k <= 4 ? 4 : k <= 8 ? 8 : k <= 16 ? 16 : 32;
     Plan P{};
     bool ok = false;
     gv_status st = plan_build(g, 0, K, s, P, &ok);
@@ -1051,7 +1050,9 @@ gv_status plan_ppr_batch(gv_graph *g, const uint32_t *sources, int src_mem, uint
     switch (K) {
         case 2: return plan_ppr_batch_k<2>(g, P, sources, src_mem, k, alpha, eps, max_iter, x_out, sweeps, mem, s);
         case 4: return plan_ppr_batch_k<4>(g, P, sources, src_mem, k, alpha, eps, max_iter, x_out, sweeps, mem, s);
-        default: return plan_ppr_batch_k<8>(g, P, sources, src_mem, k, alpha, eps, max_iter, x_out, sweeps, mem, s);
+        case 8: return plan_ppr_batch_k<8>(g, P, sources, src_mem, k, alpha, eps, max_iter, x_out, sweeps, mem, s);
+        case 16: return plan_ppr_batch_k<16>(g, P, sources, src_mem, k, alpha, eps, max_iter, x_out, sweeps, mem, s);
+        default: return plan_ppr_batch_k<32>(g, P, sources, src_mem, k, alpha, eps, max_iter, x_out, sweeps, mem, s);
     }
 }
 

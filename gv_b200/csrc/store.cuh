@@ -105,7 +105,7 @@ bool plan_pagerank_enabled(gv_graph *g);
 gv_status plan_pagerank(gv_graph *g, float alpha, float eps, int max_iter, const float *x_init, int init_mem,
                         uint32_t source, float *x_out, int32_t *sweeps, int mem, cudaStream_t s, bool *planned);
 // k personalised PageRank queries over the sweep plan (sources in src_mem
-// memory); *planned false when the plan does not take them (k outside 2..8,
+// memory); *planned false when the plan does not take them (k outside 2..32,
 // or a graph the plan cannot hold).
 gv_status plan_ppr_batch(gv_graph *g, const uint32_t *sources, int src_mem, uint32_t k, float alpha, float eps,
                          int max_iter, float *x_out, int32_t *sweeps, int mem, cudaStream_t s, bool *planned);

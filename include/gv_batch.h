@@ -58,9 +58,9 @@ gv_status gv_batch_run_ppr(gv_graph *g, const gv_batch_desc *descs, uint32_t nba
 /* k personalised PageRank queries (k <= 32) in one pass per sweep: every
  * adjacency read serves all k sources.  x_out[v * k + j] is query j's value
  * at v (vertex-major), sweeps stop when every query's L1 step < epsilon.
- * Undirected unweighted stores take the degree-ordered sweep plan for k <= 8
- * (one query: the single-vector sweep) and the store's batched sweep above;
- * GV_PR_PLAN=0 selects the store's sweep for every k. */
+ * Undirected unweighted stores take the degree-ordered sweep plan (one
+ * query: its single-vector sweep); GV_PR_PLAN=0, directed and weighted
+ * stores the store's batched sweep. */
 gv_status gv_ppr_batch(gv_graph *g, const uint32_t *sources, uint32_t k, float alpha, float epsilon,
                        int32_t max_iter, float *x_out, int32_t *sweeps, int mem, void *stream);
 

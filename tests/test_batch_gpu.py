@@ -268,9 +268,8 @@ def hub_graph13():
 @pytest.mark.parametrize("k", [1, 2, 3, 8, 13, 16, 24, 32])
 @pytest.mark.parametrize("plan", ["1", "0"])
 def test_ppr_batch_plan_and_store_match_oracle(hub_graph13, k, plan, monkeypatch):
-    """Batched PPR over the sweep plan (default; strides 2 to 8, the
-    single-vector sweep for one query, the store's batched sweep above 8
-    queries) and over the store (GV_PR_PLAN=0):
+    """Batched PPR over the sweep plan (default; strides 2 to 32, the
+    single-vector sweep for one query) and over the store (GV_PR_PLAN=0):
     sources that are the hub, leaves, isolated vertices and a repeated
     source, per query against the oracle.  Twenty sweeps exactly (epsilon
     0): with epsilon 1e-6 some queries on this graph reach the fp32 floor of
