@@ -600,7 +600,7 @@ __device__ __forceinline__ void plk_residual(double res, double *__restrict__ pa
 }
 
 template <int K>
-__global__ void __launch_bounds__(PL_THREADS) k_plk_sweep(PlanBatch a) {
+__device__ __forceinline__ void plk_sweep_body(const PlanBatch &a) {
     if (a.state[0]) return;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t my_src = a.srow[lane % K];
@@ -611,6 +611,21 @@ __global__ void __launch_bounds__(PL_THREADS) k_plk_sweep(PlanBatch a) {
     else if (r < t0 + t1) plk_warp_rows<K>(a, my_src, w * t1 + (r - t0), waves * t1, res);
     else plk_group_rows<K>(a, my_src, w * t2 + (r - t0 - t1), waves * t2, res);
     plk_residual<K>(res, a.partial, blockIdx.x);
+}
+
+// One sweep.  16 and 32 queries are compiled for six resident CTAs (40
+// registers, a few spilled): at R-MAT scale 25 that took their sweeps from
+// 17.4 to 14.9 ms and from 31.6 to 26.4 ms; fewer queries keep the
+// compiler's choice (32-40 registers; capped at 40, 4 queries went from 4.9
+// to 5.4 ms).
+template <int K>
+__global__ void __launch_bounds__(PL_THREADS) k_plk_sweep(PlanBatch a) {
+    plk_sweep_body<K>(a);
+}
+
+template <int K>
+__global__ void __launch_bounds__(PL_THREADS, 6) k_plk_sweep_wide(PlanBatch a) {
+    plk_sweep_body<K>(a);
 }
 
 // hub rows: a thread per (row, query), the row's item partials in item order
@@ -973,7 +988,10 @@ gv_status plan_ppr_batch_k(gv_graph *g, const Plan &P, const uint32_t *sources, 
     // most of the SM's on-chip memory to L1, but room for the residual
     // tables (2 KB, plus 1 KB the system keeps per CTA) of 8 resident CTAs: a
     // zero carveout held the SM to two CTAs (25% of its warps)
-    cudaFuncSetAttribute(k_plk_sweep<K>, cudaFuncAttributePreferredSharedMemoryCarveout, 12);
+    void (*sweep)(PlanBatch) = nullptr;
+    if constexpr (K >= 16) sweep = k_plk_sweep_wide<K>;
+    else sweep = k_plk_sweep<K>;
+    cudaFuncSetAttribute(sweep, cudaFuncAttributePreferredSharedMemoryCarveout, 12);
     cudaGetLastError();
     PlanBatch a{};
     a.off = P.off;
@@ -1006,7 +1024,7 @@ gv_status plan_ppr_batch_k(gv_graph *g, const Plan &P, const uint32_t *sources, 
             a.cnew = cb;
             {
                 ProfScope ps(PROF_PULL, s);
-                GV_LAUNCH(k_plk_sweep<K>, grid, PL_THREADS, 0, s, a);
+                GV_LAUNCH(sweep, grid, PL_THREADS, 0, s, a);
                 if (P.rH) GV_LAUNCH(k_plk_hub_fin<K>, PL_FIN, PL_THREADS, 0, s, a, grid);
             }
             GV_LAUNCH(k_plk_done, 1, 32 * k, 0, s, (const double *)partial, nparts, k, eps, state);
@@ -1037,9 +1055,8 @@ gv_status plan_ppr_batch(gv_graph *g, const uint32_t *sources, int src_mem, uint
                          int max_iter, float *x_out, int32_t *sweeps, int mem, cudaStream_t s, bool *planned) {
     *planned = false;
     // Per sweep at R-MAT scale 25 (1.05 G entries): 3.9 ms for 2 queries,
-    // 9.8 for 8, 17.8 for 16 and 32.3 for 32, against 32.0, 37.1, 39.6 and
-    // 43.8 for the store's batched sweep and 3.3 ms for one query's plan
-    // sweep; at scale 22, 0.45 to 3.5 ms against 4.4 to 5.6.
+    // 9.6 for 8, 15.0 for 16 and 26.0 for 32, against 31-43 ms for the
+    // store's batched sweep and 3.3 ms for one query's plan sweep.
     if (k < 2 || k > 32) return GV_OK;
     const uint32_t K = k <= 2 ? 2 : k <= 4 ? 4 : k <= 8 ? 8 : k <= 16 ? 16 : 32;
     Plan P{};
