@@ -431,34 +431,43 @@ extern "C" gv_status gv_serve_trace(gv_graph *g, const gv_serve_config *cfg, con
             if (read_ctl(g, &cc, us) == GV_OK) S.live_edges = cc.live_edges;
             else S.live_edges = g->d.P * (uint64_t)g->d.B;  // fall back to the pool's capacity
         }
+        const uint32_t first_group = group + 1;  // this dispatch's groups
         for (size_t j = 0; j < jobs.size(); ++j) {
             Job &jb = jobs[j];
             jb.epoch = epoch;
             jb.group = ++group;
             jb.mem = S.estimate(jb.kind, (uint32_t)jb.reqs.size());
             if (j && jobs[j - 1].kind != jb.kind) {
-                // Each kind takes its turn alone: beside one another the
-                // kinds ran several times slower (at scale 25 the triangle
+                // Each kind of the dispatch takes its turn: beside one another
+                // the kinds ran several times slower (at scale 25 the triangle
                 // count and PPR took 1.3 to 2.2 s beside BC passes, against
                 // about 0.3 s each alone), which held every result back.
+                // Groups of earlier dispatches keep running (their turn was
+                // then), so arrivals do not queue behind them.
                 std::unique_lock<std::mutex> lk(S.mu);
-                S.cv.wait(lk, [&] { return S.inflight == 0; });
-                // The device is idle: the workers free the previous kinds'
-                // scratch now, while their cudaFree waits for nothing (later,
-                // it would wait for the new kind's groups on the other workers).
-                for (uint32_t w = 0; w < W; ++w)
-                    if (S.held[w] && S.held_kind[w] != (int)jb.kind) {
-                        S.held_mem -= S.held[w];
-                        S.held[w] = 0;
-                        S.held_kind[w] = -1;
-                        S.release[w] = 1;
-                    }
-                S.cv.notify_all();
                 S.cv.wait(lk, [&] {
                     for (uint32_t w = 0; w < W; ++w)
-                        if (S.release[w]) return false;
+                        if (S.busy[w] && S.job[w].group >= first_group) return false;
                     return true;
                 });
+                if (S.inflight == 0) {
+                    // The device is idle: the workers free the previous kinds'
+                    // scratch now, while their cudaFree waits for nothing
+                    // (later, it would wait for the new kind's groups).
+                    for (uint32_t w = 0; w < W; ++w)
+                        if (S.held[w] && S.held_kind[w] != (int)jb.kind) {
+                            S.held_mem -= S.held[w];
+                            S.held[w] = 0;
+                            S.held_kind[w] = -1;
+                            S.release[w] = 1;
+                        }
+                    S.cv.notify_all();
+                    S.cv.wait(lk, [&] {
+                        for (uint32_t w = 0; w < W; ++w)
+                            if (S.release[w]) return false;
+                        return true;
+                    });
+                }
             }
             std::unique_lock<std::mutex> lk(S.mu);
             int w = -1;
