@@ -1154,6 +1154,13 @@ def run_gv(args, rank, world, local_rank):
                    "forward_ms_per_call": prof["bfs_level"][0] / bc_calls,
                    "dependency_ms_per_call": prof["bc_dep"][0] / bc_calls,
                    "gteps": m_now * args.bc_sources * bc_calls / (bc_ms / 1e3) / 1e9}
+        # algorithmic bytes per source: two passes over the adjacency (4 m
+        # each) and sigma, dist and delta read and written (2 n (8 + 4 + 4))
+        bc_alg = args.bc_sources * (8 * m_now + 32 * n)
+        bc_info["algorithmic_bytes_per_call"] = bc_alg
+        bc_info["hbm_frac"] = bc_alg / (bc_ms / bc_calls) / 1e6 / hbm_peak
+        bc_info["bytes_note"] = (f"per source 2*(4m) + n*(8 sigma + 4 dist + 4 delta)*2; fraction of "
+                                 f"{peak_src} HBM copy bandwidth")
     phases = {k: {"ms_total": v[0], "launches": v[1]} for k, v in prof.items() if v[1]}
     line = {"metric": METRIC, "value": value, "unit": "edge updates/s", "n_gpus": world, "steps": K,
             "warmup": W, "ms_per_step": elapsed_ms / K, "higher_is_better": True,
