@@ -1841,7 +1841,9 @@ gv_status tc_core_count(gv_graph *g, const TcBufs &b, uint64_t mplus, TcCore &k,
     }
     {
         ProfScope ps(PROF_TC_PROBE, s);
-        GV_LAUNCH(k_tcc_probe, 148 * 8, TCC_THREADS, 0, s, k, b.tcount, work + 1);
+        // 32 CTAs per SM of shares (7.0 ms for the probes at R-MAT scale 22,
+        // 7.7 with 8): the block scheduler evens out the rows' uneven work
+        GV_LAUNCH(k_tcc_probe, 148 * 32, TCC_THREADS, 0, s, k, b.tcount, work + 1);
     }
     cudaMemcpyAsync(work + 2, k.ctl + 1, 4, cudaMemcpyDeviceToDevice, s);  // core size (low word)
     return cuda_status(cudaGetLastError(), "tc core");
@@ -2006,7 +2008,7 @@ gv_status tc_run(gv_graph *g, cudaStream_t s, int mode, unsigned long long **tco
         nrest = core.ctl + 2;
     }
     {
-        const unsigned cgrid = grid_for(mplus, AN_THREADS / 8, 148 * 16);
+        const unsigned cgrid = grid_for(mplus, AN_THREADS / 8, 148 * 64);  // 4.1 ms at scale 22 (4.4 capped at 148 * 16)
         ProfScope ps(PROF_TC_COUNT, s);
         const unsigned long long *off_c = b.off;
         if (mode == TC_INCIDENT)

@@ -51,8 +51,13 @@ constexpr int MS_THREADS = 256;
 constexpr int MS_WARPS = MS_THREADS / 32;
 constexpr uint32_t MS_HEAVY_FILL = 1024;  // entries; above: one CTA per vertex
 constexpr uint32_t MS_TAB = 2048;         // blocks per shared-memory table window
-constexpr unsigned MS_LIGHT_GRID = 148 * 8;
-constexpr unsigned MS_HEAVY_GRID = 148 * 2;
+// CTAs of a level launch: many small shares, so the block scheduler evens
+// out the heavy-tailed work per vertex.  BC at R-MAT scale 25 (32 / 64
+// sources): 283 / 382 ms with 148 * (8 + 2) CTAs, 241 / 339 with twice as
+// many, 214 / 284 with 8 times, 207 / 287 with 16 times (this), 204 / 282
+// with 32 times.
+constexpr unsigned MS_LIGHT_GRID = 148 * 128;
+constexpr unsigned MS_HEAVY_GRID = 148 * 32;
 constexpr uint32_t MS_MAX_LEVELS = 1u << 16;
 constexpr uint32_t MS_MAX_NW = 2;
 

@@ -110,7 +110,14 @@ def test_reference_matches_oracle_and_libgv(tmp_path):
     (t / "script").write_text(
         f"graph {t}/g.mtx\ninsert {t}/i.mtx\ndump {t}/a1.bin\npagerank 0.85 1e-6 100 {t}/pr1.bin\ntc {t}/tc1.bin\n"
         f"delete {t}/d.mtx\ncompact\ndump {t}/a2.bin\npagerank 0.85 1e-6 100 {t}/pr2.bin\ntc {t}/tc2.bin\n")
-    r = subprocess.run([str(HARNESS), str(t / "script")], capture_output=True, text=True, timeout=600)
+    # The reference does not check its allocations (its pool is half of the
+    # GPU's memory, taken unchecked), and a run on a box whose memory is
+    # fragmented can end in a failed copy into a null buffer; one more try
+    # in a fresh process.
+    for attempt in range(2):
+        r = subprocess.run([str(HARNESS), str(t / "script")], capture_output=True, text=True, timeout=600)
+        if r.returncode == 0:
+            break
     assert r.returncode == 0, r.stderr[-2000:]
 
     o = oracle.OracleGraph(n)
