@@ -519,8 +519,12 @@ __global__ void __launch_bounds__(MS_THREADS) k_ms_fwd(DevGraph g, MsBufs<NW> b,
 
 // Pull (bottom-up) forward level: each candidate gathers the path counts of
 // its neighbours at level L; no atomics, one write of its row.
+// Five resident CTAs (48 registers, a few spilled) for the pull and the
+// dependency pass: at R-MAT scale 25, 64 sources, 290 -> 268 ms (two
+// requests in one pass 317 -> 302 ms) against four CTAs at 56-64 registers;
+// six (40 registers) were slower.
 template <int NW>
-__global__ void __launch_bounds__(MS_THREADS, 4) k_ms_pull(DevGraph g, MsBufs<NW> b,
+__global__ void __launch_bounds__(MS_THREADS, 5) k_ms_pull(DevGraph g, MsBufs<NW> b,
                                                            const typename MaskOf<NW>::type *__restrict__ mask) {
     if (!ms_pull_level(b)) return;  // k_ms_fwd does this level
     uint32_t vb, vgl, vgh;
@@ -731,7 +735,7 @@ __device__ __forceinline__ void ms_bwd_heavy(const DevGraph &g, const MsBufs<NW>
 }
 
 template <int NW>
-__global__ void __launch_bounds__(MS_THREADS, 4) k_ms_bwd(DevGraph g, MsBufs<NW> b,
+__global__ void __launch_bounds__(MS_THREADS, 5) k_ms_bwd(DevGraph g, MsBufs<NW> b,
                                                        const typename MaskOf<NW>::type *__restrict__ mask,
                                                        const typename MaskOf<NW>::type *__restrict__ deeper) {
     uint32_t vb, vgl, vgh;
