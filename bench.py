@@ -492,6 +492,12 @@ def run_batching(args, dev, hbm_peak):
     torch.cuda.synchronize()
     wq_ms = e[0].elapsed_time(e[1])
     wq_l1 = float((xw.double() - xb.double()).abs().sum(0).max())
+    # The two runs sum in different orders (the window's sweeps walk the
+    # store, the separate call sweeps the plan) and stop at different sweeps;
+    # each stops on an L1 step below epsilon, so each is within
+    # epsilon * alpha / (1 - alpha) of the fixed point.
+    wq_tol = 2 * EPS * ALPHA / (1 - ALPHA)
+    wq_tol_note = "2 eps alpha / (1 - alpha): each result within eps alpha / (1 - alpha) of the fixed point"
     wq_stats = {k: gq.last_stat(k) for k in ("window_captures", "window_replays")}
     gq.close()
     del xw, xb
@@ -502,7 +508,8 @@ def run_batching(args, dev, hbm_peak):
         "ms": wq_ms, "sweeps": sw_w, "plain_ms": plain_ms + pr_plain_ms,
         "speedup_vs_plain": (plain_ms + pr_plain_ms) / wq_ms,
         "separate_batched_ms": batched_ms + pr_batched_ms,
-        "max_query_l1_vs_separate_calls": wq_l1, "tolerance_l1": 1e-6, "graphs": wq_stats}
+        "max_query_l1_vs_separate_calls": wq_l1, "tolerance_l1": wq_tol, "tolerance_note": wq_tol_note,
+        "ok": wq_l1 <= wq_tol, "graphs": wq_stats}
     return {"workload": (f"R-MAT scale {scale} ef {args.edge_factor}, {len(batches)} batches log-uniform in "
                          f"[1K, 4M] updates, Zipf(1.1) sources, insert fraction U[0.2, 0.8]; 32 PPR queries"),
             "m_initial_entries": m0, "updates": tot, "edges_after_plain": m_p, "edges_after_batched": m_b,
@@ -535,7 +542,8 @@ def run_batching(args, dev, hbm_peak):
             "window_and_queries": window_queries,
             "parity": {"same_graph_as_batch_by_batch": same_graph, "entries": int(dig_p[0].sum()),
                        "tolerance": "bit-exact (degrees + order-independent digests)",
-                       "window_queries_max_l1_vs_separate_calls": wq_l1},
+                       "window_queries_max_l1_vs_separate_calls": wq_l1,
+                       "window_queries_tolerance_l1": wq_tol, "window_queries_ok": wq_l1 <= wq_tol},
             "autotune_best": best, "autotune": tune}
 
 
