@@ -1899,7 +1899,10 @@ gv_status tc_run(gv_graph *g, cudaStream_t s, int mode, unsigned long long **tco
         }
         dispatch_tpv(tpv, [&](auto t) {
             constexpr int T = decltype(t)::value;
-            GV_LAUNCH((k_tc_outdeg<T>), grid_for(n, AN_THREADS / T), AN_THREADS, 0, s, d, (const uint32_t *)deg, b.dplus);
+            // per-vertex lists of uneven length: many CTA shares (the snapshot
+            // 2.1 ms at R-MAT scale 22 against 2.4 capped at 148 * 8)
+            GV_LAUNCH((k_tc_outdeg<T>), grid_for(n, AN_THREADS / T, 148 * 32), AN_THREADS, 0, s, d, (const uint32_t *)deg,
+                      b.dplus);
         });
         if (it.nitems) {
             GV_LAUNCH(k_tc_items<false>, PULL_GRID, AN_THREADS, 0, s, d, (const uint32_t *)deg, it, icnt,
@@ -1914,7 +1917,7 @@ gv_status tc_run(gv_graph *g, cudaStream_t s, int mode, unsigned long long **tco
         cudaMemsetAsync(b.tcount, 0, (size_t)n * 8, s);
         dispatch_tpv(tpv, [&](auto t) {
             constexpr int T = decltype(t)::value;
-            GV_LAUNCH((k_tc_write<T>), grid_for(n, AN_THREADS / T), AN_THREADS, 0, s, d, (const uint32_t *)deg,
+            GV_LAUNCH((k_tc_write<T>), grid_for(n, AN_THREADS / T, 148 * 32), AN_THREADS, 0, s, d, (const uint32_t *)deg,
                       (const unsigned long long *)b.off, b.snap);
         });
         if (it.nitems)
@@ -1983,7 +1986,7 @@ gv_status tc_run(gv_graph *g, cudaStream_t s, int mode, unsigned long long **tco
         ProfScope ps(PROF_TC_SORT, s);
         GV_LAUNCH(k_tc_classify, grid_for(n, 256), 256, 0, s, (const unsigned long long *)b.off, n, b.snap, b.mid,
                   b.big, b.cnts, core_of);
-        GV_LAUNCH(k_tc_sort_mid, 148 * 4, AN_THREADS, 0, s, (const unsigned long long *)b.off, b.snap,
+        GV_LAUNCH(k_tc_sort_mid, 148 * 32, AN_THREADS, 0, s, (const unsigned long long *)b.off, b.snap,  // 1.1 ms (1.3 with 148 * 4)
                   (const uint32_t *)b.mid, (const unsigned long long *)b.cnts);
         // the longest list bounds the CTA sort's shared memory
         unsigned long long h[3] = {0, 0, 0};
